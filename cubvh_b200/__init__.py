@@ -1,0 +1,14 @@
+"""cubvh_b200: B200-native (sm_100a) mesh queries behind cubvh's Python API.
+
+    import cubvh_b200 as cubvh
+    bvh = cubvh.cuBVH(vertices, faces)
+    dist, face_id, uvw = bvh.unsigned_distance(points, return_uvw=True)
+    sdf, face_id, _ = bvh.signed_distance(points, mode="watertight")
+    pos, face_id, depth = bvh.ray_trace(rays_o, rays_d)
+    labels = cubvh.floodfill(occupancy)
+"""
+
+from ._lib import version
+from .api import cuBVH, floodfill
+
+__all__ = ["cuBVH", "floodfill", "version"]

@@ -1,0 +1,202 @@
+"""Drop-in query API of cubvh (reference: cubvh/api.py:1-140).
+
+``cuBVH(vertices, triangles)`` builds the BVH on the host (no GPU work; the
+first query on a device uploads it), ``ray_trace`` / ``unsigned_distance`` /
+``signed_distance`` take and return torch tensors with the reference's
+shapes and dtypes, ``state_dict`` / ``from_state_dict`` use the reference's
+record format, and ``floodfill`` labels free-voxel components.  Queries run
+on the current CUDA stream of the input's device and are asynchronous, like
+the reference's.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check, lib
+
+__all__ = ["cuBVH", "floodfill"]
+
+_sdf_mode_to_id = {
+    "watertight": 0,
+    "raystab": 1,
+}
+
+
+def _stream_ptr(device: torch.device) -> ctypes.c_void_p:
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def _ptr(t) -> ctypes.c_void_p:
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
+
+
+class _Handle:
+    """Owner of one native cubvh_bvh*."""
+
+    def __init__(self, raw: ctypes.c_void_p):
+        self.raw = raw
+
+    def __del__(self):
+        raw = getattr(self, "raw", None)
+        if raw is not None and raw.value and _lib._lib is not None:
+            _lib._lib.cubvh_bvh_destroy(raw)
+            self.raw = None
+
+
+def _mesh_arrays(vertices, triangles):
+    if torch.is_tensor(vertices):
+        vertices = vertices.detach().cpu().numpy()
+    if torch.is_tensor(triangles):
+        triangles = triangles.detach().cpu().numpy()
+    V = np.ascontiguousarray(np.asarray(vertices), dtype=np.float32)
+    F = np.asarray(triangles)
+    if V.ndim != 2 or V.shape[1] != 3:
+        raise RuntimeError(f"vertices must have shape [N, 3], got {tuple(V.shape)}")
+    if F.ndim != 2 or F.shape[1] != 3:
+        raise RuntimeError(f"triangles must have shape [M, 3], got {tuple(F.shape)}")
+    F = np.ascontiguousarray(F, dtype=np.int64)
+    return V, F
+
+
+class cuBVH:
+    def __init__(self, vertices, triangles):
+        # vertices: np.ndarray / torch.Tensor [N, 3]; triangles: [M, 3]
+        V, F = _mesh_arrays(vertices, triangles)
+        assert F.shape[0] > 8, "BVH needs at least 8 triangles."
+        raw = ctypes.c_void_p()
+        check(lib().cubvh_bvh_create(V.ctypes.data, V.shape[0], F.ctypes.data, F.shape[0],
+                                     ctypes.byref(raw)), "cuBVH")
+        self.impl = _Handle(raw)
+
+    # ---------------------------------------------------------------- info
+    def _info(self):
+        nf, nn, dp = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int32()
+        check(lib().cubvh_bvh_info(self.impl.raw, ctypes.byref(nf), ctypes.byref(nn), ctypes.byref(dp)),
+              "info")
+        return int(nf.value), int(nn.value), int(dp.value)
+
+    @property
+    def num_faces(self) -> int:
+        return self._info()[0]
+
+    # ----------------------------------------------------------- state dict
+    def state_dict(self):
+        """{'nodes': int32 [n, 9], 'triangles': int32 [F, 12]} in the
+        reference's record format (CPU tensors)."""
+        nn, nt = ctypes.c_int64(), ctypes.c_int64()
+        check(lib().cubvh_bvh_state_dict_sizes(self.impl.raw, ctypes.byref(nn), ctypes.byref(nt)),
+              "state_dict")
+        nodes = torch.empty(int(nn.value), 9, dtype=torch.int32)
+        tris = torch.empty(int(nt.value), 12, dtype=torch.int32)
+        check(lib().cubvh_bvh_state_dict(self.impl.raw, _ptr(nodes), _ptr(tris)), "state_dict")
+        return {"nodes": nodes, "triangles": tris}
+
+    @staticmethod
+    def from_state_dict(state_dict):
+        if "triangles" not in state_dict:
+            raise RuntimeError("state_dict missing 'triangles' tensor")
+        if "nodes" not in state_dict:
+            raise RuntimeError("State dict does not contain 'nodes'")
+        tris = state_dict["triangles"]
+        if not torch.is_tensor(tris) or tris.device.type != "cpu":
+            raise RuntimeError("triangles must be on CPU")
+        tris = tris.contiguous()
+        if tris.dtype != torch.int32 or tris.dim() != 2 or tris.shape[1] != 12:
+            raise RuntimeError("triangles must be an int32 [F, 12] tensor of triangle records")
+        raw = ctypes.c_void_p()
+        check(lib().cubvh_bvh_create_from_records(_ptr(tris), tris.shape[0], ctypes.byref(raw)),
+              "from_state_dict")
+        obj = cuBVH.__new__(cuBVH)
+        obj.impl = _Handle(raw)
+        return obj
+
+    # -------------------------------------------------------------- queries
+    def ray_trace(self, rays_o, rays_d):
+        # rays_o, rays_d: torch.Tensor, float, [N, 3]
+        rays_o = rays_o.float().contiguous()
+        rays_d = rays_d.float().contiguous()
+        if not rays_o.is_cuda: rays_o = rays_o.cuda()
+        if rays_d.device != rays_o.device: rays_d = rays_d.to(rays_o.device)
+
+        prefix = rays_o.shape[:-1]
+        rays_o = rays_o.view(-1, 3)
+        rays_d = rays_d.view(-1, 3)
+        N = rays_o.shape[0]
+
+        positions = torch.empty(N, 3, dtype=torch.float32, device=rays_o.device)
+        face_id = torch.empty(N, dtype=torch.int64, device=rays_o.device)
+        depth = torch.empty(N, dtype=torch.float32, device=rays_o.device)
+
+        with torch.cuda.device(rays_o.device):
+            check(lib().cubvh_ray_trace(self.impl.raw, _ptr(rays_o), _ptr(rays_d), N, _ptr(positions),
+                                        _ptr(face_id), _ptr(depth), _stream_ptr(rays_o.device)), "ray_trace")
+
+        return positions.view(*prefix, 3), face_id.view(*prefix), depth.view(*prefix)
+
+    def _distance(self, positions, return_uvw, mode):
+        positions = positions.float().contiguous()
+        if not positions.is_cuda: positions = positions.cuda()
+
+        prefix = positions.shape[:-1]
+        positions = positions.view(-1, 3)
+        N = positions.shape[0]
+
+        distances = torch.empty(N, dtype=torch.float32, device=positions.device)
+        face_id = torch.empty(N, dtype=torch.int64, device=positions.device)
+        uvw = torch.empty(N, 3, dtype=torch.float32, device=positions.device) if return_uvw else None
+
+        with torch.cuda.device(positions.device):
+            stream = _stream_ptr(positions.device)
+            if mode is None:
+                rc = lib().cubvh_unsigned_distance(self.impl.raw, _ptr(positions), N, _ptr(distances),
+                                                   _ptr(face_id), _ptr(uvw), stream)
+            else:
+                rc = lib().cubvh_signed_distance(self.impl.raw, _ptr(positions), N, mode, _ptr(distances),
+                                                 _ptr(face_id), _ptr(uvw), stream)
+            check(rc, "signed_distance" if mode is not None else "unsigned_distance")
+
+        distances = distances.view(*prefix)
+        face_id = face_id.view(*prefix)
+        if uvw is not None:
+            uvw = uvw.view(*prefix, 3)
+        return distances, face_id, uvw
+
+    def unsigned_distance(self, positions, return_uvw=False):
+        # positions: torch.Tensor, float, [N, 3]
+        return self._distance(positions, return_uvw, None)
+
+    def signed_distance(self, positions, return_uvw=False, mode="watertight"):
+        # positions: torch.Tensor, float, [N, 3]; inside is negative
+        return self._distance(positions, return_uvw, _sdf_mode_to_id[mode])
+
+
+def floodfill(grid, check_bounds: bool = False):
+    # grid: torch.Tensor, bool, [B, H, W, D] or [H, W, D]
+    # return: torch.Tensor, int32, same shape: -1 for occupied voxels, else the
+    # smallest linear index of the voxel's free component (not remapped)
+    grid = grid.contiguous()
+    if not grid.is_cuda: grid = grid.cuda()
+    squeeze = grid.dim() == 3
+    if squeeze:
+        grid = grid.unsqueeze(0)
+    if grid.dtype != torch.bool:
+        raise RuntimeError(f"floodfill expects a bool grid, got {grid.dtype}")
+    if grid.dim() != 4:
+        raise RuntimeError(f"floodfill expects [B, H, W, D] or [H, W, D], got {tuple(grid.shape)}")
+    B, H, W, D = (int(s) for s in grid.shape)
+    mask = torch.empty((B, H, W, D), dtype=torch.int32, device=grid.device)
+    with torch.cuda.device(grid.device):
+        nbytes = ctypes.c_size_t()
+        check(lib().cubvh_floodfill_workspace_size(B, H, W, D, ctypes.byref(nbytes)), "floodfill")
+        ws = torch.empty(max(int(nbytes.value), 1), dtype=torch.uint8, device=grid.device)
+        stream = _stream_ptr(grid.device)
+        check(lib().cubvh_floodfill(_ptr(grid), B, H, W, D, _ptr(mask), _ptr(ws), int(nbytes.value), stream),
+              "floodfill")
+        if check_bounds:
+            check(lib().cubvh_floodfill_check(_ptr(ws), B, H, W, D, stream), "floodfill")
+    return mask.squeeze(0) if squeeze else mask

@@ -1,0 +1,323 @@
+// C ABI (include/cubvh_b200.h): BVH handles, lazy per-device upload, query
+// and floodfill entry points.  Every entry point catches C++ exceptions and
+// turns them into a status code plus a per-thread message.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <exception>
+#include <deque>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/cubvh_b200.h"
+#include "build.h"
+#include "kernels.h"
+
+using namespace cubvh;
+
+struct DevCopy {
+    int device = -1;
+    CNode* nodes = nullptr;
+    CTri* tris = nullptr;
+};
+
+struct cubvh_bvh {
+    HostBvh host;
+    std::vector<float> xyz;       // [F, 9] a, b, c of each face, face order
+    std::vector<int64_t> ids;     // face id of each face (position for meshes)
+    std::mutex mu;
+    std::deque<DevCopy> dev;      // stable addresses across push_back
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+int cuda_fail(cudaError_t e, const char* what) {
+    return fail(CUBVH_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+std::mutex g_const_mu;
+std::vector<int> g_const_ready;  // devices whose __constant__ tables are set
+
+cudaError_t ensure_constants(int device) {
+    std::lock_guard<std::mutex> lk(g_const_mu);
+    for (int d : g_const_ready) if (d == device) return cudaSuccess;
+    const cudaError_t e = upload_constants();
+    if (e == cudaSuccess) g_const_ready.push_back(device);
+    return e;
+}
+
+// Device copy of the BVH on the current device (uploaded on first use).
+int device_copy(cubvh_bvh* h, DevCopy** out) {
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    std::lock_guard<std::mutex> lk(h->mu);
+    for (auto& d : h->dev)
+        if (d.device == device) { *out = &d; return CUBVH_OK; }
+    if ((e = ensure_constants(device)) != cudaSuccess) return cuda_fail(e, "constant upload");
+    DevCopy d;
+    d.device = device;
+    const size_t nb = h->host.nodes.size() * sizeof(CNode), tb = h->host.tris.size() * sizeof(CTri);
+    if ((e = cudaMalloc(&d.nodes, nb)) != cudaSuccess) return cuda_fail(e, "cudaMalloc(nodes)");
+    if ((e = cudaMalloc(&d.tris, tb)) != cudaSuccess) { cudaFree(d.nodes); return cuda_fail(e, "cudaMalloc(triangles)"); }
+    if ((e = cudaMemcpy(d.nodes, h->host.nodes.data(), nb, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(d.tris, h->host.tris.data(), tb, cudaMemcpyHostToDevice)) != cudaSuccess) {
+        cudaFree(d.nodes); cudaFree(d.tris);
+        return cuda_fail(e, "BVH upload");
+    }
+    h->dev.push_back(d);
+    *out = &h->dev.back();
+    return CUBVH_OK;
+}
+
+int finish_build(cubvh_bvh* h) {
+    std::string err;
+    if (!build_bvh(h->xyz.data(), (int64_t)h->ids.size(), h->host, err)) return fail(CUBVH_ERR_INVALID, err);
+    // triangle ids: stored face ids (int32 in the node layout)
+    for (auto& t : h->host.tris) {
+        const int64_t id = h->ids[(size_t)t.id];
+        if (id < INT32_MIN || id > INT32_MAX) return fail(CUBVH_ERR_INVALID, "face id does not fit in int32");
+        t.id = (int32_t)id;
+    }
+    return CUBVH_OK;
+}
+
+}  // namespace
+
+#define CUBVH_GUARD_BEGIN try {
+#define CUBVH_GUARD_END                                                          \
+    } catch (const std::bad_alloc&) {                                            \
+        return fail(CUBVH_ERR_NOMEM, "host allocation failed");                  \
+    } catch (const std::exception& ex) {                                         \
+        return fail(CUBVH_ERR_INVALID, ex.what());                               \
+    } catch (...) {                                                              \
+        return fail(CUBVH_ERR_INVALID, "unknown error");                         \
+    }
+
+extern "C" {
+
+const char* cubvh_version(void) { return "cubvh_b200 0.1.0 (sm_100a)"; }
+
+const char* cubvh_last_error(void) { return g_err.c_str(); }
+
+int cubvh_bvh_create(const float* vertices, int64_t n_vertices, const int64_t* faces, int64_t n_faces,
+                     cubvh_bvh** out) {
+    CUBVH_GUARD_BEGIN
+    if (!out) return fail(CUBVH_ERR_INVALID, "out is null");
+    *out = nullptr;
+    if (!vertices || !faces) return fail(CUBVH_ERR_INVALID, "vertices/faces is null");
+    if (n_vertices <= 0 || n_faces <= 0) return fail(CUBVH_ERR_INVALID, "empty mesh");
+    auto* h = new cubvh_bvh();
+    h->xyz.resize((size_t)n_faces * 9);
+    h->ids.resize((size_t)n_faces);
+    h->host.faces.resize((size_t)n_faces * 3);
+    h->host.n_vertices = n_vertices;
+    for (int64_t f = 0; f < n_faces; ++f) {
+        for (int k = 0; k < 3; ++k) {
+            const int64_t v = faces[3 * f + k];
+            if (v < 0 || v >= n_vertices) {
+                delete h;
+                return fail(CUBVH_ERR_INVALID, "face " + std::to_string(f) + " has vertex index " +
+                                                   std::to_string(v) + " outside [0, " + std::to_string(n_vertices) + ")");
+            }
+            std::memcpy(&h->xyz[(size_t)f * 9 + 3 * k], vertices + 3 * v, 3 * sizeof(float));
+            h->host.faces[(size_t)f * 3 + k] = (int32_t)v;
+        }
+        h->ids[(size_t)f] = f;
+    }
+    const int rc = finish_build(h);
+    if (rc != CUBVH_OK) { delete h; return rc; }
+    *out = h;
+    return CUBVH_OK;
+    CUBVH_GUARD_END
+}
+
+int cubvh_bvh_create_from_records(const int32_t* rec, int64_t n_faces, cubvh_bvh** out) {
+    CUBVH_GUARD_BEGIN
+    if (!out) return fail(CUBVH_ERR_INVALID, "out is null");
+    *out = nullptr;
+    if (!rec) return fail(CUBVH_ERR_INVALID, "triangle records are null");
+    if (n_faces <= 0) return fail(CUBVH_ERR_INVALID, "no triangle records");
+    auto* h = new cubvh_bvh();
+    h->xyz.resize((size_t)n_faces * 9);
+    h->ids.resize((size_t)n_faces);
+    for (int64_t f = 0; f < n_faces; ++f) {
+        std::memcpy(&h->xyz[(size_t)f * 9], rec + 12 * f, 9 * sizeof(float));
+        std::memcpy(&h->ids[(size_t)f], rec + 12 * f + 10, sizeof(int64_t));
+    }
+    const int rc = finish_build(h);
+    if (rc != CUBVH_OK) { delete h; return rc; }
+    *out = h;
+    return CUBVH_OK;
+    CUBVH_GUARD_END
+}
+
+int cubvh_bvh_destroy(cubvh_bvh* h) {
+    CUBVH_GUARD_BEGIN
+    if (!h) return CUBVH_OK;
+    int cur = 0;
+    const bool have = cudaGetDevice(&cur) == cudaSuccess;
+    for (auto& d : h->dev) {
+        if (cudaSetDevice(d.device) == cudaSuccess) { cudaFree(d.nodes); cudaFree(d.tris); }
+    }
+    if (have && !h->dev.empty()) cudaSetDevice(cur);
+    delete h;
+    return CUBVH_OK;
+    CUBVH_GUARD_END
+}
+
+int cubvh_bvh_info(const cubvh_bvh* h, int64_t* n_faces, int64_t* n_nodes, int32_t* depth) {
+    if (!h) return fail(CUBVH_ERR_INVALID, "bvh is null");
+    if (n_faces) *n_faces = (int64_t)h->ids.size();
+    if (n_nodes) *n_nodes = (int64_t)h->host.nodes.size();
+    if (depth) *depth = h->host.depth;
+    return CUBVH_OK;
+}
+
+int cubvh_bvh_state_dict_sizes(const cubvh_bvh* h, int64_t* n_node_records, int64_t* n_tri_records) {
+    CUBVH_GUARD_BEGIN
+    if (!h || !n_node_records || !n_tri_records) return fail(CUBVH_ERR_INVALID, "null argument");
+    RefFormat rf;
+    export_reference_format(h->xyz.data(), h->ids.data(), (int64_t)h->ids.size(), rf);
+    *n_node_records = (int64_t)(rf.nodes.size() / 9);
+    *n_tri_records = (int64_t)(rf.tris.size() / 12);
+    return CUBVH_OK;
+    CUBVH_GUARD_END
+}
+
+int cubvh_bvh_state_dict(const cubvh_bvh* h, int32_t* node_records, int32_t* tri_records) {
+    CUBVH_GUARD_BEGIN
+    if (!h || !node_records || !tri_records) return fail(CUBVH_ERR_INVALID, "null argument");
+    RefFormat rf;
+    export_reference_format(h->xyz.data(), h->ids.data(), (int64_t)h->ids.size(), rf);
+    std::memcpy(node_records, rf.nodes.data(), rf.nodes.size() * sizeof(int32_t));
+    std::memcpy(tri_records, rf.tris.data(), rf.tris.size() * sizeof(int32_t));
+    return CUBVH_OK;
+    CUBVH_GUARD_END
+}
+
+int cubvh_bvh_layout(const cubvh_bvh* h, void* nodes_out, void* tris_out) {
+    if (!h || !nodes_out || !tris_out) return fail(CUBVH_ERR_INVALID, "null argument");
+    std::memcpy(nodes_out, h->host.nodes.data(), h->host.nodes.size() * sizeof(CNode));
+    std::memcpy(tris_out, h->host.tris.data(), h->host.tris.size() * sizeof(CTri));
+    return CUBVH_OK;
+}
+
+int cubvh_bvh_upload(cubvh_bvh* h) {
+    CUBVH_GUARD_BEGIN
+    if (!h) return fail(CUBVH_ERR_INVALID, "bvh is null");
+    DevCopy* d;
+    return device_copy(h, &d);
+    CUBVH_GUARD_END
+}
+
+int cubvh_unsigned_distance(cubvh_bvh* h, const float* points, int64_t n, float* distances, int64_t* face_id,
+                            float* uvw, void* stream) {
+    return cubvh_signed_distance(h, points, n, 0xFFFFFFFFu, distances, face_id, uvw, stream);
+}
+
+int cubvh_signed_distance(cubvh_bvh* h, const float* points, int64_t n, uint32_t mode, float* distances,
+                          int64_t* face_id, float* uvw, void* stream) {
+    CUBVH_GUARD_BEGIN
+    if (!h) return fail(CUBVH_ERR_INVALID, "bvh is null");
+    if (n < 0) return fail(CUBVH_ERR_INVALID, "negative query count");
+    if (mode != 0 && mode != 1 && mode != 0xFFFFFFFFu)
+        return fail(CUBVH_ERR_INVALID, "mode must be 0 (watertight) or 1 (raystab)");
+    if (n == 0) return CUBVH_OK;
+    if (!points || !distances || !face_id) return fail(CUBVH_ERR_INVALID, "points/distances/face_id is null");
+    if (n > (int64_t)UINT32_MAX) return fail(CUBVH_ERR_INVALID, "more than 2^32-1 queries in one call");
+    DevCopy* d;
+    const int rc = device_copy(h, &d);
+    if (rc != CUBVH_OK) return rc;
+    const int kmode = mode == 0xFFFFFFFFu ? 0 : (int)mode + 1;
+    const cudaError_t e = launch_distance(kmode, uvw != nullptr, n, points, distances, face_id, uvw, d->nodes,
+                                          d->tris, (int)h->host.slot_of_face0, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "distance kernel launch");
+    return CUBVH_OK;
+    CUBVH_GUARD_END
+}
+
+int cubvh_ray_trace(cubvh_bvh* h, const float* rays_o, const float* rays_d, int64_t n, float* positions,
+                    int64_t* face_id, float* depth, void* stream) {
+    CUBVH_GUARD_BEGIN
+    if (!h) return fail(CUBVH_ERR_INVALID, "bvh is null");
+    if (n < 0) return fail(CUBVH_ERR_INVALID, "negative ray count");
+    if (n == 0) return CUBVH_OK;
+    if (!rays_o || !rays_d || !positions || !face_id || !depth)
+        return fail(CUBVH_ERR_INVALID, "null ray or output pointer");
+    DevCopy* d;
+    const int rc = device_copy(h, &d);
+    if (rc != CUBVH_OK) return rc;
+    const cudaError_t e = launch_ray(n, rays_o, rays_d, positions, face_id, depth, d->nodes, d->tris,
+                                     (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "ray kernel launch");
+    return CUBVH_OK;
+    CUBVH_GUARD_END
+}
+
+static int check_grid_dims(int B, int H, int W, int D) {
+    if (B < 0 || H < 0 || W < 0 || D < 0) return fail(CUBVH_ERR_INVALID, "negative grid dimension");
+    const int64_t ntot = (int64_t)B * H * W * D;
+    if (ntot >= (int64_t)INT32_MAX) return fail(CUBVH_ERR_INVALID, "grid has 2^31 or more voxels (int32 labels)");
+    return CUBVH_OK;
+}
+
+int cubvh_floodfill_workspace_size(int B, int H, int W, int D, size_t* bytes) {
+    if (!bytes) return fail(CUBVH_ERR_INVALID, "bytes is null");
+    const int rc = check_grid_dims(B, H, W, D);
+    if (rc != CUBVH_OK) return rc;
+    *bytes = floodfill_workspace_bytes(B, H, W, D);
+    return CUBVH_OK;
+}
+
+int cubvh_floodfill(const uint8_t* grid, int B, int H, int W, int D, int32_t* labels, void* workspace,
+                    size_t workspace_bytes, void* stream) {
+    CUBVH_GUARD_BEGIN
+    int rc = check_grid_dims(B, H, W, D);
+    if (rc != CUBVH_OK) return rc;
+    if ((int64_t)B * H * W * D == 0) return CUBVH_OK;
+    if (!grid || !labels) return fail(CUBVH_ERR_INVALID, "grid/labels is null");
+    const size_t need = floodfill_workspace_bytes(B, H, W, D);
+    cudaStream_t s = (cudaStream_t)stream;
+    void* ws = workspace;
+    cudaError_t e;
+    if (ws) {
+        if (workspace_bytes < need) return fail(CUBVH_ERR_INVALID, "workspace smaller than cubvh_floodfill_workspace_size()");
+        if (reinterpret_cast<uintptr_t>(ws) & 255) return fail(CUBVH_ERR_INVALID, "workspace must be 256-byte aligned");
+    } else if ((e = cudaMallocAsync(&ws, need, s)) != cudaSuccess) {
+        return cuda_fail(e, "cudaMallocAsync(floodfill workspace)");
+    }
+    e = launch_floodfill(grid, B, H, W, D, labels, ws, s);
+    if (!workspace) {
+        const cudaError_t e2 = cudaFreeAsync(ws, s);
+        if (e == cudaSuccess) e = e2;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "floodfill launch");
+    return CUBVH_OK;
+    CUBVH_GUARD_END
+}
+
+int cubvh_floodfill_check(const void* workspace, int B, int H, int W, int D, void* stream) {
+    CUBVH_GUARD_BEGIN
+    if (!workspace) return fail(CUBVH_ERR_INVALID, "workspace is null");
+    const int rc = check_grid_dims(B, H, W, D);
+    if (rc != CUBVH_OK) return rc;
+    int status = 0;
+    const char* p = static_cast<const char*>(workspace) + floodfill_status_offset(B, H, W, D);
+    cudaError_t e = cudaMemcpyAsync(&status, p, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "floodfill status read");
+    if (status != 0) return fail(CUBVH_ERR_DEVICE_BOUND, "floodfill: a union-find walk exceeded its step bound");
+    return CUBVH_OK;
+    CUBVH_GUARD_END
+}
+
+}  // extern "C"

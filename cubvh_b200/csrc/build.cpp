@@ -1,0 +1,365 @@
+// Host BVH construction: binned-SAH binary tree, collapsed to 8-wide nodes,
+// emitted in breadth-first order with quantised child boxes (layout.h).
+//
+// The reference builds a BVH4 by centroid median splits on the host
+// (src/bvh.cu:515-620) and stores 36-byte nodes; this builder targets the
+// 80-byte compressed node instead.  export_reference_format() writes the
+// reference's own record format for state_dict compatibility.
+#include "build.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <limits>
+#include <numeric>
+
+namespace cubvh {
+namespace {
+
+struct Box {
+    float lo[3] = {INFINITY, INFINITY, INFINITY};
+    float hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    void grow(const float* p) {
+        for (int k = 0; k < 3; ++k) { lo[k] = std::min(lo[k], p[k]); hi[k] = std::max(hi[k], p[k]); }
+    }
+    void grow(const Box& b) {
+        for (int k = 0; k < 3; ++k) { lo[k] = std::min(lo[k], b.lo[k]); hi[k] = std::max(hi[k], b.hi[k]); }
+    }
+    float area() const {
+        const float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+        if (!(dx >= 0.f)) return 0.f;
+        return 2.f * (dx * dy + dy * dz + dz * dx);
+    }
+};
+
+struct Node2 {
+    Box box;
+    int left = -1, right = -1;     // internal children
+    int begin = 0, count = 0;      // leaf range (count > 0 for leaves)
+};
+
+struct Builder {
+    const float* xyz;              // [F, 9]
+    std::vector<Box> pbox;
+    std::vector<float> cen;        // [F, 3]
+    std::vector<int> idx;
+    std::vector<Node2> nodes;
+
+    static constexpr int kBins = 32;
+    static constexpr float kTrav = 1.0f, kIsect = 1.0f;
+
+    int make_leaf(int b, int e, const Box& box) {
+        Node2 n; n.box = box; n.begin = b; n.count = e - b;
+        nodes.push_back(n);
+        return (int)nodes.size() - 1;
+    }
+
+    int build(int b, int e) {
+        Box box, cb;
+        for (int i = b; i < e; ++i) { box.grow(pbox[idx[i]]); cb.grow(&cen[3 * idx[i]]); }
+        const int n = e - b;
+        if (n == 1) return make_leaf(b, e, box);
+
+        // binned SAH over the three axes
+        float best_cost = INFINITY; int best_axis = -1, best_split = -1;
+        for (int ax = 0; ax < 3; ++ax) {
+            const float ext = cb.hi[ax] - cb.lo[ax];
+            if (!(ext > 0.f)) continue;
+            Box bb[kBins]; int bc[kBins] = {0};
+            const float k = (float)kBins * (1.f - 1e-6f) / ext;
+            for (int i = b; i < e; ++i) {
+                int bi = (int)((cen[3 * idx[i] + ax] - cb.lo[ax]) * k);
+                bi = std::min(std::max(bi, 0), kBins - 1);
+                bb[bi].grow(pbox[idx[i]]); bc[bi]++;
+            }
+            float ra[kBins]; int rc[kBins];
+            Box acc; int cnt = 0;
+            for (int i = kBins - 1; i > 0; --i) {
+                acc.grow(bb[i]); cnt += bc[i];
+                ra[i] = acc.area(); rc[i] = cnt;
+            }
+            acc = Box(); cnt = 0;
+            for (int i = 0; i < kBins - 1; ++i) {
+                acc.grow(bb[i]); cnt += bc[i];
+                if (cnt == 0 || rc[i + 1] == 0) continue;
+                const float c = acc.area() * cnt + ra[i + 1] * rc[i + 1];
+                if (c < best_cost) { best_cost = c; best_axis = ax; best_split = i; }
+            }
+        }
+        const float parea = std::max(box.area(), 1e-30f);
+        const float split_cost = kTrav + kIsect * best_cost / parea;
+        if (n <= kMaxLeafTris && (best_axis < 0 || kIsect * n <= split_cost))
+            return make_leaf(b, e, box);
+
+        int mid;
+        if (best_axis < 0) {
+            mid = b + n / 2;  // all centroids coincide: split the range
+        } else {
+            const float ext = cb.hi[best_axis] - cb.lo[best_axis];
+            const float k = (float)kBins * (1.f - 1e-6f) / ext;
+            auto it = std::partition(idx.begin() + b, idx.begin() + e, [&](int t) {
+                int bi = (int)((cen[3 * t + best_axis] - cb.lo[best_axis]) * k);
+                bi = std::min(std::max(bi, 0), kBins - 1);
+                return bi <= best_split;
+            });
+            mid = (int)(it - idx.begin());
+            if (mid == b || mid == e) mid = b + n / 2;
+        }
+        const int me = (int)nodes.size();
+        nodes.emplace_back();
+        nodes[me].box = box;
+        const int l = build(b, mid);
+        const int r = build(mid, e);
+        nodes[me].left = l; nodes[me].right = r;
+        return me;
+    }
+};
+
+// Smallest e such that o + 255 * 2^e >= hi in float arithmetic.
+int pick_exponent(float o, float hi) {
+    if (!(hi > o)) return -100;
+    int e = (int)std::ceil(std::log2((double)(hi - o) / 255.0)) - 1;
+    e = std::max(e, -100);
+    while (o + 255.0f * std::ldexp(1.0f, e) < hi) ++e;
+    return e;
+}
+
+void quantise_child(const CNode& nd, int j, const Box& cb, CNode& out) {
+    const float o[3] = {nd.ox, nd.oy, nd.oz};
+    const int ex[3] = {nd.ex, nd.ey, nd.ez};
+    uint8_t* qlo[3] = {out.qlo_x, out.qlo_y, out.qlo_z};
+    uint8_t* qhi[3] = {out.qhi_x, out.qhi_y, out.qhi_z};
+    for (int k = 0; k < 3; ++k) {
+        const float s = std::ldexp(1.0f, ex[k]);
+        int ql = (int)std::floor((double)(cb.lo[k] - o[k]) / (double)s);
+        int qh = (int)std::ceil((double)(cb.hi[k] - o[k]) / (double)s);
+        ql = std::min(std::max(ql, 0), 255); qh = std::min(std::max(qh, 0), 255);
+        while (ql > 0 && o[k] + (float)ql * s > cb.lo[k]) --ql;
+        while (qh < 255 && o[k] + (float)qh * s < cb.hi[k]) ++qh;
+        qlo[k][j] = (uint8_t)ql; qhi[k][j] = (uint8_t)qh;
+    }
+}
+
+void set_frame(CNode& nd, const Box& b) {
+    nd.ox = b.lo[0]; nd.oy = b.lo[1]; nd.oz = b.lo[2];
+    nd.ex = (int8_t)pick_exponent(b.lo[0], b.hi[0]);
+    nd.ey = (int8_t)pick_exponent(b.lo[1], b.hi[1]);
+    nd.ez = (int8_t)pick_exponent(b.lo[2], b.hi[2]);
+}
+
+// Error scales used by the single-precision filters of the query kernels.
+void set_error_scales(CTri& t) {
+    const float v[3][3] = {{t.ax, t.ay, t.az}, {t.bx, t.by, t.bz}, {t.cx, t.cy, t.cz}};
+    float e2 = 0.f, einf = 0.f;
+    for (int u = 0; u < 3; ++u) {
+        const float* q0 = v[u]; const float* q1 = v[(u + 1) % 3];
+        const float dx = q1[0] - q0[0], dy = q1[1] - q0[1], dz = q1[2] - q0[2];
+        e2 = std::max(e2, dx * dx + dy * dy + dz * dz);
+    }
+    for (int u = 1; u < 3; ++u)
+        for (int k = 0; k < 3; ++k) einf = std::max(einf, std::fabs(v[u][k] - v[0][k]));
+    t.e2 = e2; t.einf = einf;
+}
+
+Box tri_box(const CTri& t) {
+    Box b;
+    const float a[3] = {t.ax, t.ay, t.az}, bb[3] = {t.bx, t.by, t.bz}, c[3] = {t.cx, t.cy, t.cz};
+    b.grow(a); b.grow(bb); b.grow(c);
+    return b;
+}
+
+}  // namespace
+
+bool build_bvh(const float* xyz, int64_t nf, HostBvh& out, std::string& err) {
+    if (nf <= 0) { err = "mesh has no faces"; return false; }
+    if (nf > (int64_t)(1 << 28)) { err = "too many faces (limit 2^28)"; return false; }
+    for (int64_t i = 0; i < nf * 9; ++i)
+        if (!std::isfinite(xyz[i])) { err = "vertex coordinates must be finite"; return false; }
+
+    Builder B;
+    B.xyz = xyz;
+    B.pbox.resize(nf); B.cen.resize(3 * nf); B.idx.resize(nf);
+    for (int64_t f = 0; f < nf; ++f) {
+        Box b; b.grow(xyz + 9 * f); b.grow(xyz + 9 * f + 3); b.grow(xyz + 9 * f + 6);
+        B.pbox[f] = b;
+        for (int k = 0; k < 3; ++k) B.cen[3 * f + k] = 0.5f * (b.lo[k] + b.hi[k]);
+        B.idx[f] = (int)f;
+    }
+    B.nodes.reserve(2 * nf);
+    const int root = B.build(0, (int)nf);
+
+    // collapse to 8-wide: each wide node lists binary-tree nodes as children
+    auto expand = [&](int r) {
+        std::vector<int> ch;
+        if (B.nodes[r].count > 0) { ch.push_back(r); return ch; }
+        ch.push_back(B.nodes[r].left); ch.push_back(B.nodes[r].right);
+        while ((int)ch.size() < kWidth) {
+            int bi = -1; float ba = -1.f;
+            for (int i = 0; i < (int)ch.size(); ++i) {
+                const Node2& n = B.nodes[ch[i]];
+                if (n.count > 0) continue;
+                const float a = n.box.area();
+                if (a > ba) { ba = a; bi = i; }
+            }
+            if (bi < 0) break;
+            const int c = ch[bi];
+            ch[bi] = B.nodes[c].left;
+            ch.insert(ch.begin() + bi + 1, B.nodes[c].right);
+        }
+        return ch;
+    };
+
+    out.nodes.clear(); out.tris.clear();
+    out.tris.reserve(nf);
+    struct Item { int bin; int level; };
+    std::vector<Item> queue{{root, 1}};
+    out.nodes.emplace_back();
+    int max_depth = 1;
+    for (size_t qi = 0; qi < queue.size(); ++qi) {
+        const Item it = queue[qi];
+        const std::vector<int> ch = expand(it.bin);
+        CNode nd;
+        std::memset(&nd, 0, sizeof(nd));
+        std::memset(nd.meta, kEmpty, sizeof(nd.meta));
+        set_frame(nd, B.nodes[it.bin].box);
+        nd.child_base = (int32_t)out.nodes.size();
+        nd.tri_base = (int32_t)out.tris.size();
+        int slot = 0;
+        for (int j = 0; j < (int)ch.size(); ++j) {
+            const Node2& c = B.nodes[ch[j]];
+            quantise_child(nd, j, c.box, nd);
+            if (c.count > 0) {
+                const int off = (int)out.tris.size() - nd.tri_base;
+                for (int t = c.begin; t < c.begin + c.count; ++t) {
+                    const int f = B.idx[t];
+                    const float* p = xyz + 9 * (int64_t)f;
+                    CTri tr;
+                    tr.ax = p[0]; tr.ay = p[1]; tr.az = p[2]; tr.id = f;
+                    tr.bx = p[3]; tr.by = p[4]; tr.bz = p[5];
+                    tr.cx = p[6]; tr.cy = p[7]; tr.cz = p[8];
+                    set_error_scales(tr);
+                    if (f == 0) out.slot_of_face0 = (int64_t)out.tris.size();
+                    out.tris.push_back(tr);
+                }
+                nd.meta[j] = (uint8_t)(((c.count - 1) << 5) | off);
+            } else {
+                nd.meta[j] = (uint8_t)(0x80 | slot);
+                ++slot;
+                queue.push_back({ch[j], it.level + 1});
+                out.nodes.emplace_back();
+                max_depth = std::max(max_depth, it.level + 1);
+            }
+        }
+        nd.n_internal = (uint8_t)slot;
+        out.nodes[qi] = nd;
+    }
+    out.depth = max_depth;
+    const Box& rb = B.nodes[root].box;
+    for (int k = 0; k < 3; ++k) { out.lo[k] = rb.lo[k]; out.hi[k] = rb.hi[k]; }
+    if (out.depth > kMaxDepth) {
+        err = "BVH deeper than the traversal stack supports (" + std::to_string(out.depth) + " levels)";
+        return false;
+    }
+    return true;
+}
+
+void refit_host(HostBvh& bvh) {
+    // children always follow their parent in breadth-first order: sweep back
+    const int64_t nn = (int64_t)bvh.nodes.size();
+    std::vector<Box> nb(nn);
+    for (int64_t i = nn - 1; i >= 0; --i) {
+        CNode& nd = bvh.nodes[i];
+        Box cbox[kWidth];
+        Box all;
+        for (int j = 0; j < kWidth; ++j) {
+            const uint8_t m = nd.meta[j];
+            if (m == kEmpty) continue;
+            if (m & 0x80) cbox[j] = nb[nd.child_base + (m & 7)];
+            else {
+                const int off = m & 31, cnt = (m >> 5) + 1;
+                for (int t = 0; t < cnt; ++t) cbox[j].grow(tri_box(bvh.tris[nd.tri_base + off + t]));
+            }
+            all.grow(cbox[j]);
+        }
+        set_frame(nd, all);
+        for (int j = 0; j < kWidth; ++j)
+            if (nd.meta[j] != kEmpty) quantise_child(nd, j, cbox[j], nd);
+        nb[i] = all;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// reference record format (state_dict)
+// ---------------------------------------------------------------------------
+void export_reference_format(const float* xyz, const int64_t* ids, int64_t nf, RefFormat& out) {
+    struct RNode { float lo[3], hi[3]; int32_t left, right, escape; };
+    static_assert(sizeof(RNode) == 36, "reference node record is 36 bytes");
+    std::vector<int> order(nf);
+    std::iota(order.begin(), order.end(), 0);
+    std::vector<float> cen(3 * nf);
+    for (int64_t f = 0; f < nf; ++f)
+        for (int k = 0; k < 3; ++k)
+            cen[3 * f + k] = (xyz[9 * f + k] + xyz[9 * f + 3 + k] + xyz[9 * f + 6 + k]) / 3.0f;
+    auto box_of = [&](int b, int e, RNode& n) {
+        for (int k = 0; k < 3; ++k) { n.lo[k] = INFINITY; n.hi[k] = -INFINITY; }
+        for (int i = b; i < e; ++i)
+            for (int v = 0; v < 3; ++v)
+                for (int k = 0; k < 3; ++k) {
+                    const float c = xyz[9 * (int64_t)order[i] + 3 * v + k];
+                    n.lo[k] = std::min(n.lo[k], c); n.hi[k] = std::max(n.hi[k], c);
+                }
+    };
+    // 4-ary tree, exactly four children per inner node (the reference's
+    // traversal always reads four), leaves of at most 8 triangles: each inner
+    // range is ordered along its widest centroid axis and cut in four.
+    std::vector<RNode> nodes(1);
+    box_of(0, (int)nf, nodes[0]);
+    nodes[0].left = nodes[0].right = nodes[0].escape = -1;
+    struct W { int node, b, e; };
+    std::vector<W> stack;
+    if (nf > 8) stack.push_back({0, 0, (int)nf});
+    else { nodes[0].left = -1; nodes[0].right = -(int)nf - 1; }
+    while (!stack.empty()) {
+        const W w = stack.back(); stack.pop_back();
+        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (int i = w.b; i < w.e; ++i)
+            for (int k = 0; k < 3; ++k) {
+                lo[k] = std::min(lo[k], cen[3 * order[i] + k]); hi[k] = std::max(hi[k], cen[3 * order[i] + k]);
+            }
+        int ax = 0;
+        for (int k = 1; k < 3; ++k) if (hi[k] - lo[k] > hi[ax] - lo[ax]) ax = k;
+        std::stable_sort(order.begin() + w.b, order.begin() + w.e,
+                         [&](int a, int b) { return cen[3 * a + ax] < cen[3 * b + ax]; });
+        const int n = w.e - w.b;
+        const int first = (int)nodes.size();
+        nodes[w.node].left = first; nodes[w.node].right = first + 4;
+        for (int c = 0; c < 4; ++c) {
+            const int cb = w.b + (int)((int64_t)n * c / 4), ce = w.b + (int)((int64_t)n * (c + 1) / 4);
+            RNode rn; box_of(cb, ce, rn); rn.escape = -1;
+            if (ce - cb <= 8) { rn.left = -cb - 1; rn.right = -ce - 1; nodes.push_back(rn); }
+            else { rn.left = rn.right = 0; nodes.push_back(rn); stack.push_back({first + c, cb, ce}); }
+        }
+    }
+    // pre-order escape links: the next sibling, else the parent's escape
+    std::vector<std::pair<int, int>> work{{0, -1}};
+    while (!work.empty()) {
+        const auto [ni, esc] = work.back(); work.pop_back();
+        nodes[ni].escape = esc;
+        if (nodes[ni].left < 0) continue;  // leaf
+        const int f0 = nodes[ni].left, f1 = nodes[ni].right;
+        for (int c = f1 - 1; c >= f0; --c) work.push_back({c, c + 1 < f1 ? c + 1 : esc});
+    }
+    out.nodes.resize(nodes.size() * 9);
+    std::memcpy(out.nodes.data(), nodes.data(), nodes.size() * sizeof(RNode));
+    out.tris.assign(nf * 12, 0);
+    for (int64_t i = 0; i < nf; ++i) {
+        const int f = order[i];
+        float* dst = reinterpret_cast<float*>(&out.tris[12 * i]);
+        std::memcpy(dst, xyz + 9 * (int64_t)f, 9 * sizeof(float));
+        const int64_t id = ids ? ids[f] : (int64_t)f;
+        std::memcpy(&out.tris[12 * i + 10], &id, sizeof(int64_t));
+    }
+}
+
+}  // namespace cubvh

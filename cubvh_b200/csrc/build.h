@@ -1,0 +1,43 @@
+// Host-side BVH construction and the reference's state_dict format.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "layout.h"
+
+namespace cubvh {
+
+struct HostBvh {
+    std::vector<CNode> nodes;      // node 0 is the root
+    std::vector<CTri> tris;        // leaf-ordered soup
+    int depth = 0;                 // internal levels (root = 1)
+    int64_t slot_of_face0 = 0;     // soup slot of original face 0
+    float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};  // scene bounds
+    // face -> vertex indices, for refit / vertex gradients (empty when the
+    // BVH was created from triangle records)
+    std::vector<int32_t> faces;    // [F, 3], original face order
+    int64_t n_vertices = 0;
+};
+
+// Builds the wide BVH over triangles (a, b, c per face, original face index
+// = position).  tri_xyz: [F, 9] floats.  Returns false and sets err on bad input.
+bool build_bvh(const float* tri_xyz, int64_t n_faces, HostBvh& out, std::string& err);
+
+// Recomputes the quantised boxes of every node from the current triangle
+// soup, keeping the topology (used after the soup's vertices moved).
+void refit_host(HostBvh& bvh);
+
+// The reference's on-disk format (include/gpu/bvh.cuh:84-109,
+// src/api_gpu.cu:110-121): a BVH4 built by median splits (src/bvh.cu:515-620)
+// as int32 [n_nodes, 9] records (box min, box max, left, right, escape) and
+// the triangle soup in that BVH's order as int32 [F, 12] records (a, b, c,
+// 4 pad bytes, int64 original index).
+struct RefFormat {
+    std::vector<int32_t> nodes;    // n_nodes * 9
+    std::vector<int32_t> tris;     // n_faces * 12
+};
+// ids: face id of each triangle of tri_xyz (NULL = its position).
+void export_reference_format(const float* tri_xyz, const int64_t* ids, int64_t n_faces, RefFormat& out);
+
+}  // namespace cubvh

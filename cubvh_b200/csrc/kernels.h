@@ -1,0 +1,27 @@
+// Kernel launchers shared by the C-ABI layer (abi.cu).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "layout.h"
+
+namespace cubvh {
+
+cudaError_t upload_constants();
+
+// mode 0 unsigned, 1 watertight sign, 2 raystab sign
+cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts, float* dist, int64_t* fid,
+                            float* uvw, const CNode* nodes, const CTri* tris, int slot_face0,
+                            cudaStream_t stream);
+cudaError_t launch_ray(int64_t n, const float* ro, const float* rd, float* pos, int64_t* fid, float* depth,
+                       const CNode* nodes, const CTri* tris, cudaStream_t stream);
+
+// floodfill (floodfill.cu)
+size_t floodfill_workspace_bytes(int B, int H, int W, int D);
+cudaError_t launch_floodfill(const uint8_t* grid, int B, int H, int W, int D, int32_t* labels,
+                             void* workspace, cudaStream_t stream);
+// Offset of the int32 status word inside the floodfill workspace.
+size_t floodfill_status_offset(int B, int H, int W, int D);
+
+}  // namespace cubvh

@@ -1,0 +1,129 @@
+/*
+ * cubvh_b200 C ABI: mesh queries (unsigned / signed distance, closest-hit
+ * ray tracing) over a BVH, and voxel floodfill, on NVIDIA B200 (sm_100a).
+ *
+ * Plain C: pointers, sizes, int status codes.  Device pointers are CUDA
+ * device (or managed) memory on the current device; `stream` is a
+ * cudaStream_t passed as void* (NULL = the legacy default stream).  Query
+ * calls are asynchronous with respect to the host, like the reference's
+ * (they launch on the given stream and return).  No C++ exception crosses
+ * this boundary; on failure a call returns a non-zero status and
+ * cubvh_last_error() describes it (per calling thread).
+ *
+ * Each entry point names the reference interface it replaces (paths inside
+ * the ashawkey/cubvh project).
+ */
+#ifndef CUBVH_B200_H
+#define CUBVH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum cubvh_status {
+    CUBVH_OK = 0,
+    CUBVH_ERR_INVALID = 1,      /* bad argument (null pointer, size, mode) */
+    CUBVH_ERR_CUDA = 2,         /* a CUDA runtime call or launch failed */
+    CUBVH_ERR_DEVICE_BOUND = 3, /* a device-side loop bound was hit */
+    CUBVH_ERR_NOMEM = 4         /* host or device allocation failed */
+};
+
+typedef struct cubvh_bvh cubvh_bvh;
+
+/* Library version string. */
+const char* cubvh_version(void);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* cubvh_last_error(void);
+
+/* Build a BVH on the host from an indexed mesh; touches no GPU (the device
+ * copy is made by the first query on each device).
+ * vertices: float32 [n_vertices, 3] (host); faces: int64 [n_faces, 3] (host),
+ * each index in [0, n_vertices).  face_id outputs are face row indices.
+ * Replaces cuBVHImpl(vertices, triangles) + TriangleBvh4::build
+ * (src/api_gpu.cu:21-44, src/bvh.cu:515-620) behind create_cuBVH
+ * (src/bindings.cpp:23). */
+int cubvh_bvh_create(const float* vertices, int64_t n_vertices, const int64_t* faces, int64_t n_faces,
+                     cubvh_bvh** out);
+
+/* Build a BVH from triangle records in the reference's state_dict format:
+ * int32 [n_faces, 12] per record = float a[3], b[3], c[3], 4 pad bytes,
+ * int64 face id (host).  The reference's node records are not needed (the
+ * BVH is rebuilt).  Replaces cuBVHImpl(state_dict) (src/api_gpu.cu:47-68)
+ * behind from_state_dict (src/bindings.cpp:24). */
+int cubvh_bvh_create_from_records(const int32_t* tri_records, int64_t n_faces, cubvh_bvh** out);
+
+/* Release the BVH and its device copies.  Replaces the pybind-owned
+ * delete of cuBVH (src/bindings.cpp:17-21). */
+int cubvh_bvh_destroy(cubvh_bvh* bvh);
+
+/* Sizes / shape of the built BVH (host memory only). */
+int cubvh_bvh_info(const cubvh_bvh* bvh, int64_t* n_faces, int64_t* n_nodes, int32_t* depth);
+
+/* Reference-format state_dict: number of node records (int32 x 9 each) and
+ * triangle records (int32 x 12 each), then the records themselves written to
+ * host buffers of those sizes.  Replaces cuBVH::state_dict
+ * (src/api_gpu.cu:110-121, include/gpu/bvh.cuh:84-94). */
+int cubvh_bvh_state_dict_sizes(const cubvh_bvh* bvh, int64_t* n_node_records, int64_t* n_tri_records);
+int cubvh_bvh_state_dict(const cubvh_bvh* bvh, int32_t* node_records, int32_t* tri_records);
+
+/* Inspection (no counterpart in the reference): host copies of the
+ * in-memory layout, nodes as n_nodes * 80 bytes and triangles as
+ * n_faces * 48 bytes (see cubvh_b200/csrc/layout.h). */
+int cubvh_bvh_layout(const cubvh_bvh* bvh, void* nodes_out, void* tris_out);
+
+/* Copy the BVH to the current device now (otherwise the first query does;
+ * the first query on a device is therefore synchronous). */
+int cubvh_bvh_upload(cubvh_bvh* bvh);
+
+/* Unsigned distance from each point to the mesh.
+ * points float32 [n, 3]; distances float32 [n]; face_id int64 [n];
+ * uvw float32 [n, 3] barycentric weights of the closest point on face_id,
+ * or NULL.  Points farther than 1000 from every triangle get distance 0 and
+ * face 0.  Replaces cuBVH::unsigned_distance (src/api_gpu.cu:83-95,
+ * src/bvh.cu:468-488, 687-712). */
+int cubvh_unsigned_distance(cubvh_bvh* bvh, const float* points, int64_t n, float* distances, int64_t* face_id,
+                            float* uvw, void* stream);
+
+/* Signed distance, inside negative.  mode 0 = 'watertight' (sign of the
+ * averaged normal around the closest point), 1 = 'raystab' (negative iff all
+ * 64 stab rays of the query hit the mesh).  The raystab rays of point i use
+ * the query index i within this call.  Replaces cuBVH::signed_distance
+ * (src/api_gpu.cu:97-108, src/bvh.cu:430-466, 631-685). */
+int cubvh_signed_distance(cubvh_bvh* bvh, const float* points, int64_t n, uint32_t mode, float* distances,
+                          int64_t* face_id, float* uvw, void* stream);
+
+/* Closest hit along each ray with 0 <= t < 1000.
+ * rays_o, rays_d float32 [n, 3]; positions float32 [n, 3] = o + t d;
+ * face_id int64 [n] (-1 on a miss); depth float32 [n] (1000 on a miss).
+ * Replaces cuBVH::ray_trace (src/api_gpu.cu:70-81, src/bvh.cu:490-513,
+ * 714-740). */
+int cubvh_ray_trace(cubvh_bvh* bvh, const float* rays_o, const float* rays_d, int64_t n, float* positions,
+                    int64_t* face_id, float* depth, void* stream);
+
+/* Floodfill of a batch of boolean grids: grid uint8/bool [B, H, W, D]
+ * (nonzero = occupied), labels int32 [B, H, W, D]: -1 for occupied voxels,
+ * else the smallest global linear index of the voxel's 6-connected free
+ * component (neighbourhood as the reference: the memory of each volume read
+ * as C-order [D][H][W]).  B*H*W*D must be below 2^31.
+ * Scratch: pass `workspace` of at least cubvh_floodfill_workspace_size()
+ * bytes (device memory, 256-byte aligned), or NULL to let the call take it
+ * from the device's stream-ordered memory pool.  Asynchronous; when a
+ * workspace is passed, cubvh_floodfill_check() reports device-side bound
+ * hits of the last call that used it.
+ * Replaces floodfill (src/api_gpu.cu:136-152, include/gpu/floodfill.cuh:157-272). */
+int cubvh_floodfill_workspace_size(int B, int H, int W, int D, size_t* bytes);
+int cubvh_floodfill(const uint8_t* grid, int B, int H, int W, int D, int32_t* labels, void* workspace,
+                    size_t workspace_bytes, void* stream);
+/* Synchronises `stream` and returns CUBVH_ERR_DEVICE_BOUND if the floodfill
+ * that last used `workspace` (same B, H, W, D) hit a device-side bound. */
+int cubvh_floodfill_check(const void* workspace, int B, int H, int W, int D, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUBVH_B200_H */

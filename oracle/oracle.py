@@ -1,0 +1,195 @@
+"""ctypes front end of the CPU oracle (oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py, never by the cubvh_b200 package.  See the header
+of oracle.cpp for what is restated from which reference file, and for the
+pinning status (parity against the reference's own outputs is unpinned: the
+reference cannot be built in this image).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liborc.so")
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compile liborc.so with the committed Makefile (g++, OpenMP)."""
+    if force or not os.path.exists(_LIB_PATH) or \
+            os.path.getmtime(_LIB_PATH) < os.path.getmtime(os.path.join(_HERE, "oracle.cpp")):
+        subprocess.run(["make", "-s", "-C", _HERE, "liborc.so"], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        _lib = ctypes.CDLL(_LIB_PATH)
+        _lib.orc_ref_build.restype = ctypes.c_void_p
+        _lib.orc_ref_num_nodes.restype = ctypes.c_int64
+        _lib.orc_get_threads.restype = ctypes.c_int
+    return _lib
+
+
+def _p(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else ctypes.c_void_p(0)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _i64(a):
+    return np.ascontiguousarray(a, dtype=np.int64)
+
+
+I64 = ctypes.c_int64
+F64 = ctypes.c_double
+
+
+def set_threads(n: int):
+    lib().orc_set_threads(ctypes.c_int(n))
+
+
+def threads() -> int:
+    return int(lib().orc_get_threads())
+
+
+# ---------------------------------------------------------------- FP64 oracle
+def udf64(V, F, pts, tie_eps=1e-7):
+    """-> dist, fid (lowest index among exact minima), uvw, cp, n_near."""
+    V, F, pts = _f32(V), _i64(F), _f32(pts)
+    n = len(pts)
+    dist = np.empty(n, np.float64); fid = np.empty(n, np.int64)
+    uvw = np.empty((n, 3), np.float64); cp = np.empty((n, 3), np.float64)
+    nn = np.empty(n, np.int32)
+    lib().orc_udf64(_p(V), I64(len(V)), _p(F), I64(len(F)), _p(pts), I64(n), F64(tie_eps),
+                    _p(dist), _p(fid), _p(uvw), _p(cp), _p(nn))
+    return dist, fid, uvw, cp, nn
+
+
+def face_dist64(V, F, pts, fids):
+    V, F, pts, fids = _f32(V), _i64(F), _f32(pts), _i64(fids)
+    n = len(pts)
+    dist = np.empty(n, np.float64); uvw = np.empty((n, 3), np.float64)
+    lib().orc_face_dist64(_p(V), _p(F), _p(pts), _p(fids), I64(n), _p(dist), _p(uvw))
+    return dist, uvw
+
+
+def ray64(V, F, ro, rd, tmax=1000.0, eps_b=1e-9, eps_g=1e-9, tie_eps=1e-7):
+    """-> t (tmax on miss), fid (-1 on miss), flags (bit0 ambiguous, bit1 tie)."""
+    V, F, ro, rd = _f32(V), _i64(F), _f32(ro), _f32(rd)
+    n = len(ro)
+    t = np.empty(n, np.float64); fid = np.empty(n, np.int64); fl = np.empty(n, np.int32)
+    lib().orc_ray64(_p(V), _p(F), I64(len(F)), _p(ro), _p(rd), I64(n), F64(tmax), F64(eps_b),
+                    F64(eps_g), F64(tie_eps), _p(t), _p(fid), _p(fl))
+    return t, fid, fl
+
+
+def sdf_watertight64(V, F, pts):
+    V, F, pts = _f32(V), _i64(F), _f32(pts)
+    n = len(pts)
+    sd = np.empty(n, np.float64); fid = np.empty(n, np.int64); fl = np.empty(n, np.int32)
+    lib().orc_sdf_watertight64(_p(V), _p(F), I64(len(F)), _p(pts), I64(n), _p(sd), _p(fid), _p(fl))
+    return sd, fid, fl
+
+
+def sdf_raystab64(V, F, pts, i0=0, eps_b=1e-9, eps_g=1e-9):
+    V, F, pts = _f32(V), _i64(F), _f32(pts)
+    n = len(pts)
+    sd = np.empty(n, np.float64); fid = np.empty(n, np.int64); fl = np.empty(n, np.int32)
+    lib().orc_sdf_raystab64(_p(V), _p(F), I64(len(F)), _p(pts), I64(n), I64(i0), F64(eps_b),
+                            F64(eps_g), _p(sd), _p(fid), _p(fl))
+    return sd, fid, fl
+
+
+def pcg32_seq(initstate, initseq, n):
+    out = np.empty(n, np.uint32)
+    lib().orc_pcg32_seq(ctypes.c_uint64(initstate), ctypes.c_uint64(initseq), ctypes.c_int(n), _p(out))
+    return out
+
+
+def stab_offsets(n, i0=0):
+    out = np.empty((n, 2), np.float32)
+    lib().orc_stab_offsets(I64(n), I64(i0), _p(out))
+    return out
+
+
+def stab_dirs(n, i0=0, use_libm=False):
+    out = np.empty((n, 32, 3), np.float32)
+    lib().orc_stab_dirs(I64(n), I64(i0), ctypes.c_int(1 if use_libm else 0), _p(out))
+    return out
+
+
+def floodfill(grid):
+    """grid: bool/uint8 [B,H,W,D] or [H,W,D] -> int32 labels (reference semantics)."""
+    g = np.ascontiguousarray(grid, dtype=np.uint8)
+    squeeze = g.ndim == 3
+    if squeeze:
+        g = g[None]
+    B, H, W, D = g.shape
+    out = np.empty(g.shape, np.int32)
+    rc = lib().orc_floodfill(_p(g), ctypes.c_int(B), ctypes.c_int(H), ctypes.c_int(W),
+                             ctypes.c_int(D), _p(out))
+    if rc != 0:
+        raise ValueError("grid too large for int32 labels")
+    return out[0] if squeeze else out
+
+
+# ------------------------------------------------- FP32 mirror of the reference
+class RefBVH:
+    """FP32 restatement of the reference's BVH4 build + traversals (CPU)."""
+
+    def __init__(self, V, F, n_per_leaf=8):
+        V, F = _f32(V), _i64(F)
+        self._h = ctypes.c_void_p(lib().orc_ref_build(_p(V), I64(len(V)), _p(F), I64(len(F)),
+                                                      ctypes.c_int(n_per_leaf)))
+        self.n_faces = len(F)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _lib is not None:
+            _lib.orc_ref_free(h)
+            self._h = None
+
+    @property
+    def n_nodes(self):
+        return int(lib().orc_ref_num_nodes(self._h))
+
+    def state_dict_arrays(self):
+        nodes = np.empty((self.n_nodes, 9), np.int32)
+        tris = np.empty((self.n_faces, 12), np.int32)
+        lib().orc_ref_state(self._h, _p(nodes), _p(tris))
+        return nodes, tris
+
+    def unsigned_distance(self, pts, return_uvw=False, count=False):
+        pts = _f32(pts); n = len(pts)
+        d = np.empty(n, np.float32); fid = np.empty(n, np.int64)
+        uvw = np.empty((n, 3), np.float32) if return_uvw else None
+        c = np.zeros(2, np.int64) if count else None
+        lib().orc_ref_udf(self._h, _p(pts), I64(n), _p(d), _p(fid), _p(uvw), _p(c))
+        return (d, fid, uvw, c) if count else (d, fid, uvw)
+
+    def ray_trace(self, ro, rd, count=False):
+        ro, rd = _f32(ro), _f32(rd); n = len(ro)
+        pos = np.empty((n, 3), np.float32); fid = np.empty(n, np.int64); dep = np.empty(n, np.float32)
+        c = np.zeros(2, np.int64) if count else None
+        lib().orc_ref_ray(self._h, _p(ro), _p(rd), I64(n), _p(pos), _p(fid), _p(dep), _p(c))
+        return (pos, fid, dep, c) if count else (pos, fid, dep)
+
+    def signed_distance(self, pts, mode=0, return_uvw=False, count=False):
+        pts = _f32(pts); n = len(pts)
+        d = np.empty(n, np.float32); fid = np.empty(n, np.int64)
+        uvw = np.empty((n, 3), np.float32) if return_uvw else None
+        c = np.zeros(2, np.int64) if count else None
+        lib().orc_ref_sdf(self._h, _p(pts), I64(n), ctypes.c_int(mode), _p(d), _p(fid), _p(uvw), _p(c))
+        return (d, fid, uvw, c) if count else (d, fid, uvw)

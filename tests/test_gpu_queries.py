@@ -1,0 +1,222 @@
+"""GPU parity of the query kernels against the FP64 CPU oracle.
+
+The kernels decide every distance, closest point, uvw, hit and sign in double
+with the oracle's operation order, so on the same float inputs the float32
+outputs must equal the oracle's double results rounded to float32 (bit for
+bit), and face_id must equal the oracle's lowest-index minimiser.  The
+tolerance the north star allows (1e-6 relative / 1e-7 absolute) is checked
+as well and the maximum error reported.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+import cubvh_b200 as cubvh
+from cubvh_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+RTOL, ATOL = 1e-6, 1e-7
+
+
+def _np(t):
+    return t.detach().cpu().numpy()
+
+
+def assert_close(got, want, what):
+    err = np.abs(got.astype(np.float64) - want)
+    bound = ATOL + RTOL * np.abs(want)
+    bad = err > bound
+    assert not bad.any(), f"{what}: {bad.sum()} outside tolerance, max err {err.max():.3g}"
+    return float(err.max()) if err.size else 0.0
+
+
+def check_udf(oracle, v, f, pts, out, with_uvw=True):
+    d, fid, uvw = out
+    od, ofid, ouvw, _, nn = oracle.udf64(v, f, pts)
+    d, fid = _np(d), _np(fid)
+    assert_close(d, od, "distance")
+    assert np.array_equal(d, od.astype(np.float32)), f"distance bits differ at {np.nonzero(d != od.astype(np.float32))[0][:8]}"
+    bad = fid != ofid
+    assert not bad.any(), f"face_id differs at {bad.sum()} points (ties there: {nn[bad][:8]})"
+    if with_uvw:
+        uvw = _np(uvw)
+        assert_close(uvw, ouvw, "uvw")
+        assert np.array_equal(uvw, ouvw.astype(np.float32))
+
+
+@pytest.mark.parametrize("level,n", [(2, 4000), (4, 20000)])
+def test_udf_icosphere(oracle, dev, level, n):
+    v, f = W.icosphere(level, 0.8)
+    bvh = cubvh.cuBVH(v, f)
+    pts = W.uniform_points(n, level)
+    out = bvh.unsigned_distance(torch.from_numpy(pts).to(dev), return_uvw=True)
+    check_udf(oracle, v, f, pts, out)
+
+
+def test_udf_dodecahedron_randn(oracle, dev):
+    # the reference's unsigned_distance test setup: dodecahedron, randn points
+    v, f = W.dodecahedron()
+    bvh = cubvh.cuBVH(v, f)
+    pts = np.random.default_rng(11).standard_normal((5000, 3)).astype(np.float32)
+    out = bvh.unsigned_distance(torch.from_numpy(pts).to(dev), return_uvw=True)
+    check_udf(oracle, v, f, pts, out)
+    # closest point rebuilt from uvw + face_id (reference test, atol 1e-5)
+    d, fid, uvw = (_np(x) for x in out)
+    cp = np.einsum("nk,nkj->nj", uvw.astype(np.float64), v[f[fid]].astype(np.float64))
+    assert np.abs(np.linalg.norm(pts - cp, axis=1) - d).max() < 1e-5
+
+
+def test_udf_displaced_near_surface(oracle, dev):
+    v, f = W.displaced_icosphere(5, 1)
+    bvh = cubvh.cuBVH(v, f)
+    rng = np.random.default_rng(5)
+    pts = np.concatenate([W.surface_points(v, f, 6000, 0.02, rng), W.surface_points(v, f, 2000, 1e-4, rng),
+                          rng.uniform(-1, 1, (4000, 3)).astype(np.float32)])
+    out = bvh.unsigned_distance(torch.from_numpy(pts).to(dev), return_uvw=True)
+    check_udf(oracle, v, f, pts, out)
+
+
+def test_udf_tori_open_mesh(oracle, dev):
+    v, f = W.random_tori(2, n_tori=3, n_major=64, n_minor=16)
+    bvh = cubvh.cuBVH(v, f)
+    g = W.dense_grid(24)
+    out = bvh.unsigned_distance(torch.from_numpy(g).to(dev), return_uvw=False)
+    check_udf(oracle, v, f, g, out, with_uvw=False)
+
+
+def test_udf_far_points_and_shapes(oracle, dev):
+    v, f = W.icosphere(2, 0.8)
+    bvh = cubvh.cuBVH(v, f)
+    pts = torch.tensor([[2000.0, 0, 0], [0, 0, 999.0], [0.1, 0.2, 0.3]], device=dev)
+    d, fid, uvw = bvh.unsigned_distance(pts, return_uvw=True)
+    assert d[0].item() == 0.0 and fid[0].item() == 0     # beyond MAX_DIST: distance 0, face 0
+    od, ofid, ouvw, _, _ = oracle.udf64(v, f, _np(pts))
+    assert np.array_equal(_np(d), od.astype(np.float32)) and np.array_equal(_np(fid), ofid)
+    assert np.array_equal(_np(uvw), ouvw.astype(np.float32))
+    # prefix shapes, CPU float64 input, empty input
+    p = torch.from_numpy(W.uniform_points(60, 1)).double().view(3, 4, 5, 3)
+    d, fid, uvw = bvh.unsigned_distance(p, return_uvw=True)
+    assert d.shape == (3, 4, 5) and fid.shape == (3, 4, 5) and uvw.shape == (3, 4, 5, 3)
+    assert d.dtype == torch.float32 and fid.dtype == torch.int64 and d.is_cuda
+    d, fid, uvw = bvh.unsigned_distance(torch.zeros(0, 3, device=dev))
+    assert d.shape == (0,) and uvw is None
+
+
+def check_rays(oracle, v, f, ro, rd, out):
+    pos, fid, depth = (_np(x) for x in out)
+    ot, ofid, fl = oracle.ray64(v, f, ro, rd)
+    assert_close(depth, ot, "depth")
+    assert np.array_equal(depth, ot.astype(np.float32))
+    assert np.array_equal(fid, ofid), f"{(fid != ofid).sum()} ray faces differ"
+    opos = (ro.astype(np.float64) + ot[:, None] * rd.astype(np.float64)).astype(np.float32)
+    assert np.array_equal(pos, opos)
+    return fl
+
+
+def test_ray_trace_camera(oracle, dev):
+    v, f = W.displaced_icosphere(4, 1)
+    bvh = cubvh.cuBVH(v, f)
+    ro, rd = W.camera_rays(2, 64, 50.0, 2.5, 1)
+    out = bvh.ray_trace(torch.from_numpy(ro).to(dev), torch.from_numpy(rd).to(dev))
+    check_rays(oracle, v, f, ro, rd, out)
+    hit = _np(out[1]) >= 0
+    assert 0.1 < hit.mean() < 0.9
+
+
+def test_ray_trace_inside_and_random(oracle, dev):
+    v, f = W.random_tori(2, n_tori=3, n_major=48, n_minor=12)
+    bvh = cubvh.cuBVH(v, f)
+    rng = np.random.default_rng(9)
+    ro = rng.uniform(-1, 1, (6000, 3)).astype(np.float32)
+    rd = rng.standard_normal((6000, 3)).astype(np.float32)
+    rd[:100, 0] = 0.0          # axis-parallel components
+    rd[100:150, :2] = 0.0
+    rd /= np.linalg.norm(rd, axis=1, keepdims=True)
+    out = bvh.ray_trace(torch.from_numpy(ro).to(dev), torch.from_numpy(rd).to(dev))
+    check_rays(oracle, v, f, ro, rd, out)
+    assert out[0].shape == (6000, 3)
+
+
+def check_sdf(got, sd_o, fid_o, what):
+    d, fid, _ = (_np(x) if x is not None else None for x in got)
+    assert np.array_equal(fid, fid_o), f"{what}: face ids differ at {(fid != fid_o).sum()} points"
+    want = sd_o.astype(np.float32)
+    bad = d != want
+    assert not bad.any(), f"{what}: {bad.sum()} values differ, e.g. {d[bad][:5]} vs {want[bad][:5]}"
+    assert np.array_equal(np.signbit(d), np.signbit(want))
+
+
+def test_sdf_watertight(oracle, dev):
+    v, f = W.displaced_icosphere(4, 1)
+    bvh = cubvh.cuBVH(v, f)
+    rng = np.random.default_rng(2)
+    pts = np.concatenate([rng.uniform(-1, 1, (3000, 3)).astype(np.float32),
+                          W.surface_points(v, f, 3000, 0.02, rng)])
+    got = bvh.signed_distance(torch.from_numpy(pts).to(dev), return_uvw=True, mode="watertight")
+    sd, fid, fl = oracle.sdf_watertight64(v, f, pts)
+    check_sdf(got, sd, fid, "watertight")
+    r = np.linalg.norm(pts, axis=1)
+    inner = r < 0.5
+    assert (_np(got[0])[inner] < 0).all()
+
+
+@pytest.mark.parametrize("mesh", ["sphere", "tori"])
+def test_sdf_raystab(oracle, dev, mesh):
+    if mesh == "sphere":
+        v, f = W.displaced_icosphere(3, 1)
+    else:
+        v, f = W.random_tori(2, n_tori=2, n_major=32, n_minor=8)
+    bvh = cubvh.cuBVH(v, f)
+    rng = np.random.default_rng(4)
+    pts = np.concatenate([rng.uniform(-1, 1, (1500, 3)).astype(np.float32),
+                          W.surface_points(v, f, 1500, 0.02, rng)])
+    got = bvh.signed_distance(torch.from_numpy(pts).to(dev), mode="raystab")
+    sd, fid, fl = oracle.sdf_raystab64(v, f, pts)
+    check_sdf(got, sd, fid, "raystab")
+    assert got[2] is None
+
+
+def test_sdf_bad_mode(dev):
+    v, f = W.icosphere(1)
+    bvh = cubvh.cuBVH(v, f)
+    with pytest.raises(KeyError):
+        bvh.signed_distance(torch.zeros(4, 3, device=dev), mode="pathescape")
+
+
+def test_state_dict_roundtrip(oracle, dev):
+    v, f = W.displaced_icosphere(3, 1)
+    bvh = cubvh.cuBVH(v, f)
+    pts = torch.from_numpy(W.uniform_points(3000, 3)).to(dev)
+    d0, f0, u0 = bvh.unsigned_distance(pts, return_uvw=True)
+    sd = bvh.state_dict()
+    bvh2 = cubvh.cuBVH.from_state_dict({k: val.clone() for k, val in sd.items()})
+    d1, f1, u1 = bvh2.unsigned_distance(pts, return_uvw=True)
+    assert torch.equal(d0, d1) and torch.equal(f0, f1) and torch.equal(u0, u1)
+
+
+def test_load_reference_records(oracle, dev):
+    # records in the reference's byte format (as its state_dict() writes them)
+    v, f = W.displaced_icosphere(3, 1)
+    nodes, tris = oracle.RefBVH(v, f).state_dict_arrays()
+    bvh = cubvh.cuBVH.from_state_dict({"nodes": torch.from_numpy(nodes), "triangles": torch.from_numpy(tris)})
+    pts = W.uniform_points(3000, 8)
+    out = bvh.unsigned_distance(torch.from_numpy(pts).to(dev), return_uvw=True)
+    check_udf(oracle, v, f, pts, out)
+
+
+def test_reference_mirror_agreement(oracle, dev):
+    """Our exact results next to the FP32 restatement of the reference: the
+    distances agree to FP32 rounding and faces differ only at ties."""
+    v, f = W.icosphere(4, 0.8)
+    bvh = cubvh.cuBVH(v, f)
+    pts = W.uniform_points(20000, 0)
+    d, fid, _ = (_np(x) if x is not None else None for x in bvh.unsigned_distance(torch.from_numpy(pts).to(dev)))
+    rd, rfid, _ = oracle.RefBVH(v, f).unsigned_distance(pts)
+    assert np.abs(d.astype(np.float64) - rd).max() < 2e-7
+    diff = fid != rfid
+    if diff.any():
+        a, _ = oracle.face_dist64(v, f, pts[diff], fid[diff])
+        b, _ = oracle.face_dist64(v, f, pts[diff], rfid[diff])
+        assert np.abs(a - b).max() <= 1e-7
