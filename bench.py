@@ -1,0 +1,460 @@
+"""Throughput benchmark of the cubvh query path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload rays_displaced|udf_icosphere|dense_tori]
+
+Default workload (``rays_displaced``): displaced icosphere level 6 (81,920
+faces); one step = ray_trace of 33,554,432 camera rays (8 poses x 2048^2,
+fov 50 deg, radius 2.5) + signed_distance(mode='watertight') of 8,388,608
+points (half uniform in [-1,1]^3, half within +-0.02 of the surface).
+Metric: queries/s (rays + points) over the whole job.  Inputs are larger
+than L2 (805 MB of rays), so no L2 flush is inserted between steps.
+
+``value`` times the kernels with inputs and outputs resident in HBM; ``e2e``
+times the public API (cuBVH.ray_trace / signed_distance) fed from pinned host
+tensors, with every output copied back to pinned host memory inside the timed
+region.  ``--impl reference`` times the reference's algorithm restated on the
+CPU (the oracle's FP32 mirror of its BVH4 build and traversals) on all host
+cores, on a bounded sample of the same workload per step.
+
+Multi-GPU: one process per GPU (torchrun); each rank runs its own replica of
+the workload (weak scaling; the path has no cross-GPU exchange).
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "mesh queries/s (ray_trace + signed_distance watertight), 1 B200"
+# launches of this library's kernels per op call (floodfill: zero status,
+# pack, count, 3 scan passes, runs, union, root, root label, write)
+KERNELS_PER_OP = {"ray": 1, "sdf_watertight": 1, "udf": 1, "udf_uvw": 1, "floodfill": 11}
+
+
+# ----------------------------------------------------------------- helpers
+def _rank_info():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _profile_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch of `kernel` from a committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", f"traffic_{workload}.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)[kernel]["dram_bytes_per_full_launch"])
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clock and throttle reasons during a region."""
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu),
+                 "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ""
+            self.out = out
+        return False
+
+    def summary(self):
+        if self.proc is None:
+            return None
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in getattr(self, "out", "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0])); mx.append(float(f[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------- workloads
+def build_workload(name: str, res: int = 2048, sdf_points: int = 8 << 20):
+    from cubvh_b200 import workloads as W
+    if name == "rays_displaced":
+        w = W.rays_displaced(res=res, n_sdf=sdf_points)
+        return dict(name=name, vertices=w["vertices"], faces=w["faces"],
+                    ops=[("ray", (w["rays_o"], w["rays_d"])), ("sdf_watertight", (w["points"],))],
+                    desc=f"displaced icosphere L6 (81,920 faces); {8 * res * res:,} rays (8 x {res}^2 pinhole, "
+                         f"fov 50, r 2.5) + {sdf_points:,} watertight SDF points")
+    if name == "udf_icosphere":
+        w = W.udf_icosphere()
+        return dict(name=name, vertices=w["vertices"], faces=w["faces"],
+                    ops=[("udf_uvw", (w["points"],))],
+                    desc="icosphere L4 r 0.8 (5,120 faces); 1,048,576 points U[-1,1]^3, uvw on")
+    if name == "dense_tori":
+        w = W.dense_tori()
+        g = W.dense_grid(w["grid_res"])
+        return dict(name=name, vertices=w["vertices"], faces=w["faces"], ops=[("udf", (g,)), ("floodfill", (512,))],
+                    desc="12 tori (174,778 faces, 10% removed); UDF on the 512^3 grid + floodfill of udf < 2/512")
+    raise SystemExit(f"unknown workload {name}")
+
+
+def n_queries(op, args):
+    if op == "floodfill":
+        return 0
+    return len(args[0])
+
+
+def io_bytes_per_query(op):
+    return {"ray": 48, "sdf_watertight": 24, "udf": 24, "udf_uvw": 36}.get(op, 0)
+
+
+def traversal_counts(wl, sample_stride=64):
+    """Box / triangle tests per query of the reference traversal (FP32 mirror
+    of the reference, oracle/), measured on a strided sample."""
+    from oracle import oracle as O
+    ref = O.RefBVH(wl["vertices"], wl["faces"])
+    out = {}
+    for op, args in wl["ops"]:
+        if op == "floodfill":
+            continue
+        if op == "ray":
+            ro, rd = args[0][::sample_stride], args[1][::sample_stride]
+            *_, c = ref.ray_trace(ro, rd, count=True)
+            n = len(ro)
+        elif op == "sdf_watertight":
+            p = args[0][::sample_stride]
+            *_, c = ref.signed_distance(p, mode=0, count=True)
+            n = len(p)
+        else:
+            p = args[0][::sample_stride]
+            *_, c = ref.unsigned_distance(p, return_uvw=False, count=True)
+            n = len(p)
+        out[op] = (c[0] / n, c[1] / n)
+    return out
+
+
+# -------------------------------------------------------------- CPU arms
+def cpu_time_sample(wl, max_queries, threads=None):
+    """Time the reference's algorithm (oracle FP32 mirror) on a strided
+    sample of at most ~max_queries queries spread over every op; returns
+    (queries, seconds, threads, description)."""
+    from oracle import oracle as O
+    if threads:
+        O.set_threads(threads)
+    ref = O.RefBVH(wl["vertices"], wl["faces"])
+    total = sum(len(a[0]) for op, a in wl["ops"] if op != "floodfill")
+    stride = max(1, -(-total // int(max_queries)))
+    q, t, parts = 0, 0.0, []
+    for op, args in wl["ops"]:
+        if op == "floodfill":
+            continue
+        if op == "ray":
+            ro, rd = np.ascontiguousarray(args[0][::stride]), np.ascontiguousarray(args[1][::stride])
+            t0 = time.perf_counter(); ref.ray_trace(ro, rd); dt = time.perf_counter() - t0
+            n = len(ro)
+        else:
+            p = np.ascontiguousarray(args[0][::stride])
+            t0 = time.perf_counter()
+            if op == "sdf_watertight":
+                ref.signed_distance(p, mode=0)
+            else:
+                ref.unsigned_distance(p, return_uvw=(op == "udf_uvw"))
+            dt = time.perf_counter() - t0
+            n = len(p)
+        q += n; t += dt
+        parts.append(f"{op}: {n} of {len(args[0])}")
+    return q, t, O.threads(), "every %d-th query (%s)" % (stride, "; ".join(parts))
+
+
+def run_reference(args):
+    rank, world, _ = _rank_info()
+    if rank != 0:
+        return
+    wl = build_workload(args.workload, args.res, args.sdf_points)
+    per_step = 4 << 20        # bounded sample of the workload per step
+    for _ in range(args.warmup):
+        cpu_time_sample(wl, per_step)
+    qs, ts = 0, 0.0
+    for _ in range(args.steps):
+        q, t, thr, desc = cpu_time_sample(wl, per_step)
+        qs += q; ts += t
+    val = qs / ts
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": "queries/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * ts / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded meshes and queries)",
+        "config": {"workload": wl["name"], "description": wl["desc"], "sample": desc},
+        "cpu_baseline": {"value": val, "unit": "queries/s", "cores": thr, "kind": "port", "sample": desc},
+        "e2e": {"value": val, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# -------------------------------------------------------------- GPU arm
+def run_ours(args):
+    import torch
+    rank, world, local = _rank_info()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    import cubvh_b200 as cubvh
+    from cubvh_b200._lib import lib, check
+
+    wl = build_workload(args.workload, args.res, args.sdf_points)
+    bvh = cubvh.cuBVH(wl["vertices"], wl["faces"])
+    L = lib()
+    h = bvh.impl.raw
+    stream = torch.cuda.current_stream(dev)
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    P = lambda t: ctypes.c_void_p(t.data_ptr())
+
+    # device-resident inputs / outputs
+    dev_ops = []
+    for op, a in wl["ops"]:
+        if op == "ray":
+            ro = torch.from_numpy(a[0]).to(dev); rd = torch.from_numpy(a[1]).to(dev)
+            n = ro.shape[0]
+            outs = (torch.empty(n, 3, device=dev), torch.empty(n, dtype=torch.int64, device=dev),
+                    torch.empty(n, device=dev))
+            fn = (lambda ro=ro, rd=rd, n=n, o=outs: check(
+                L.cubvh_ray_trace(h, P(ro), P(rd), n, P(o[0]), P(o[1]), P(o[2]), sp), "ray_trace"))
+            dev_ops.append((op, n, fn, "k_ray"))
+        elif op in ("sdf_watertight", "udf", "udf_uvw"):
+            p = torch.from_numpy(a[0]).to(dev)
+            n = p.shape[0]
+            d = torch.empty(n, device=dev); fid = torch.empty(n, dtype=torch.int64, device=dev)
+            uvw = torch.empty(n, 3, device=dev) if op == "udf_uvw" else None
+            uptr = P(uvw) if uvw is not None else ctypes.c_void_p(0)
+            if op == "sdf_watertight":
+                fn = (lambda p=p, n=n, d=d, fid=fid: check(
+                    L.cubvh_signed_distance(h, P(p), n, 0, P(d), P(fid), ctypes.c_void_p(0), sp), "sdf"))
+                kname = "k_distance<1,false>"
+            else:
+                fn = (lambda p=p, n=n, d=d, fid=fid, u=uptr: check(
+                    L.cubvh_unsigned_distance(h, P(p), n, P(d), P(fid), u, sp), "udf"))
+                kname = "k_distance<0,%s>" % ("true" if uvw is not None else "false")
+            dev_ops.append((op, n, fn, kname))
+            if args.workload == "dense_tori":
+                occ_src = d
+        elif op == "floodfill":
+            res = a[0]
+            grid = torch.empty(res, res, res, dtype=torch.bool, device=dev)
+            lab = torch.empty(res, res, res, dtype=torch.int32, device=dev)
+            nb = ctypes.c_size_t()
+            check(L.cubvh_floodfill_workspace_size(1, res, res, res, ctypes.byref(nb)), "ws")
+            ws = torch.empty(nb.value, dtype=torch.uint8, device=dev)
+
+            def fn(res=res, grid=grid, lab=lab, ws=ws, nb=nb.value):
+                torch.lt(occ_src.view(res, res, res), 2.0 / res, out=grid)
+                check(L.cubvh_floodfill(P(grid), 1, res, res, res, P(lab), P(ws), nb, sp), "floodfill")
+            dev_ops.append((op, 0, fn, "floodfill"))
+
+    q_per_step = sum(n for _, n, _, _ in dev_ops)
+
+    def step(evs=None):
+        for i, (_, _, fn, _) in enumerate(dev_ops):
+            if evs is not None:
+                evs[i][0].record(stream)
+            fn()
+            if evs is not None:
+                evs[i][1].record(stream)
+
+    # warm-up (also uploads the BVH)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    kev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in dev_ops]
+           for _ in range(args.steps)]
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    with ClockSampler(local) as clk:
+        t0.record(stream)
+        for s in range(args.steps):
+            step(kev[s])
+        t1.record(stream)
+        barrier()
+    ms = t0.elapsed_time(t1)
+    per_op_ms = [sum(kev[s][i][0].elapsed_time(kev[s][i][1]) for s in range(args.steps)) / args.steps
+                 for i in range(len(dev_ops))]
+    if world > 1:
+        tt = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = world * q_per_step * args.steps / (ms / 1e3)
+
+    # ---- e2e through the public API from pinned host buffers
+    host_in = []
+    for op, a in wl["ops"]:
+        if op == "floodfill":
+            continue
+        host_in.append((op, [torch.from_numpy(x).pin_memory() for x in a]))
+    e2e_steps = max(2, min(args.steps, 5))
+    pinned_out = {}
+
+    def e2e_step():
+        h2d = d2h = 0
+        results = []
+        for op, tensors in host_in:
+            h2d += sum(t.numel() * t.element_size() for t in tensors)
+            if op == "ray":
+                res = bvh.ray_trace(tensors[0], tensors[1])
+            elif op == "sdf_watertight":
+                res = bvh.signed_distance(tensors[0], mode="watertight")
+            else:
+                res = bvh.unsigned_distance(tensors[0], return_uvw=(op == "udf_uvw"))
+            for j, r in enumerate(res):
+                if r is None:
+                    continue
+                key = (op, j)
+                if key not in pinned_out:
+                    pinned_out[key] = torch.empty(r.shape, dtype=r.dtype, pin_memory=True)
+                pinned_out[key].copy_(r, non_blocking=True)
+                d2h += r.numel() * r.element_size()
+            results.append(res)
+        return h2d, d2h
+
+    e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    # wall clock: host dispatch, both copies and the kernels, synchronised
+    w0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        h2d, d2h = e2e_step()
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - w0) * 1e3
+    barrier()
+    if world > 1:
+        tt = torch.tensor([e2e_ms], device=dev)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+    e2e_val = world * q_per_step * e2e_steps / (e2e_ms / 1e3)
+
+    line = None
+    if rank == 0:
+        # roofline of the dominant kernel: algorithmic bytes per launch (query
+        # I/O + box and triangle bytes of the reference traversal) / its time
+        counts = traversal_counts(wl)
+        peak, peak_kind = _peaks()
+        dom = max(range(len(dev_ops)), key=lambda i: per_op_ms[i])
+        op, n, _, kname = dev_ops[dom]
+        if op == "floodfill":
+            alg = 5.0 * 512 ** 3
+        else:
+            nb_, nt_ = counts[op]
+            alg = n * (io_bytes_per_query(op) + 24.0 * nb_ + 36.0 * nt_)
+        achieved = alg / (per_op_ms[dom] / 1e3) / 1e9
+        cpu_q, cpu_t, cpu_thr, cpu_desc = cpu_time_sample(wl, 16 << 20)
+        ops_detail = {}
+        for i, (o, nq, _, kn) in enumerate(dev_ops):
+            d = {"kernel": kn, "ms_per_launch": per_op_ms[i]}
+            if nq:
+                d["queries"] = nq
+                d["queries_per_s"] = nq / (per_op_ms[i] / 1e3)
+                if o in counts:
+                    d["ref_traversal_boxes_per_query"] = counts[o][0]
+                    d["ref_traversal_tris_per_query"] = counts[o][1]
+            ops_detail[o] = d
+        line = {
+            "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded meshes and queries)",
+            "config": {"workload": wl["name"], "description": wl["desc"], "queries_per_step": q_per_step,
+                       "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
+            "e2e": {"value": e2e_val, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "steps": e2e_steps},
+            "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": _profile_traffic(kname, wl["name"]),
+                         "algorithmic_bytes_per_launch": alg},
+            "cpu_baseline": {"value": cpu_q / cpu_t, "unit": "queries/s", "cores": cpu_thr, "kind": "port",
+                             "sample": cpu_desc},
+            "gpu_launches": args.steps * sum(KERNELS_PER_OP[o] for o, _, _, _ in dev_ops),
+            "clocks": clk.summary(),
+            "ops": ops_detail,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="rays_displaced",
+                    choices=["rays_displaced", "udf_icosphere", "dense_tori"])
+    ap.add_argument("--res", type=int, default=2048, help="camera resolution (rays_displaced)")
+    ap.add_argument("--sdf-points", type=int, default=8 << 20, help="SDF queries (rays_displaced)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

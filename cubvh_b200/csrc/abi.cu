@@ -238,8 +238,17 @@ int cubvh_signed_distance(cubvh_bvh* h, const float* points, int64_t n, uint32_t
     const int rc = device_copy(h, &d);
     if (rc != CUBVH_OK) return rc;
     const int kmode = mode == 0xFFFFFFFFu ? 0 : (int)mode + 1;
-    const cudaError_t e = launch_distance(kmode, uvw != nullptr, n, points, distances, face_id, uvw, d->nodes,
-                                          d->tris, (int)h->host.slot_of_face0, (cudaStream_t)stream);
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t wsb = query_workspace_bytes(kmode, n);
+    void* ws = nullptr;
+    cudaError_t e;
+    if (wsb && (e = cudaMallocAsync(&ws, wsb, s)) != cudaSuccess) return cuda_fail(e, "cudaMallocAsync(query workspace)");
+    e = launch_distance(kmode, uvw != nullptr, n, points, distances, face_id, uvw, d->nodes, d->tris,
+                        (int)h->host.slot_of_face0, ws, s);
+    if (ws) {
+        const cudaError_t e2 = cudaFreeAsync(ws, s);
+        if (e == cudaSuccess) e = e2;
+    }
     if (e != cudaSuccess) return cuda_fail(e, "distance kernel launch");
     return CUBVH_OK;
     CUBVH_GUARD_END

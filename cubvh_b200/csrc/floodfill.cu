@@ -26,11 +26,11 @@
 #include <cuda_runtime.h>
 
 #include "kernels.h"
+#include "scan.cuh"
 
 namespace cubvh {
 namespace {
 
-constexpr int kScanChunk = 2048;      // rows per scan block
 constexpr int kStepLimit = 1 << 24;   // bound on any union-find walk
 
 struct FFPlan {
@@ -47,7 +47,7 @@ FFPlan make_plan(int B, int H, int W, int D) {
     p.words = p.rows * p.wpr;
     p.max_runs = p.rows * (int64_t)((W + 1) / 2);
     p.ntot = p.rows * W;
-    const int64_t nblk = (p.rows + kScanChunk - 1) / kScanChunk;
+    const int64_t nblk = scan::num_chunks(p.rows);
     size_t o = 0;
     p.off_bits = o; o = align256(o + sizeof(uint32_t) * p.words);
     p.off_wpref = o; o = align256(o + sizeof(uint32_t) * p.words);
@@ -76,7 +76,7 @@ __global__ void k_pack(const uint8_t* __restrict__ grid, uint32_t* __restrict__ 
         if (lane == 0) bits[w] = m;
     }
 }
-// fast path for W % 16 == 0 with a 16-byte aligned grid: one uint4 (16
+// fast path for W % 32 == 0 with a 16-byte aligned grid: one uint4 (16
 // voxels) per thread, two threads per 32-bit word
 __global__ void k_pack16(const uint4* __restrict__ grid, uint32_t* __restrict__ bits, int64_t n16) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -117,61 +117,7 @@ __global__ void k_count(const uint32_t* __restrict__ bits, uint32_t* __restrict_
     rowcnt[r] = acc;
 }
 
-// 3. exclusive scan of rowcnt (in place, rows + 1 entries; the last becomes
-// the total) in three passes: block sums, scan of the sums, block scans.
-__global__ void k_scan_sums(const uint32_t* __restrict__ cnt, uint32_t* __restrict__ bsum, int64_t n) {
-    __shared__ uint32_t sh[32];
-    const int64_t base = (int64_t)blockIdx.x * kScanChunk;
-    uint32_t s = 0;
-    for (int i = threadIdx.x; i < kScanChunk; i += blockDim.x)
-        if (base + i < n) s += cnt[base + i];
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xFFFFFFFFu, s, o);
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        uint32_t v = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0;
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
-        if (threadIdx.x == 0) bsum[blockIdx.x] = v;
-    }
-}
-__global__ void k_scan_top(uint32_t* __restrict__ bsum, int64_t nblk) {
-    // single block of 1024 threads; each thread scans a contiguous slice
-    __shared__ uint32_t sh[1024];
-    const int64_t per = (nblk + 1023) / 1024;
-    const int64_t b0 = threadIdx.x * per, b1 = min(b0 + per, nblk);
-    uint32_t s = 0;
-    for (int64_t i = b0; i < b1; ++i) s += bsum[i];
-    sh[threadIdx.x] = s;
-    __syncthreads();
-    for (int o = 1; o < 1024; o <<= 1) {
-        const uint32_t v = threadIdx.x >= (unsigned)o ? sh[threadIdx.x - o] : 0;
-        __syncthreads();
-        sh[threadIdx.x] += v;
-        __syncthreads();
-    }
-    uint32_t run = threadIdx.x ? sh[threadIdx.x - 1] : 0;
-    for (int64_t i = b0; i < b1; ++i) { const uint32_t v = bsum[i]; bsum[i] = run; run += v; }
-    if (threadIdx.x == 1023) bsum[nblk] = sh[1023];
-}
-__global__ void k_scan_apply(uint32_t* __restrict__ cnt, const uint32_t* __restrict__ bsum, int64_t n) {
-    // one block of 1024 threads scans kScanChunk entries (2 per thread)
-    __shared__ uint32_t sh[1024];
-    const int64_t base = (int64_t)blockIdx.x * kScanChunk;
-    const int64_t i0 = base + 2 * threadIdx.x;
-    const uint32_t a = i0 < n ? cnt[i0] : 0, b = i0 + 1 < n ? cnt[i0 + 1] : 0;
-    sh[threadIdx.x] = a + b;
-    __syncthreads();
-    for (int o = 1; o < 1024; o <<= 1) {
-        const uint32_t v = threadIdx.x >= (unsigned)o ? sh[threadIdx.x - o] : 0;
-        __syncthreads();
-        sh[threadIdx.x] += v;
-        __syncthreads();
-    }
-    const uint32_t excl = (threadIdx.x ? sh[threadIdx.x - 1] : 0) + bsum[blockIdx.x];
-    if (i0 < n) cnt[i0] = excl;
-    if (i0 + 1 < n) cnt[i0 + 1] = excl + a;
-    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) cnt[n] = bsum[gridDim.x];
-}
+// 3. exclusive scan of the per-row counts: scan.cuh
 
 // 4a. run records: start index and self parent
 __global__ void k_runs(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ rowoff,
@@ -336,7 +282,6 @@ cudaError_t launch_floodfill(const uint8_t* grid, int B, int H, int W, int D, in
     int32_t* start = reinterpret_cast<int32_t*>(base + p.off_start);
     int32_t* parent = reinterpret_cast<int32_t*>(base + p.off_parent);
     int* status = reinterpret_cast<int*>(base + p.off_status);
-    const int64_t nblk = (p.rows + kScanChunk - 1) / kScanChunk;
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -351,9 +296,7 @@ cudaError_t launch_floodfill(const uint8_t* grid, int B, int H, int W, int D, in
     }
     const unsigned rgrid = (unsigned)((p.rows + 255) / 256);
     k_count<<<rgrid, 256, 0, stream>>>(bits, wpref, rowoff, p.rows, p.wpr);
-    k_scan_sums<<<(unsigned)nblk, 256, 0, stream>>>(rowoff, bsum, p.rows);
-    k_scan_top<<<1, 1024, 0, stream>>>(bsum, nblk);
-    k_scan_apply<<<(unsigned)nblk, 1024, 0, stream>>>(rowoff, bsum, p.rows);
+    scan::exclusive(rowoff, bsum, p.rows, stream);
     k_runs<<<rgrid, 256, 0, stream>>>(bits, rowoff, start, parent, p.rows, p.wpr, W);
     const unsigned ugrid = (unsigned)((2 * p.rows + 255) / 256);
     k_union<<<ugrid, 256, 0, stream>>>(bits, rowoff, wpref, parent, status, p.rows, p.wpr, H, D);

@@ -10,9 +10,15 @@ namespace cubvh {
 
 cudaError_t upload_constants();
 
-// mode 0 unsigned, 1 watertight sign, 2 raystab sign
+// Point queries at least this many are visited in Morton-cell order.
+constexpr int64_t kSortMinQueries = 2048;
+
+// Device scratch bytes launch_distance needs for n queries (0: none).
+size_t query_workspace_bytes(int mode, int64_t n);
+// mode 0 unsigned, 1 watertight sign, 2 raystab sign.  ws:
+// query_workspace_bytes(mode, n) bytes, 256-byte aligned.
 cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts, float* dist, int64_t* fid,
-                            float* uvw, const CNode* nodes, const CTri* tris, int slot_face0,
+                            float* uvw, const CNode* nodes, const CTri* tris, int slot_face0, void* ws,
                             cudaStream_t stream);
 cudaError_t launch_ray(int64_t n, const float* ro, const float* rd, float* pos, int64_t* fid, float* depth,
                        const CNode* nodes, const CTri* tris, cudaStream_t stream);

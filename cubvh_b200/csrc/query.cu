@@ -1,18 +1,39 @@
-// Query kernels: unsigned distance, signed distance (watertight / raystab) and
-// closest-hit ray tracing over one compressed 8-wide BVH (layout.h).
+// Query kernels over one compressed 8-wide BVH (layout.h): unsigned distance,
+// the two sign passes of signed distance (watertight / raystab), and
+// closest-hit ray tracing.
 //
-// Reference kernels replaced: src/bvh.cu:631-740 (unsigned_distance_kernel,
-// signed_distance_{watertight,raystab}_kernel, raytrace_kernel) and the
-// traversals they call (src/bvh.cu:250-427).  One thread owns one query; the
-// traversal stack (node or leaf reference + lower-bound key) lives in local
-// memory; children are visited nearest-first (sorted 32-bit keys).
+// Reference kernels replaced: src/bvh.cu:631-740 and the traversals they
+// call (src/bvh.cu:250-427): one thread per query, 128-thread blocks, a
+// 32-entry local stack, children re-sorted per visit.
+//
+// Execution model here:
+//  * one thread owns one query, but warps are persistent: each warp walks a
+//    block-cyclic sequence of 32-query blocks (warp w takes blocks w, w + W,
+//    w + 2W, ...) and hands the next query of its current block to any lane
+//    whose query finished (ballot + popc), so lanes never idle while the warp
+//    still has work; there are no global atomics and the assignment is
+//    deterministic;
+//  * traversal is "while-while": lanes keep descending inner nodes until
+//    every lane of the warp holds a leaf (or is done), then all test their
+//    leaves together, which keeps node and leaf work converged;
+//  * point queries are visited in Morton-cell order (a counting sort of the
+//    points into 2^(3b) cells of the BVH box) so that the 32 lanes of a warp
+//    traverse nearly the same nodes; the permutation only reorders work,
+//    every result is written to the query's own index;
+//  * children are visited nearest-first (8 keys sorted as packed 32-bit
+//    integers); the nearest child is descended directly, the rest pushed on
+//    a local-memory stack with their lower-bound key, re-checked on pop.
 #include <cstdint>
 #include <cuda_runtime.h>
 
 #include "geom.cuh"
 #include "kernels.h"
+#include "scan.cuh"
 
 namespace cubvh {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+constexpr int kQBlock = 128;  // threads per block of the query kernels
 
 // ------------------------------------------------------------------ nodes
 struct NodeView {
@@ -39,15 +60,20 @@ __device__ __forceinline__ NodeView load_node(const CNode* __restrict__ nodes, i
 __device__ __forceinline__ uint32_t meta_of(const NodeView& n, int j) {
     return ((j < 4 ? n.meta0 : n.meta1) >> (8 * (j & 3))) & 0xFFu;
 }
+// byte k of w as a float: 0x4B0000qq is 2^23 + q, minus 2^23 is q exactly
+__device__ __forceinline__ float qbyte(uint32_t w, int k) {
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u + (unsigned)k)) - 8388608.0f;
+}
+// origin + q * 2^e: exact product, one rounding (same as the host check)
 __device__ __forceinline__ void child_box(const NodeView& n, int j, float3& lo, float3& hi) {
     const int b = j & 3;
     const bool h = j >= 4;
-    lo.x = fmaf(qf(h ? n.lx1 : n.lx0, b), n.sx, n.ox);
-    lo.y = fmaf(qf(h ? n.ly1 : n.ly0, b), n.sy, n.oy);
-    lo.z = fmaf(qf(h ? n.lz1 : n.lz0, b), n.sz, n.oz);
-    hi.x = fmaf(qf(h ? n.hx1 : n.hx0, b), n.sx, n.ox);
-    hi.y = fmaf(qf(h ? n.hy1 : n.hy0, b), n.sy, n.oy);
-    hi.z = fmaf(qf(h ? n.hz1 : n.hz0, b), n.sz, n.oz);
+    lo.x = fmaf(qbyte(h ? n.lx1 : n.lx0, b), n.sx, n.ox);
+    lo.y = fmaf(qbyte(h ? n.ly1 : n.ly0, b), n.sy, n.oy);
+    lo.z = fmaf(qbyte(h ? n.lz1 : n.lz0, b), n.sz, n.oz);
+    hi.x = fmaf(qbyte(h ? n.hx1 : n.hx0, b), n.sx, n.ox);
+    hi.y = fmaf(qbyte(h ? n.hy1 : n.hy0, b), n.sy, n.oy);
+    hi.z = fmaf(qbyte(h ? n.hz1 : n.hz0, b), n.sz, n.oz);
 }
 // >= 0: internal node index; < 0: leaf, -(slot * 4 + count - 1) - 1
 __device__ __forceinline__ int child_ref(const NodeView& n, uint32_t m) {
@@ -90,152 +116,164 @@ __device__ __forceinline__ void leaf_range(int ref, int& s0, int& s1) {
     s0 = code >> 2; s1 = s0 + (code & 3) + 1;
 }
 
-// ---------------------------------------------------------- nearest triangle
-// Exact (double) nearest triangle within squared distance best (in/out);
-// ties -> lowest original face index.  slot = -1 if none.
-__device__ void nearest_tri(const CNode* __restrict__ nodes, const CTri* __restrict__ tris, float3 p,
-                            double& best, int& slot, int& id) {
-    int2 st[kStack];
+__device__ __forceinline__ float3 load3(const float* __restrict__ a, int64_t i) {
+    return make_float3(a[3 * i], a[3 * i + 1], a[3 * i + 2]);
+}
+
+// ------------------------------------------------------- unsigned distance
+// Warp-uniform stack of a packet traversal, distributed over the lanes'
+// registers: entry e lives in lane e % 32, register slot e / 32 (kStack = 96
+// entries).  push / pop are called by all lanes with the same arguments.
+struct WarpStack {
+    int r0 = 0, r1 = 0, r2 = 0;
+    uint32_t k0 = 0, k1 = 0, k2 = 0;
     int sp = 0;
-    st[sp++] = make_int2(0, 0);
-    float cull = cull_of(best);
-    const d3 pd = to_d3(p);
-    while (sp > 0) {
-        const int2 e = st[--sp];
-        if (__int_as_float(e.y) > cull) continue;
-        if (e.x >= 0) {
-            const NodeView n = load_node(nodes, e.x);
-            uint32_t k[8];
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                float3 lo, hi;
-                child_box(n, j, lo, hi);
-                const float d2 = box_d2(p, lo, hi);
-                k[j] = (meta_of(n, j) != kEmpty && d2 <= cull) ? ((__float_as_uint(d2) & ~7u) | (uint32_t)j)
-                                                                 : 0xFFFFFFFFu;
-            }
-            sort8(k);
-#pragma unroll
-            for (int i = 7; i >= 0; --i)
-                if (k[i] != 0xFFFFFFFFu)
-                    st[sp++] = make_int2(child_ref(n, meta_of(n, (int)(k[i] & 7u))), (int)(k[i] & ~7u));
-        } else {
-            int s0, s1;
-            leaf_range(e.x, s0, s1);
-            for (int s = s0; s < s1; ++s) {
-                const TriV t = load_tri(tris, s);
-                float err;
-                const float d2 = tri_d2_f(p, t, &err);
-                if (d2 - err > cull) continue;
+    __device__ __forceinline__ void push(int ref, uint32_t key) {
+        if ((int)(threadIdx.x & 31) == (sp & 31)) {
+            const int s = sp >> 5;
+            if (s == 0) { r0 = ref; k0 = key; } else if (s == 1) { r1 = ref; k1 = key; } else { r2 = ref; k2 = key; }
+        }
+        ++sp;
+    }
+    __device__ __forceinline__ void pop(int& ref, uint32_t& key) {
+        --sp;
+        const int s = sp >> 5;
+        ref = __shfl_sync(kFull, s == 0 ? r0 : (s == 1 ? r1 : r2), sp & 31);
+        key = __shfl_sync(kFull, s == 0 ? k0 : (s == 1 ? k1 : k2), sp & 31);
+    }
+    // next entry whose key some lane still needs (key <= cullmax)
+    __device__ __forceinline__ bool next(uint32_t cullmax, int& cur) {
+        while (sp > 0) {
+            int ref; uint32_t key;
+            pop(ref, key);
+            if (key <= cullmax) { cur = ref; return true; }
+        }
+        return false;
+    }
+};
+
+constexpr int kCand = 8;  // per-lane candidate list of the distance search
+
+// Exact nearest triangle of 32 Morton-adjacent points per warp (a packet):
+// the warp walks the union of the lanes' search paths with warp-uniform
+// control flow.  A child is visited if any lane's FP32 box distance is within
+// that lane's bound (ballot), in the order of the smallest such distance
+// (warp min).  Leaves run the FP32 triangle test in every lane; each lane
+// keeps U, an upper bound of its squared distance (FP32 estimate + its error
+// bound), and a short list of triangles whose lower bound is within U.  At
+// the end every lane evaluates its surviving candidates in double: the
+// minimum (ties -> lowest face index) is the exact nearest triangle.
+template <bool UVW, bool SLOT>
+__global__ void __launch_bounds__(kQBlock) k_udf(int64_t n, const uint32_t* __restrict__ order,
+                                                 const float* __restrict__ pts, float* __restrict__ dist,
+                                                 int64_t* __restrict__ face_id, float* __restrict__ uvw,
+                                                 int32_t* __restrict__ slot_out, const CNode* __restrict__ nodes,
+                                                 const CTri* __restrict__ tris, int slot_face0) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = warp * 32; base < n; base += nwarps * 32) {
+        const int64_t qi = base + lane;
+        const bool act = qi < n;
+        const int64_t idx = act ? (order ? (int64_t)order[qi] : qi) : 0;
+        const float3 p = act ? load3(pts, idx) : make_float3(0.f, 0.f, 0.f);
+        const d3 pd = to_d3(p);
+        // U: upper bound of the lane's nearest squared distance (MAX_DIST^2)
+        float U = act ? 1e6f : -1.f;
+        float cull = act ? U * 1.000002f : -1.f;
+        int cs[kCand];
+        float cl[kCand];
+        int nc = 0;
+        double bx = 1e6;     // exact best of flushed candidates
+        int sx = -1, ix = 0;
+        auto flush = [&](bool final_pass) {
+            for (int i = 0; i < nc; ++i) {
+                if (final_pass && cl[i] > U) continue;
+                const TriV t = load_tri(tris, cs[i]);
                 double bary[3]; d3 cp;
-                const double e64 = closest_on_tri_d(pd, to_d3(t.a), to_d3(t.b), to_d3(t.c), bary, &cp);
-                if (e64 < best || (e64 == best && (slot < 0 || t.id < id))) {
-                    best = e64; slot = s; id = t.id;
-                    cull = cull_of(best);
+                const double e = closest_on_tri_d(pd, to_d3(t.a), to_d3(t.b), to_d3(t.c), bary, &cp);
+                if (e < bx || (e == bx && (sx < 0 || t.id < ix))) { bx = e; sx = cs[i]; ix = t.id; }
+            }
+            nc = 0;
+        };
+        uint32_t cullmax = __reduce_max_sync(kFull, __float_as_uint(fmaxf(cull, 0.f)) | (act ? 0u : 0u));
+        WarpStack st;
+        int cur = 0;
+        bool live = __any_sync(kFull, act);
+        while (live) {
+            if (cur >= 0) {
+                const NodeView nd = load_node(nodes, cur);
+                uint32_t k[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    float3 lo, hi;
+                    child_box(nd, j, lo, hi);
+                    const float d2 = box_d2(p, lo, hi);
+                    const bool need = meta_of(nd, j) != kEmpty && d2 <= cull;
+                    const uint32_t kmin = __reduce_min_sync(kFull, need ? __float_as_uint(d2) : kFull);
+                    k[j] = kmin != kFull ? ((kmin & ~7u) | (uint32_t)j) : kFull;
                 }
+                sort8(k);
+#pragma unroll
+                for (int i = 7; i >= 1; --i)
+                    if (k[i] != kFull) st.push(child_ref(nd, meta_of(nd, (int)(k[i] & 7u))), k[i] & ~7u);
+                if (k[0] != kFull) cur = child_ref(nd, meta_of(nd, (int)(k[0] & 7u)));
+                else live = st.next(cullmax, cur);
+            } else {
+                int s0, s1;
+                leaf_range(cur, s0, s1);
+                for (int s = s0; s < s1; ++s) {
+                    const TriV t = load_tri(tris, s);
+                    float err;
+                    const float e32 = tri_d2_f(p, t, &err);
+                    const float lb = e32 - err;
+                    if (act && lb <= U) {
+                        U = fminf(U, e32 + err);
+                        if (nc == kCand) {  // keep only live candidates, else settle them exactly
+                            int m = 0;
+                            for (int i = 0; i < nc; ++i)
+                                if (cl[i] <= U) { cs[m] = cs[i]; cl[m] = cl[i]; ++m; }
+                            nc = m;
+                            if (nc == kCand) {
+                                flush(false);
+                                U = fminf(U, __double2float_ru(bx));
+                            }
+                        }
+                        cs[nc] = s; cl[nc] = lb; ++nc;
+                    }
+                }
+                cull = act ? U * 1.000002f : -1.f;
+                cullmax = __reduce_max_sync(kFull, __float_as_uint(fmaxf(cull, 0.f)));
+                live = st.next(cullmax, cur);
             }
         }
-    }
-}
-
-// --------------------------------------------------------------- ray search
-// Closest hit with 0 <= t < tmax (exact double t; ties -> lowest face index).
-__device__ void closest_hit(const CNode* __restrict__ nodes, const CTri* __restrict__ tris, float3 o, float3 d,
-                            double& best_t, int& slot, int& id) {
-    const float3 inv = make_float3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
-    const float dinf = f3inf(d);
-    const float tmaxf = (float)best_t;
-    const double tmax = best_t;
-    const d3 od = to_d3(o), dd = to_d3(d);
-    int2 st[kStack];
-    int sp = 0;
-    st[sp++] = make_int2(0, 0);
-    float cull = cull_of(best_t);
-    while (sp > 0) {
-        const int2 e = st[--sp];
-        if (__int_as_float(e.y) > cull) continue;
-        if (e.x >= 0) {
-            const NodeView n = load_node(nodes, e.x);
-            uint32_t k[8];
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                float3 lo, hi;
-                child_box(n, j, lo, hi);
-                float tn, tf;
-                box_ray(o, inv, lo, hi, tn, tf);
-                const float key = fmaxf(tn, 0.f);
-                k[j] = (meta_of(n, j) != kEmpty && tn <= tf && tf >= 0.f && key <= cull)
-                           ? ((__float_as_uint(key) & ~7u) | (uint32_t)j) : 0xFFFFFFFFu;
-            }
-            sort8(k);
-#pragma unroll
-            for (int i = 7; i >= 0; --i)
-                if (k[i] != 0xFFFFFFFFu)
-                    st[sp++] = make_int2(child_ref(n, meta_of(n, (int)(k[i] & 7u))), (int)(k[i] & ~7u));
+        if (!act) continue;
+        flush(true);
+        double d64;
+        if (sx < 0) {  // nothing within MAX_DIST: distance 0 on face 0
+            sx = slot_face0; d64 = 0.0;
+            ix = load_tri(tris, sx).id;
         } else {
-            int s0, s1;
-            leaf_range(e.x, s0, s1);
-            for (int s = s0; s < s1; ++s) {
-                const TriV t = load_tri(tris, s);
-                float tt, terr;
-                const int r = ray_tri_f(o, d, dinf, t, tmaxf, &tt, &terr);
-                if (r == 0 || tt - terr > cull) continue;
-                double t64;
-                if (!ray_tri_d(od, dd, to_d3(t.a), to_d3(t.b), to_d3(t.c), tmax, &t64)) continue;
-                if (t64 < best_t || (t64 == best_t && (slot < 0 || t.id < id))) {
-                    best_t = t64; slot = s; id = t.id;
-                    cull = cull_of(best_t);
-                }
-            }
+            d64 = __dsqrt_rn(bx);
+        }
+        dist[idx] = __double2float_rn(d64);
+        face_id[idx] = (int64_t)ix;
+        if (SLOT) slot_out[idx] = sx;
+        if (UVW) {
+            const TriV t = load_tri(tris, sx);
+            double bary[3]; d3 cp;
+            closest_on_tri_d(pd, to_d3(t.a), to_d3(t.b), to_d3(t.c), bary, &cp);
+            uvw[3 * idx] = __double2float_rn(bary[0]);
+            uvw[3 * idx + 1] = __double2float_rn(bary[1]);
+            uvw[3 * idx + 2] = __double2float_rn(bary[2]);
         }
     }
 }
 
-// Any hit with 0 <= t < tmax.
-__device__ bool any_hit(const CNode* __restrict__ nodes, const CTri* __restrict__ tris, float3 o, float3 d,
-                        double tmax) {
-    const float3 inv = make_float3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
-    const float dinf = f3inf(d);
-    const float tmaxf = (float)tmax;
-    const float cull = cull_of(tmax);
-    const d3 od = to_d3(o), dd = to_d3(d);
-    int st[kStack];
-    int sp = 0;
-    st[sp++] = 0;
-    while (sp > 0) {
-        const int ref = st[--sp];
-        if (ref >= 0) {
-            const NodeView n = load_node(nodes, ref);
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const uint32_t m = meta_of(n, j);
-                float3 lo, hi;
-                child_box(n, j, lo, hi);
-                float tn, tf;
-                box_ray(o, inv, lo, hi, tn, tf);
-                if (m != kEmpty && tn <= tf && tf >= 0.f && tn <= cull) st[sp++] = child_ref(n, m);
-            }
-        } else {
-            int s0, s1;
-            leaf_range(ref, s0, s1);
-            for (int s = s0; s < s1; ++s) {
-                const TriV t = load_tri(tris, s);
-                float tt, terr;
-                const int r = ray_tri_f(o, d, dinf, t, tmaxf, &tt, &terr);
-                if (r == 1) return true;
-                if (r < 0) {
-                    double t64;
-                    if (ray_tri_d(od, dd, to_d3(t.a), to_d3(t.b), to_d3(t.c), tmax, &t64)) return true;
-                }
-            }
-        }
-    }
-    return false;
-}
-
+// ------------------------------------------------------------ watertight
 // Sum of unit normals of every triangle whose squared distance to cp is
-// below 1e-6 (src/bvh.cu:356-396, without the division by the count, which
-// does not change the sign).
+// below 1e-6 (src/bvh.cu:356-396; the division by the count does not change
+// the sign and is omitted).
 __device__ d3 normal_sum(const CNode* __restrict__ nodes, const CTri* __restrict__ tris, d3 cp) {
     const float3 cf = make_float3(__double2float_rn(cp.x), __double2float_rn(cp.y), __double2float_rn(cp.z));
     const float cinf = f3inf(cf);
@@ -249,13 +287,13 @@ __device__ d3 normal_sum(const CNode* __restrict__ nodes, const CTri* __restrict
     while (sp > 0) {
         const int ref = st[--sp];
         if (ref >= 0) {
-            const NodeView n = load_node(nodes, ref);
+            const NodeView nd = load_node(nodes, ref);
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
-                const uint32_t m = meta_of(n, j);
+                const uint32_t m = meta_of(nd, j);
                 float3 lo, hi;
-                child_box(n, j, lo, hi);
-                if (m != kEmpty && box_d2(cf, lo, hi) <= r2) st[sp++] = child_ref(n, m);
+                child_box(nd, j, lo, hi);
+                if (m != kEmpty && box_d2(cf, lo, hi) <= r2) st[sp++] = child_ref(nd, m);
             }
         } else {
             int s0, s1;
@@ -278,93 +316,350 @@ __device__ d3 normal_sum(const CNode* __restrict__ nodes, const CTri* __restrict
     return sum;
 }
 
-// ------------------------------------------------------------------ kernels
-template <int MODE, bool UVW>
-__global__ void __launch_bounds__(128) k_distance(int64_t n, const float* __restrict__ pts,
-                                                  float* __restrict__ dist, int64_t* __restrict__ face_id,
-                                                  float* __restrict__ uvw, const CNode* __restrict__ nodes,
-                                                  const CTri* __restrict__ tris, int slot_face0) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float3 p = make_float3(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]);
-    double best = 1e6;  // MAX_DIST^2 (src/bvh.cu:17-18)
-    int slot = -1, id = 0;
-    nearest_tri(nodes, tris, p, best, slot, id);
-    double dist64;
-    if (slot < 0) {  // nothing within MAX_DIST: distance 0 on face 0
-        slot = slot_face0; dist64 = 0.0;
-        id = load_tri(tris, slot).id;
-    } else {
-        dist64 = __dsqrt_rn(best);
-    }
-    const d3 pd = to_d3(p);
-    double out = dist64;
-    if (MODE != 0 || UVW) {
-        const TriV t = load_tri(tris, slot);
+__global__ void __launch_bounds__(kQBlock) k_sign_watertight(int64_t n, const uint32_t* __restrict__ order,
+                                                             const float* __restrict__ pts,
+                                                             float* __restrict__ dist,
+                                                             const int32_t* __restrict__ slots,
+                                                             const CNode* __restrict__ nodes,
+                                                             const CTri* __restrict__ tris) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) {
+        const int64_t idx = order ? (int64_t)order[q] : q;
+        const d3 pd = to_d3(load3(pts, idx));
+        const TriV t = load_tri(tris, slots[idx]);
         double bary[3]; d3 cp;
         closest_on_tri_d(pd, to_d3(t.a), to_d3(t.b), to_d3(t.c), bary, &cp);
-        if (UVW) {
-            uvw[3 * i] = __double2float_rn(bary[0]);
-            uvw[3 * i + 1] = __double2float_rn(bary[1]);
-            uvw[3 * i + 2] = __double2float_rn(bary[2]);
-        }
-        if (MODE == 1) {
-            const d3 ns = normal_sum(nodes, tris, cp);
-            out = copysign(dist64, ddot(ns, dsub(pd, cp)));
+        const d3 ns = normal_sum(nodes, tris, cp);
+        // copysign(distance, avg_normal . (p - cp))
+        const double s = ddot(ns, dsub(pd, cp));
+        const float d = dist[idx];
+        dist[idx] = signbit(s) ? -d : d;
+    }
+}
+
+// --------------------------------------------------------------- raystab
+// Any hit with 0 <= t < tmax (FP32 filter, FP64 for undecided triangles).
+__device__ bool any_hit(const CNode* __restrict__ nodes, const CTri* __restrict__ tris, float3 o, float3 d,
+                        double tmax) {
+    const float3 inv = make_float3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    const float dinf = f3inf(d);
+    const float tmaxf = (float)tmax;
+    const float cull = cull_of(tmax);
+    int st[kStack];
+    int sp = 0;
+    st[sp++] = 0;
+    while (sp > 0) {
+        const int ref = st[--sp];
+        if (ref >= 0) {
+            const NodeView nd = load_node(nodes, ref);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const uint32_t m = meta_of(nd, j);
+                float3 lo, hi;
+                child_box(nd, j, lo, hi);
+                float tn, tf;
+                box_ray(o, inv, lo, hi, tn, tf);
+                if (m != kEmpty && tn <= tf && tf >= 0.f && tn <= cull) st[sp++] = child_ref(nd, m);
+            }
+        } else {
+            int s0, s1;
+            leaf_range(ref, s0, s1);
+            for (int s = s0; s < s1; ++s) {
+                const TriV t = load_tri(tris, s);
+                float tt, terr;
+                const int r = ray_tri_f(o, d, dinf, t, tmaxf, &tt, &terr);
+                if (r == 1) return true;
+                if (r < 0) {
+                    double t64;
+                    if (ray_tri_d(to_d3(o), to_d3(d), to_d3(t.a), to_d3(t.b), to_d3(t.c), tmax, &t64)) return true;
+                }
+            }
         }
     }
-    if (MODE == 2) {
-        const float2 off = stab_offset((uint32_t)i);
+    return false;
+}
+
+// Negative iff all 64 stab rays (for k = 0..31: -d_k, then +d_k) hit the mesh
+// within [0, 1000) (src/bvh.cu:408-427); the first miss ends the query.
+// Queries are visited in Morton-cell order so neighbouring lanes trace
+// neighbouring origins.
+__global__ void __launch_bounds__(kQBlock) k_sign_raystab(int64_t n, const uint32_t* __restrict__ order,
+                                                          const float* __restrict__ pts, float* __restrict__ dist,
+                                                          const CNode* __restrict__ nodes,
+                                                          const CTri* __restrict__ tris) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) {
+        const int64_t idx = order ? (int64_t)order[q] : q;
+        const float3 p = load3(pts, idx);
+        const float2 off = stab_offset((uint32_t)idx);
         bool inside = true;
         for (uint32_t k = 0; k < 32 && inside; ++k) {
             const float3 dir = stab_dir(k, off);
-            const float3 ndir = make_float3(-dir.x, -dir.y, -dir.z);
-            if (!any_hit(nodes, tris, p, ndir, 1000.0) || !any_hit(nodes, tris, p, dir, 1000.0)) inside = false;
+            if (!any_hit(nodes, tris, p, make_float3(-dir.x, -dir.y, -dir.z), 1000.0) ||
+                !any_hit(nodes, tris, p, dir, 1000.0))
+                inside = false;
         }
-        if (inside) out = -dist64;
+        if (inside) dist[idx] = -dist[idx];
     }
-    dist[i] = __double2float_rn(out);
-    face_id[i] = (int64_t)id;
 }
 
-__global__ void __launch_bounds__(128) k_ray(int64_t n, const float* __restrict__ ro, const float* __restrict__ rd,
-                                             float* __restrict__ pos, int64_t* __restrict__ face_id,
-                                             float* __restrict__ depth, const CNode* __restrict__ nodes,
-                                             const CTri* __restrict__ tris) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float3 o = make_float3(ro[3 * i], ro[3 * i + 1], ro[3 * i + 2]);
-    const float3 d = make_float3(rd[3 * i], rd[3 * i + 1], rd[3 * i + 2]);
-    double t = 1000.0;  // MAX_DIST
-    int slot = -1, id = -1;
-    closest_hit(nodes, tris, o, d, t, slot, id);
-    depth[i] = __double2float_rn(t);
-    pos[3 * i] = __double2float_rn(dA((double)o.x, dM(t, (double)d.x)));
-    pos[3 * i + 1] = __double2float_rn(dA((double)o.y, dM(t, (double)d.y)));
-    pos[3 * i + 2] = __double2float_rn(dA((double)o.z, dM(t, (double)d.z)));
-    face_id[i] = slot >= 0 ? (int64_t)id : (int64_t)-1;
+// ---------------------------------------------------------------- rays
+// Closest hit of 32 consecutive rays per warp (a packet): warp-uniform walk of
+// the union of the rays' paths, children in the order of the smallest entry
+// distance of any ray that needs them.  Each lane keeps U, an upper bound of
+// its closest hit (certain FP32 hits: t + error bound), and a short list of
+// triangles that may still be closer (certain or undecided hits whose lower
+// bound is within U); the list is settled in double at the end: exact t of
+// the closest hit, ties -> lowest face index.
+__global__ void __launch_bounds__(kQBlock) k_ray(int64_t n, const float* __restrict__ ro,
+                                                 const float* __restrict__ rd, float* __restrict__ pos,
+                                                 int64_t* __restrict__ face_id, float* __restrict__ depth,
+                                                 const CNode* __restrict__ nodes, const CTri* __restrict__ tris) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = warp * 32; base < n; base += nwarps * 32) {
+        const int64_t q = base + lane;
+        const bool act = q < n;
+        const float3 o = act ? load3(ro, q) : make_float3(0.f, 0.f, 0.f);
+        const float3 d = act ? load3(rd, q) : make_float3(1.f, 1.f, 1.f);
+        const float3 inv = make_float3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+        const float dinf = f3inf(d);
+        const d3 od = to_d3(o), dd = to_d3(d);
+        float U = act ? 1000.0f : -1.f;             // MAX_DIST
+        float cull = act ? U * 1.000002f : -1.f;
+        int cs[kCand];
+        float cl[kCand];
+        int nc = 0;
+        double bt = 1000.0;
+        int sx = -1, ix = -1;
+        auto flush = [&](bool final_pass) {
+            for (int i = 0; i < nc; ++i) {
+                if (final_pass && cl[i] > U) continue;
+                const TriV t = load_tri(tris, cs[i]);
+                double t64;
+                if (!ray_tri_d(od, dd, to_d3(t.a), to_d3(t.b), to_d3(t.c), 1000.0, &t64)) continue;
+                if (t64 < bt || (t64 == bt && (sx < 0 || t.id < ix))) { bt = t64; sx = cs[i]; ix = t.id; }
+            }
+            nc = 0;
+        };
+        uint32_t cullmax = __reduce_max_sync(kFull, __float_as_uint(fmaxf(cull, 0.f)));
+        WarpStack st;
+        int cur = 0;
+        bool live = __any_sync(kFull, act);
+        while (live) {
+            if (cur >= 0) {
+                const NodeView nd = load_node(nodes, cur);
+                uint32_t k[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    float3 lo, hi;
+                    child_box(nd, j, lo, hi);
+                    float tn, tf;
+                    box_ray(o, inv, lo, hi, tn, tf);
+                    const float key = fmaxf(tn, 0.f);
+                    const bool need = meta_of(nd, j) != kEmpty && tn <= tf && tf >= 0.f && key <= cull;
+                    const uint32_t kmin = __reduce_min_sync(kFull, need ? __float_as_uint(key) : kFull);
+                    k[j] = kmin != kFull ? ((kmin & ~7u) | (uint32_t)j) : kFull;
+                }
+                sort8(k);
+#pragma unroll
+                for (int i = 7; i >= 1; --i)
+                    if (k[i] != kFull) st.push(child_ref(nd, meta_of(nd, (int)(k[i] & 7u))), k[i] & ~7u);
+                if (k[0] != kFull) cur = child_ref(nd, meta_of(nd, (int)(k[0] & 7u)));
+                else live = st.next(cullmax, cur);
+            } else {
+                int s0, s1;
+                leaf_range(cur, s0, s1);
+                for (int s = s0; s < s1; ++s) {
+                    const TriV t = load_tri(tris, s);
+                    float tt, terr;
+                    const int r = ray_tri_f(o, d, dinf, t, 1000.0f, &tt, &terr);
+                    const float lb = tt - terr;
+                    if (act && r != 0 && lb <= U) {
+                        if (r == 1) U = fminf(U, tt + terr);
+                        if (nc == kCand) {
+                            int m = 0;
+                            for (int i = 0; i < nc; ++i)
+                                if (cl[i] <= U) { cs[m] = cs[i]; cl[m] = cl[i]; ++m; }
+                            nc = m;
+                            if (nc == kCand) {
+                                flush(false);
+                                if (sx >= 0) U = fminf(U, __double2float_ru(bt));
+                            }
+                        }
+                        cs[nc] = s; cl[nc] = lb; ++nc;
+                    }
+                }
+                cull = act ? U * 1.000002f : -1.f;
+                cullmax = __reduce_max_sync(kFull, __float_as_uint(fmaxf(cull, 0.f)));
+                live = st.next(cullmax, cur);
+            }
+        }
+        if (!act) continue;
+        flush(true);
+        depth[q] = __double2float_rn(bt);
+        pos[3 * q] = __double2float_rn(dA((double)o.x, dM(bt, (double)d.x)));
+        pos[3 * q + 1] = __double2float_rn(dA((double)o.y, dM(bt, (double)d.y)));
+        pos[3 * q + 2] = __double2float_rn(dA((double)o.z, dM(bt, (double)d.z)));
+        face_id[q] = sx >= 0 ? (int64_t)ix : (int64_t)-1;
+    }
+}
+
+// ------------------------------------------------------ Morton bucketing
+// Points are counted into 2^(3b) cells of their own bounding box (computed
+// on the device) and scattered in Morton order of the cells.  Within a cell
+// the order is that of the atomics (irrelevant: results are per query).
+__device__ __forceinline__ uint32_t spread3(uint32_t v) {  // 10 bits -> every third bit
+    v &= 0x3FFu;
+    v = (v | (v << 16)) & 0x030000FFu;
+    v = (v | (v << 8)) & 0x0300F00Fu;
+    v = (v | (v << 4)) & 0x030C30C3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+// order-preserving float <-> uint32 map (for atomicMin / atomicMax)
+__device__ __forceinline__ uint32_t f2o(float f) {
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float o2f(uint32_t u) {
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u);
+}
+__global__ void k_box_init(uint32_t* box) {
+    if (threadIdx.x < 3) box[threadIdx.x] = 0xFFFFFFFFu;
+    else if (threadIdx.x < 6) box[threadIdx.x] = 0u;
+}
+__global__ void k_box(int64_t n, const float* __restrict__ pts, uint32_t* __restrict__ box) {
+    uint32_t lo[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, hi[3] = {0u, 0u, 0u};
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const float3 p = load3(pts, i);
+        const float c[3] = {p.x, p.y, p.z};
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            if (isfinite(c[k])) { lo[k] = min(lo[k], f2o(c[k])); hi[k] = max(hi[k], f2o(c[k])); }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = __reduce_min_sync(kFull, lo[k]);
+        hi[k] = __reduce_max_sync(kFull, hi[k]);
+    }
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { atomicMin(&box[k], lo[k]); atomicMax(&box[3 + k], hi[k]); }
+    }
+}
+__device__ __forceinline__ uint32_t cell_of(float3 p, const uint32_t* __restrict__ box, int bits) {
+    const float side = (float)(1 << bits), m = side - 1.f;
+    const float c[3] = {p.x, p.y, p.z};
+    uint32_t g[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float lo = o2f(box[k]), hi = o2f(box[3 + k]);
+        const float s = hi > lo ? side / (hi - lo) : 0.f;
+        const float v = (c[k] - lo) * s;
+        g[k] = (uint32_t)fminf(fmaxf(v == v ? v : 0.f, 0.f), m);
+    }
+    return spread3(g[0]) | (spread3(g[1]) << 1) | (spread3(g[2]) << 2);
+}
+__global__ void k_cell_hist(int64_t n, const float* __restrict__ pts, const uint32_t* __restrict__ box, int bits,
+                            uint32_t* __restrict__ hist) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        atomicAdd(&hist[cell_of(load3(pts, i), box, bits)], 1u);
+}
+__global__ void k_cell_scatter(int64_t n, const float* __restrict__ pts, const uint32_t* __restrict__ box, int bits,
+                               uint32_t* __restrict__ offs, uint32_t* __restrict__ order) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        order[atomicAdd(&offs[cell_of(load3(pts, i), box, bits)], 1u)] = (uint32_t)i;
 }
 
 // --------------------------------------------------------------- launchers
-static inline unsigned grid_for(int64_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+namespace {
+
+int sm_count() {
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    return nsm;
+}
+template <class K>
+unsigned persistent_grid(K kernel, int64_t n) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kQBlock, 0);
+    if (per_sm < 1) per_sm = 1;
+    const int64_t want = (n + kQBlock - 1) / kQBlock;
+    const int64_t cap = (int64_t)sm_count() * per_sm;
+    return (unsigned)(want < cap ? (want > 0 ? want : 1) : cap);
+}
+
+int cell_bits(int64_t n) {
+    int b = 4;
+    while (b < 8 && ((int64_t)1 << (3 * (b + 1))) <= 2 * n) ++b;
+    return b;
+}
+
+}  // namespace
+
+size_t query_workspace_bytes(int mode, int64_t n) {
+    if (n < kSortMinQueries && mode == 0) return 0;
+    size_t b = 0;
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    if (n >= kSortMinQueries) {
+        const int64_t cells = (int64_t)1 << (3 * cell_bits(n));
+        b += al(sizeof(uint32_t) * n);                            // order
+        b += al(sizeof(uint32_t) * (cells + 1));                  // cell counts / offsets
+        b += al(sizeof(uint32_t) * (scan::num_chunks(cells) + 1));
+        b += al(sizeof(uint32_t) * 8);                            // query box
+    }
+    if (mode != 0) b += al(sizeof(int32_t) * n);                  // winning slots
+    return b;
+}
 
 cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts, float* dist, int64_t* fid,
-                            float* uvw, const CNode* nodes, const CTri* tris, int slot_face0,
+                            float* uvw, const CNode* nodes, const CTri* tris, int slot_face0, void* ws,
                             cudaStream_t stream) {
     if (n <= 0) return cudaSuccess;
-    const dim3 grid(grid_for(n, 128)), block(128);
-#define CUBVH_L(M, U) k_distance<M, U><<<grid, block, 0, stream>>>(n, pts, dist, fid, uvw, nodes, tris, slot_face0)
-    if (mode == 0) { if (want_uvw) CUBVH_L(0, true); else CUBVH_L(0, false); }
-    else if (mode == 1) { if (want_uvw) CUBVH_L(1, true); else CUBVH_L(1, false); }
-    else { if (want_uvw) CUBVH_L(2, true); else CUBVH_L(2, false); }
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    char* w = static_cast<char*>(ws);
+    uint32_t* order = nullptr;
+    if (n >= kSortMinQueries) {
+        const int bits = cell_bits(n);
+        const int64_t cells = (int64_t)1 << (3 * bits);
+        order = reinterpret_cast<uint32_t*>(w); w += al(sizeof(uint32_t) * n);
+        uint32_t* hist = reinterpret_cast<uint32_t*>(w); w += al(sizeof(uint32_t) * (cells + 1));
+        uint32_t* bsum = reinterpret_cast<uint32_t*>(w); w += al(sizeof(uint32_t) * (scan::num_chunks(cells) + 1));
+        uint32_t* box = reinterpret_cast<uint32_t*>(w); w += al(sizeof(uint32_t) * 8);
+        cudaError_t e = cudaMemsetAsync(hist, 0, sizeof(uint32_t) * (cells + 1), stream);
+        if (e != cudaSuccess) return e;
+        const unsigned g = (unsigned)sm_count() * 8;
+        k_box_init<<<1, 32, 0, stream>>>(box);
+        k_box<<<g, 256, 0, stream>>>(n, pts, box);
+        k_cell_hist<<<g, 256, 0, stream>>>(n, pts, box, bits, hist);
+        scan::exclusive(hist, bsum, cells, stream);
+        k_cell_scatter<<<g, 256, 0, stream>>>(n, pts, box, bits, hist, order);
+    }
+    int32_t* slots = mode != 0 ? reinterpret_cast<int32_t*>(w) : nullptr;
+#define CUBVH_L(U, S) k_udf<U, S><<<persistent_grid(k_udf<U, S>, n), kQBlock, 0, stream>>>( \
+        n, order, pts, dist, fid, uvw, slots, nodes, tris, slot_face0)
+    if (mode == 0) { if (want_uvw) CUBVH_L(true, false); else CUBVH_L(false, false); }
+    else { if (want_uvw) CUBVH_L(true, true); else CUBVH_L(false, true); }
 #undef CUBVH_L
+    if (mode == 1) {
+        k_sign_watertight<<<(unsigned)((n + kQBlock - 1) / kQBlock), kQBlock, 0, stream>>>(n, order, pts, dist, slots,
+                                                                                           nodes, tris);
+    } else if (mode == 2) {
+        k_sign_raystab<<<(unsigned)((n + kQBlock - 1) / kQBlock), kQBlock, 0, stream>>>(n, order, pts, dist, nodes, tris);
+    }
     return cudaGetLastError();
 }
 
 cudaError_t launch_ray(int64_t n, const float* ro, const float* rd, float* pos, int64_t* fid, float* depth,
                        const CNode* nodes, const CTri* tris, cudaStream_t stream) {
     if (n <= 0) return cudaSuccess;
-    k_ray<<<grid_for(n, 128), 128, 0, stream>>>(n, ro, rd, pos, fid, depth, nodes, tris);
+    k_ray<<<persistent_grid(k_ray, n), kQBlock, 0, stream>>>(n, ro, rd, pos, fid, depth, nodes, tris);
     return cudaGetLastError();
 }
 
