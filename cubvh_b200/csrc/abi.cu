@@ -242,7 +242,7 @@ int cubvh_signed_distance(cubvh_bvh* h, const float* points, int64_t n, uint32_t
     const size_t wsb = query_workspace_bytes(kmode, n);
     void* ws = nullptr;
     cudaError_t e;
-    if (wsb && (e = cudaMallocAsync(&ws, wsb, s)) != cudaSuccess) return cuda_fail(e, "cudaMallocAsync(query workspace)");
+    if ((e = cudaMallocAsync(&ws, wsb, s)) != cudaSuccess) return cuda_fail(e, "cudaMallocAsync(query workspace)");
     e = launch_distance(kmode, uvw != nullptr, n, points, distances, face_id, uvw, d->nodes, d->tris,
                         (int)h->host.slot_of_face0, ws, s);
     if (ws) {
@@ -265,8 +265,13 @@ int cubvh_ray_trace(cubvh_bvh* h, const float* rays_o, const float* rays_d, int6
     DevCopy* d;
     const int rc = device_copy(h, &d);
     if (rc != CUBVH_OK) return rc;
-    const cudaError_t e = launch_ray(n, rays_o, rays_d, positions, face_id, depth, d->nodes, d->tris,
-                                     (cudaStream_t)stream);
+    cudaStream_t s = (cudaStream_t)stream;
+    void* ws = nullptr;
+    cudaError_t e = cudaMallocAsync(&ws, query_workspace_bytes(-1, n), s);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync(ray workspace)");
+    e = launch_ray(n, rays_o, rays_d, positions, face_id, depth, d->nodes, d->tris, ws, s);
+    const cudaError_t e2 = cudaFreeAsync(ws, s);
+    if (e == cudaSuccess) e = e2;
     if (e != cudaSuccess) return cuda_fail(e, "ray kernel launch");
     return CUBVH_OK;
     CUBVH_GUARD_END

@@ -13,7 +13,8 @@ cudaError_t upload_constants();
 // Point queries at least this many are visited in Morton-cell order.
 constexpr int64_t kSortMinQueries = 2048;
 
-// Device scratch bytes launch_distance needs for n queries (0: none).
+// Device scratch bytes of a query launch: launch_distance (mode 0..2) or
+// launch_ray (mode -1) for n queries.
 size_t query_workspace_bytes(int mode, int64_t n);
 // mode 0 unsigned, 1 watertight sign, 2 raystab sign.  ws:
 // query_workspace_bytes(mode, n) bytes, 256-byte aligned.
@@ -21,7 +22,7 @@ cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts
                             float* uvw, const CNode* nodes, const CTri* tris, int slot_face0, void* ws,
                             cudaStream_t stream);
 cudaError_t launch_ray(int64_t n, const float* ro, const float* rd, float* pos, int64_t* fid, float* depth,
-                       const CNode* nodes, const CTri* tris, cudaStream_t stream);
+                       const CNode* nodes, const CTri* tris, void* ws, cudaStream_t stream);
 
 // floodfill (floodfill.cu)
 size_t floodfill_workspace_bytes(int B, int H, int W, int D);

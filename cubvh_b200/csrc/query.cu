@@ -116,6 +116,29 @@ __device__ __forceinline__ void leaf_range(int ref, int& s0, int& s1) {
     s0 = code >> 2; s1 = s0 + (code & 3) + 1;
 }
 
+
+// Dynamic packet queue: a warp takes `grab` consecutive 32-query packets per
+// atomicAdd on a per-launch counter (zeroed before the launch), so warps that
+// drew cheap packets keep taking more and no SM idles while work remains.
+struct PacketQueue {
+    unsigned long long* ctr;
+    int64_t n, grab, next, end;
+    __device__ __forceinline__ PacketQueue(unsigned long long* c, int64_t n_, int64_t g)
+        : ctr(c), n(n_), grab(g), next(0), end(0) {}
+    // base query index of the warp's next packet, or -1 when done
+    __device__ __forceinline__ int64_t take() {
+        if (next == end) {
+            unsigned long long b = 0;
+            if ((threadIdx.x & 31) == 0) b = atomicAdd(ctr, (unsigned long long)grab);
+            next = (int64_t)__shfl_sync(kFull, b, 0);
+            end = next + grab;
+        }
+        const int64_t base = next * 32;
+        ++next;
+        return base < n ? base : -1;
+    }
+};
+
 __device__ __forceinline__ float3 load3(const float* __restrict__ a, int64_t i) {
     return make_float3(a[3 * i], a[3 * i + 1], a[3 * i + 2]);
 }
@@ -168,11 +191,11 @@ __global__ void __launch_bounds__(kQBlock) k_udf(int64_t n, const uint32_t* __re
                                                  const float* __restrict__ pts, float* __restrict__ dist,
                                                  int64_t* __restrict__ face_id, float* __restrict__ uvw,
                                                  int32_t* __restrict__ slot_out, const CNode* __restrict__ nodes,
-                                                 const CTri* __restrict__ tris, int slot_face0) {
+                                                 const CTri* __restrict__ tris, int slot_face0,
+                                                 unsigned long long* __restrict__ ctr, int64_t grab) {
     const int lane = threadIdx.x & 31;
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t base = warp * 32; base < n; base += nwarps * 32) {
+    PacketQueue pq(ctr, n, grab);
+    for (int64_t base = pq.take(); base >= 0; base = pq.take()) {
         const int64_t qi = base + lane;
         const bool act = qi < n;
         const int64_t idx = act ? (order ? (int64_t)order[qi] : qi) : 0;
@@ -321,9 +344,12 @@ __global__ void __launch_bounds__(kQBlock) k_sign_watertight(int64_t n, const ui
                                                              float* __restrict__ dist,
                                                              const int32_t* __restrict__ slots,
                                                              const CNode* __restrict__ nodes,
-                                                             const CTri* __restrict__ tris) {
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) {
+                                                             const CTri* __restrict__ tris,
+                                                             unsigned long long* __restrict__ ctr, int64_t grab) {
+    PacketQueue pq(ctr, n, grab);
+    for (int64_t base = pq.take(); base >= 0; base = pq.take()) {
+        const int64_t q = base + (threadIdx.x & 31);
+        if (q >= n) continue;
         const int64_t idx = order ? (int64_t)order[q] : q;
         const d3 pd = to_d3(load3(pts, idx));
         const TriV t = load_tri(tris, slots[idx]);
@@ -386,9 +412,12 @@ __device__ bool any_hit(const CNode* __restrict__ nodes, const CTri* __restrict_
 __global__ void __launch_bounds__(kQBlock) k_sign_raystab(int64_t n, const uint32_t* __restrict__ order,
                                                           const float* __restrict__ pts, float* __restrict__ dist,
                                                           const CNode* __restrict__ nodes,
-                                                          const CTri* __restrict__ tris) {
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) {
+                                                          const CTri* __restrict__ tris,
+                                                          unsigned long long* __restrict__ ctr, int64_t grab) {
+    PacketQueue pq(ctr, n, grab);
+    for (int64_t base = pq.take(); base >= 0; base = pq.take()) {
+        const int64_t q = base + (threadIdx.x & 31);
+        if (q >= n) continue;
         const int64_t idx = order ? (int64_t)order[q] : q;
         const float3 p = load3(pts, idx);
         const float2 off = stab_offset((uint32_t)idx);
@@ -414,11 +443,11 @@ __global__ void __launch_bounds__(kQBlock) k_sign_raystab(int64_t n, const uint3
 __global__ void __launch_bounds__(kQBlock) k_ray(int64_t n, const float* __restrict__ ro,
                                                  const float* __restrict__ rd, float* __restrict__ pos,
                                                  int64_t* __restrict__ face_id, float* __restrict__ depth,
-                                                 const CNode* __restrict__ nodes, const CTri* __restrict__ tris) {
+                                                 const CNode* __restrict__ nodes, const CTri* __restrict__ tris,
+                                                 unsigned long long* __restrict__ ctr, int64_t grab) {
     const int lane = threadIdx.x & 31;
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t base = warp * 32; base < n; base += nwarps * 32) {
+    PacketQueue pq(ctr, n, grab);
+    for (int64_t base = pq.take(); base >= 0; base = pq.take()) {
         const int64_t q = base + lane;
         const bool act = q < n;
         const float3 o = act ? load3(ro, q) : make_float3(0.f, 0.f, 0.f);
@@ -604,19 +633,28 @@ int cell_bits(int64_t n) {
 }  // namespace
 
 size_t query_workspace_bytes(int mode, int64_t n) {
-    if (n < kSortMinQueries && mode == 0) return 0;
-    size_t b = 0;
+    size_t b = 256;                                               // packet counters
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
-    if (n >= kSortMinQueries) {
+    if (mode >= 0 && n >= kSortMinQueries) {
         const int64_t cells = (int64_t)1 << (3 * cell_bits(n));
         b += al(sizeof(uint32_t) * n);                            // order
         b += al(sizeof(uint32_t) * (cells + 1));                  // cell counts / offsets
         b += al(sizeof(uint32_t) * (scan::num_chunks(cells) + 1));
         b += al(sizeof(uint32_t) * 8);                            // query box
     }
-    if (mode != 0) b += al(sizeof(int32_t) * n);                  // winning slots
+    if (mode > 0) b += al(sizeof(int32_t) * n);                   // winning slots
     return b;
 }
+
+namespace {
+// packets per atomic grab: about 64 grabs per warp of the launch
+int64_t grab_for(int64_t n, unsigned grid) {
+    const int64_t packets = (n + 31) / 32;
+    const int64_t warps = (int64_t)grid * (kQBlock / 32);
+    const int64_t g = packets / (warps * 64);
+    return g < 1 ? 1 : g;
+}
+}  // namespace
 
 cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts, float* dist, int64_t* fid,
                             float* uvw, const CNode* nodes, const CTri* tris, int slot_face0, void* ws,
@@ -624,6 +662,9 @@ cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts
     if (n <= 0) return cudaSuccess;
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     char* w = static_cast<char*>(ws);
+    unsigned long long* ctr = reinterpret_cast<unsigned long long*>(w); w += 256;
+    cudaError_t e = cudaMemsetAsync(ctr, 0, 256, stream);
+    if (e != cudaSuccess) return e;
     uint32_t* order = nullptr;
     if (n >= kSortMinQueries) {
         const int bits = cell_bits(n);
@@ -632,8 +673,7 @@ cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts
         uint32_t* hist = reinterpret_cast<uint32_t*>(w); w += al(sizeof(uint32_t) * (cells + 1));
         uint32_t* bsum = reinterpret_cast<uint32_t*>(w); w += al(sizeof(uint32_t) * (scan::num_chunks(cells) + 1));
         uint32_t* box = reinterpret_cast<uint32_t*>(w); w += al(sizeof(uint32_t) * 8);
-        cudaError_t e = cudaMemsetAsync(hist, 0, sizeof(uint32_t) * (cells + 1), stream);
-        if (e != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(hist, 0, sizeof(uint32_t) * (cells + 1), stream)) != cudaSuccess) return e;
         const unsigned g = (unsigned)sm_count() * 8;
         k_box_init<<<1, 32, 0, stream>>>(box);
         k_box<<<g, 256, 0, stream>>>(n, pts, box);
@@ -642,24 +682,30 @@ cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts
         k_cell_scatter<<<g, 256, 0, stream>>>(n, pts, box, bits, hist, order);
     }
     int32_t* slots = mode != 0 ? reinterpret_cast<int32_t*>(w) : nullptr;
-#define CUBVH_L(U, S) k_udf<U, S><<<persistent_grid(k_udf<U, S>, n), kQBlock, 0, stream>>>( \
-        n, order, pts, dist, fid, uvw, slots, nodes, tris, slot_face0)
+#define CUBVH_L(U, S) do { const unsigned g_ = persistent_grid(k_udf<U, S>, n); \
+        k_udf<U, S><<<g_, kQBlock, 0, stream>>>(n, order, pts, dist, fid, uvw, slots, nodes, tris, slot_face0, \
+                                                ctr, grab_for(n, g_)); } while (0)
     if (mode == 0) { if (want_uvw) CUBVH_L(true, false); else CUBVH_L(false, false); }
     else { if (want_uvw) CUBVH_L(true, true); else CUBVH_L(false, true); }
 #undef CUBVH_L
     if (mode == 1) {
-        k_sign_watertight<<<(unsigned)((n + kQBlock - 1) / kQBlock), kQBlock, 0, stream>>>(n, order, pts, dist, slots,
-                                                                                           nodes, tris);
+        const unsigned g = persistent_grid(k_sign_watertight, n);
+        k_sign_watertight<<<g, kQBlock, 0, stream>>>(n, order, pts, dist, slots, nodes, tris, ctr + 1, grab_for(n, g));
     } else if (mode == 2) {
-        k_sign_raystab<<<(unsigned)((n + kQBlock - 1) / kQBlock), kQBlock, 0, stream>>>(n, order, pts, dist, nodes, tris);
+        const unsigned g = persistent_grid(k_sign_raystab, n);
+        k_sign_raystab<<<g, kQBlock, 0, stream>>>(n, order, pts, dist, nodes, tris, ctr + 1, grab_for(n, g));
     }
     return cudaGetLastError();
 }
 
 cudaError_t launch_ray(int64_t n, const float* ro, const float* rd, float* pos, int64_t* fid, float* depth,
-                       const CNode* nodes, const CTri* tris, cudaStream_t stream) {
+                       const CNode* nodes, const CTri* tris, void* ws, cudaStream_t stream) {
     if (n <= 0) return cudaSuccess;
-    k_ray<<<persistent_grid(k_ray, n), kQBlock, 0, stream>>>(n, ro, rd, pos, fid, depth, nodes, tris);
+    unsigned long long* ctr = reinterpret_cast<unsigned long long*>(ws);
+    cudaError_t e = cudaMemsetAsync(ctr, 0, 256, stream);
+    if (e != cudaSuccess) return e;
+    const unsigned g = persistent_grid(k_ray, n);
+    k_ray<<<g, kQBlock, 0, stream>>>(n, ro, rd, pos, fid, depth, nodes, tris, ctr, grab_for(n, g));
     return cudaGetLastError();
 }
 
