@@ -334,4 +334,18 @@ int cubvh_floodfill_check(const void* workspace, int B, int H, int W, int D, voi
     CUBVH_GUARD_END
 }
 
+// Floodfill that allocates nothing: see include/cubvh_b200.h.
+int cubvh_floodfill_noalloc(const uint8_t* grid, int B, int H, int W, int D, int32_t* labels, void* stream) {
+    CUBVH_GUARD_BEGIN
+    const int rc = check_grid_dims(B, H, W, D);
+    if (rc != CUBVH_OK) return rc;
+    if ((int64_t)B * H * W * D == 0) return CUBVH_OK;
+    if (!grid || !labels) return fail(CUBVH_ERR_INVALID, "grid/labels is null");
+    std::string err;
+    const int st = floodfill_noalloc(grid, B, H, W, D, labels, (cudaStream_t)stream, err);
+    if (st != CUBVH_OK) return fail(st, err);
+    return CUBVH_OK;
+    CUBVH_GUARD_END
+}
+
 }  // extern "C"

@@ -2,6 +2,7 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <string>
 #include <cuda_runtime.h>
 
 #include "layout.h"
@@ -30,5 +31,8 @@ cudaError_t launch_floodfill(const uint8_t* grid, int B, int H, int W, int D, in
                              void* workspace, cudaStream_t stream);
 // Offset of the int32 status word inside the floodfill workspace.
 size_t floodfill_status_offset(int B, int H, int W, int D);
+// Floodfill with the library's fixed scratch array (floodfill_noalloc.cu).
+int floodfill_noalloc(const uint8_t* grid, int B, int H, int W, int D, int32_t* labels, cudaStream_t stream,
+                      std::string& err);
 
 }  // namespace cubvh

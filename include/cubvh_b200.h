@@ -122,6 +122,23 @@ int cubvh_floodfill(const uint8_t* grid, int B, int H, int W, int D, int32_t* la
  * that last used `workspace` (same B, H, W, D) hit a device-side bound. */
 int cubvh_floodfill_check(const void* workspace, int B, int H, int W, int D, void* stream);
 
+/* Floodfill for callers that must not allocate GPU memory during the call
+ * (code running inside another framework's memory pool or arena that forbids
+ * cudaMalloc / cudaFree, or loops that must never touch the allocator).  No
+ * counterpart in the reference.  Same arguments and results as
+ * cubvh_floodfill, but the scratch is a 32 MiB array compiled into the
+ * library, so no workspace is passed and nothing is allocated: grids whose
+ * scratch (cubvh_floodfill_workspace_size) exceeds 32 MiB, about 192^3
+ * voxels, are rejected with CUBVH_ERR_INVALID.  Every GPU that loads this
+ * part of the library keeps the 32 MiB until the process exits.  The first
+ * call on each device looks up the array's device address (with that device
+ * current); make that first call before any stream capture.  All calls share
+ * the one array: calls that overlap on the GPU (different streams, or
+ * different host threads without ordering) race and corrupt each other's
+ * results, so order them.  The call clears everything it reads, so no state
+ * carries over between calls. */
+int cubvh_floodfill_noalloc(const uint8_t* grid, int B, int H, int W, int D, int32_t* labels, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
