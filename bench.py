@@ -51,6 +51,18 @@ def _rank_info():
     return rank, world, local
 
 
+def max_over_ranks(x: float, device=None) -> float:
+    """Maximum of x over all ranks of the default process group (x itself
+    when no group is initialised)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def _peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
@@ -334,10 +346,7 @@ def run_ours(args):
     ms = t0.elapsed_time(t1)
     per_op_ms = [sum(kev[s][i][0].elapsed_time(kev[s][i][1]) for s in range(args.steps)) / args.steps
                  for i in range(len(dev_ops))]
-    if world > 1:
-        tt = torch.tensor([ms], device=dev)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = max_over_ranks(ms, dev)
     value = world * q_per_step * args.steps / (ms / 1e3)
 
     # ---- e2e through the public API from pinned host buffers
@@ -382,10 +391,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     e2e_ms = (time.perf_counter() - w0) * 1e3
     barrier()
-    if world > 1:
-        tt = torch.tensor([e2e_ms], device=dev)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
+    e2e_ms = max_over_ranks(e2e_ms, dev)
     e2e_val = world * q_per_step * e2e_steps / (e2e_ms / 1e3)
 
     line = None

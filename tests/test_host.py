@@ -1,0 +1,205 @@
+"""Host-side checks that need no GPU: the C ABI exports, the BVH layout
+invariants (every quantised box contains what it bounds), the reference-format
+state_dict, the Python surface's error behaviour, and the multi-rank timing
+reduction (gloo, two processes)."""
+
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+import torch
+
+import cubvh_b200 as cubvh
+from cubvh_b200 import _lib
+from cubvh_b200 import workloads as W
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+NODE = np.dtype([('o', '<f4', 3), ('e', 'i1', 3), ('nint', 'u1'), ('cb', '<i4'), ('tb', '<i4'), ('meta', 'u1', 8),
+                 ('qlx', 'u1', 8), ('qly', 'u1', 8), ('qlz', 'u1', 8), ('qhx', 'u1', 8), ('qhy', 'u1', 8),
+                 ('qhz', 'u1', 8)])
+TRI = np.dtype([('a', '<f4', 3), ('id', '<i4'), ('b', '<f4', 3), ('e2', '<f4'), ('c', '<f4', 3), ('einf', '<f4')])
+REFNODE = np.dtype([('lo', '<f4', 3), ('hi', '<f4', 3), ('left', '<i4'), ('right', '<i4'), ('escape', '<i4')])
+
+
+def header_functions():
+    src = open(os.path.join(ROOT, "include", "cubvh_b200.h")).read()
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\*?\s+\*?(cubvh_\w+)\(", src, re.M)))
+
+
+def test_library_exports_every_header_function():
+    L = _lib.lib()
+    names = header_functions()
+    assert len(names) >= 15
+    for n in names:
+        assert hasattr(L, n), f"{n} declared in include/cubvh_b200.h but not exported"
+    assert _lib.version().startswith("cubvh_b200")
+
+
+def layout(bvh):
+    nf, nn, depth = bvh._info()
+    nodes = np.zeros(nn, NODE)
+    tris = np.zeros(nf, TRI)
+    assert _lib.lib().cubvh_bvh_layout(bvh.impl.raw, nodes.ctypes.data, tris.ctypes.data) == 0
+    return nodes, tris, depth
+
+
+def decode(n):
+    s = np.ldexp(np.float32(1), n['e'].astype(np.int32)).astype(np.float32)
+    lo = np.stack([n['o'][k] + n[f'ql{a}'].astype(np.float32) * s[k] for k, a in enumerate('xyz')], 1)
+    hi = np.stack([n['o'][k] + n[f'qh{a}'].astype(np.float32) * s[k] for k, a in enumerate('xyz')], 1)
+    return lo.astype(np.float32), hi.astype(np.float32)
+
+
+@pytest.mark.parametrize("mesh", ["ico3", "tori", "dodeca"])
+def test_bvh_layout_invariants(mesh):
+    if mesh == "ico3":
+        v, f = W.displaced_icosphere(3, 1)
+    elif mesh == "tori":
+        v, f = W.random_tori(2, n_tori=3, n_major=40, n_minor=10)
+    else:
+        v, f = W.dodecahedron()
+    nodes, tris, depth = layout(cubvh.cuBVH(v, f))
+    assert depth <= 13
+    # the soup holds every face exactly once, with its own vertices
+    assert np.array_equal(np.sort(tris['id']), np.arange(len(f)))
+    tv = v[f[tris['id']]]
+    assert np.array_equal(tris['a'], tv[:, 0]) and np.array_equal(tris['b'], tv[:, 1])
+    assert np.array_equal(tris['c'], tv[:, 2])
+    tlo = np.minimum(np.minimum(tris['a'], tris['b']), tris['c'])
+    thi = np.maximum(np.maximum(tris['a'], tris['b']), tris['c'])
+
+    def subtree_box(i):
+        n = nodes[i]
+        lo, hi = decode(n)
+        blo, bhi = np.full(3, np.inf, np.float32), np.full(3, -np.inf, np.float32)
+        for j in range(8):
+            m = n['meta'][j]
+            if m == 0xFF:
+                continue
+            if m & 0x80:
+                clo, chi = subtree_box(n['cb'] + (m & 7))
+            else:
+                s0 = n['tb'] + (m & 31)
+                s1 = s0 + ((m >> 5) & 3) + 1
+                clo, chi = tlo[s0:s1].min(0), thi[s0:s1].max(0)
+            assert (lo[j] <= clo).all() and (hi[j] >= chi).all(), "quantised child box does not contain its content"
+            blo, bhi = np.minimum(blo, clo), np.maximum(bhi, chi)
+        return blo, bhi
+
+    lo, hi = subtree_box(0)
+    assert np.array_equal(lo, tlo.min(0)) and np.array_equal(hi, thi.max(0))
+
+
+def test_state_dict_reference_format():
+    v, f = W.displaced_icosphere(3, 1)
+    bvh = cubvh.cuBVH(v, f)
+    sd = bvh.state_dict()
+    nodes, tris = sd["nodes"], sd["triangles"]
+    assert nodes.dtype == torch.int32 and nodes.shape[1] == 9
+    assert tris.dtype == torch.int32 and tris.shape == (len(f), 12)
+    N = nodes.numpy().view(REFNODE).reshape(-1)
+    T = tris.numpy()
+    xyz = T[:, :9].copy().view(np.float32).reshape(-1, 3, 3)
+    ids = T[:, 10:12].copy().view(np.int64).reshape(-1)
+    assert np.array_equal(np.sort(ids), np.arange(len(f)))
+    assert np.array_equal(xyz, v[f[ids]])
+    covered = np.zeros(len(f), int)
+    order = []
+
+    def walk(i, esc):
+        order.append(i)
+        n = N[i]
+        assert n['escape'] == esc
+        if n['left'] < 0:
+            s0, s1 = -n['left'] - 1, -n['right'] - 1
+            assert 0 < s1 - s0 <= 8 or len(f) <= 8
+            covered[s0:s1] += 1
+            box = xyz[s0:s1].reshape(-1, 3)
+            assert (n['lo'] <= box.min(0)).all() and (n['hi'] >= box.max(0)).all()
+            return
+        assert n['right'] == n['left'] + 4          # exactly four children
+        for c in range(n['left'], n['right']):
+            walk(c, c + 1 if c + 1 < n['right'] else esc)
+
+    walk(0, -1)
+    assert (covered == 1).all() and len(order) == len(N)
+    # deterministic: the reloaded BVH exports the same records
+    sd2 = cubvh.cuBVH.from_state_dict(sd).state_dict()
+    assert torch.equal(sd2["nodes"], nodes) and torch.equal(sd2["triangles"], tris)
+
+
+def test_from_state_dict_ids_survive():
+    v, f = W.icosphere(1)
+    sd = cubvh.cuBVH(v, f).state_dict()
+    _, tris, _ = layout(cubvh.cuBVH.from_state_dict(sd))
+    assert np.array_equal(np.sort(tris['id']), np.arange(len(f)))
+
+
+def test_errors_match_reference_surface():
+    v, f = W.icosphere(0)
+    with pytest.raises(AssertionError):
+        cubvh.cuBVH(v, f[:8])                      # at least 9 faces
+    bad = f.copy()
+    bad[3, 1] = len(v)
+    with pytest.raises(RuntimeError, match="vertex index"):
+        cubvh.cuBVH(v, bad)
+    vn = v.copy()
+    vn[2, 0] = np.nan
+    with pytest.raises(RuntimeError, match="finite"):
+        cubvh.cuBVH(vn, f)
+    with pytest.raises(RuntimeError):
+        cubvh.cuBVH(v[:, :2], f)
+    with pytest.raises(RuntimeError, match="triangles"):
+        cubvh.cuBVH.from_state_dict({"nodes": torch.zeros(1, 9, dtype=torch.int32)})
+    with pytest.raises(RuntimeError, match="nodes"):
+        cubvh.cuBVH.from_state_dict({"triangles": torch.zeros(9, 12, dtype=torch.int32)})
+    # torch inputs are detached and moved to the host, like the reference
+    b = cubvh.cuBVH(torch.from_numpy(v).requires_grad_(), torch.from_numpy(f))
+    assert b.num_faces == len(f)
+
+
+def test_c_abi_argument_checks():
+    L = _lib.lib()
+    out = ctypes.c_void_p()
+    assert L.cubvh_bvh_create(None, 3, None, 1, ctypes.byref(out)) == 1
+    assert b"null" in L.cubvh_last_error()
+    nb = ctypes.c_size_t()
+    assert L.cubvh_floodfill_workspace_size(1, 2048, 2048, 1024, ctypes.byref(nb)) == 1
+    assert L.cubvh_floodfill_workspace_size(1, 64, 64, 64, ctypes.byref(nb)) == 0
+    small = nb.value
+    assert L.cubvh_floodfill_workspace_size(2, 64, 64, 64, ctypes.byref(nb)) == 0 and nb.value > small
+    v, f = W.icosphere(1)
+    bvh = cubvh.cuBVH(v, f)
+    assert L.cubvh_signed_distance(bvh.impl.raw, None, 5, 7, None, None, None, None) == 1
+    assert b"mode" in L.cubvh_last_error()
+    assert L.cubvh_unsigned_distance(bvh.impl.raw, None, 0, None, None, None, None) == 0   # empty: no-op
+
+
+def _rank_main(rank, world, port, q):
+    import torch.distributed as dist
+    import bench
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    got = bench.max_over_ranks(10.0 + rank * 5.0)
+    q.put((rank, got))
+    dist.destroy_process_group()
+
+
+def test_max_over_ranks_gloo_world2():
+    import socket
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+    assert res == {0: 15.0, 1: 15.0}
