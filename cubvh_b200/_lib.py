@@ -38,6 +38,8 @@ _SIGS = {
     "cubvh_floodfill_workspace_size": [c_int, c_int, c_int, c_int, ctypes.POINTER(c_sz)],
     "cubvh_floodfill": [c_vp, c_int, c_int, c_int, c_int, c_vp, c_vp, c_sz, c_vp],
     "cubvh_floodfill_check": [c_vp, c_int, c_int, c_int, c_int, c_vp],
+    "cubvh_bvh_refit": [c_vp, c_vp, c_i64, c_vp],
+    "cubvh_distance_backward": [c_vp, c_vp, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp],
 }
 _STR_FUNCS = ("cubvh_version", "cubvh_last_error")
 

@@ -1,4 +1,4 @@
-"""Drop-in query API of cubvh (reference: cubvh/api.py:1-140).
+"""Drop-in query API of cubvh (reference: cubvh/api.py:1-140), plus gradients.
 
 ``cuBVH(vertices, triangles)`` builds the BVH on the host (no GPU work; the
 first query on a device uploads it), ``ray_trace`` / ``unsigned_distance`` /
@@ -7,6 +7,12 @@ shapes and dtypes, ``state_dict`` / ``from_state_dict`` use the reference's
 record format, and ``floodfill`` labels free-voxel components.  Queries run
 on the current CUDA stream of the input's device and are asynchronous, like
 the reference's.
+
+Additions (no counterpart in the reference): ``cuBVH.refit(vertices)`` moves
+the mesh's vertices on the GPU (same faces), and the distance queries are
+differentiable: pass ``vertices=`` (a CUDA tensor, optionally requiring grad)
+or a ``positions`` tensor that requires grad, and the returned distances
+carry gradients to both through a hand-written backward kernel.
 """
 
 from __future__ import annotations
@@ -63,6 +69,35 @@ def _mesh_arrays(vertices, triangles):
     return V, F
 
 
+class _DistanceFn(torch.autograd.Function):
+    """Distances with gradients w.r.t. the query points and the vertices."""
+
+    @staticmethod
+    def forward(ctx, positions, vertices, bvh, mode, return_uvw):
+        d, fid, uvw = bvh._distance(positions, return_uvw, mode)
+        ctx.bvh = bvh
+        ctx.save_for_backward(positions, fid, d, vertices)
+        ctx.mark_non_differentiable(fid)
+        if uvw is not None:
+            ctx.mark_non_differentiable(uvw)
+        return d, fid, uvw
+
+    @staticmethod
+    def backward(ctx, gd, _gfid, _guvw):
+        positions, fid, d, vertices = ctx.saved_tensors
+        n = positions.shape[0]
+        gp = torch.empty_like(positions) if ctx.needs_input_grad[0] else None
+        gv = torch.zeros_like(vertices) if (vertices is not None and ctx.needs_input_grad[1]) else None
+        if gd is None or n == 0:
+            return gp, gv, None, None, None
+        gd = gd.contiguous().float()
+        with torch.cuda.device(positions.device):
+            check(lib().cubvh_distance_backward(
+                ctx.bvh.impl.raw, _ptr(positions), n, _ptr(fid), _ptr(gd), _ptr(d), _ptr(vertices), _ptr(gp),
+                _ptr(gv), _stream_ptr(positions.device)), "backward")
+        return gp, gv, None, None, None
+
+
 class cuBVH:
     def __init__(self, vertices, triangles):
         # vertices: np.ndarray / torch.Tensor [N, 3]; triangles: [M, 3]
@@ -115,6 +150,23 @@ class cuBVH:
         obj.impl = _Handle(raw)
         return obj
 
+    # ---------------------------------------------------------------- refit
+    def refit(self, vertices):
+        """Move the mesh's vertices (CUDA float tensor [V, 3], same count and
+        faces as at construction) and refit the BVH on that device."""
+        v = vertices.detach()
+        if not v.is_cuda:
+            v = v.cuda()
+        v = v.float().contiguous()
+        key = (v.data_ptr(), v._version, tuple(v.shape), v.device)
+        # the held reference keeps the storage alive, so (pointer, version)
+        # identifies these exact vertex values
+        if getattr(self, "_refit_key", None) == key:
+            return
+        with torch.cuda.device(v.device):
+            check(lib().cubvh_bvh_refit(self.impl.raw, _ptr(v), v.shape[0], _stream_ptr(v.device)), "refit")
+        self._refit_key, self._refit_tensor = key, v
+
     # -------------------------------------------------------------- queries
     def ray_trace(self, rays_o, rays_d):
         # rays_o, rays_d: torch.Tensor, float, [N, 3]
@@ -138,12 +190,30 @@ class cuBVH:
 
         return positions.view(*prefix, 3), face_id.view(*prefix), depth.view(*prefix)
 
-    def _distance(self, positions, return_uvw, mode):
-        positions = positions.float().contiguous()
+    def _query(self, positions, return_uvw, mode, vertices):
+        positions = positions.float()
         if not positions.is_cuda: positions = positions.cuda()
-
         prefix = positions.shape[:-1]
-        positions = positions.view(-1, 3)
+        positions = positions.reshape(-1, 3).contiguous()
+        if vertices is not None:
+            v = vertices if vertices.is_cuda else vertices.cuda()
+            v = v.float().contiguous()
+            self.refit(v)
+        else:
+            v = None
+        grad = torch.is_grad_enabled() and (positions.requires_grad or (v is not None and v.requires_grad))
+        if grad:
+            d, fid, uvw = _DistanceFn.apply(positions, v, self, mode, return_uvw)
+        else:
+            d, fid, uvw = self._distance(positions.detach(), return_uvw, mode)
+        d = d.view(*prefix)
+        fid = fid.view(*prefix)
+        if uvw is not None:
+            uvw = uvw.view(*prefix, 3)
+        return d, fid, uvw
+
+    def _distance(self, positions, return_uvw, mode):
+        # positions: contiguous float32 CUDA [N, 3]; mode None = unsigned
         N = positions.shape[0]
 
         distances = torch.empty(N, dtype=torch.float32, device=positions.device)
@@ -159,20 +229,16 @@ class cuBVH:
                 rc = lib().cubvh_signed_distance(self.impl.raw, _ptr(positions), N, mode, _ptr(distances),
                                                  _ptr(face_id), _ptr(uvw), stream)
             check(rc, "signed_distance" if mode is not None else "unsigned_distance")
-
-        distances = distances.view(*prefix)
-        face_id = face_id.view(*prefix)
-        if uvw is not None:
-            uvw = uvw.view(*prefix, 3)
         return distances, face_id, uvw
 
-    def unsigned_distance(self, positions, return_uvw=False):
+    def unsigned_distance(self, positions, return_uvw=False, vertices=None):
         # positions: torch.Tensor, float, [N, 3]
-        return self._distance(positions, return_uvw, None)
+        # vertices: optional CUDA [V, 3]: refit to them and differentiate
+        return self._query(positions, return_uvw, None, vertices)
 
-    def signed_distance(self, positions, return_uvw=False, mode="watertight"):
+    def signed_distance(self, positions, return_uvw=False, mode="watertight", vertices=None):
         # positions: torch.Tensor, float, [N, 3]; inside is negative
-        return self._distance(positions, return_uvw, _sdf_mode_to_id[mode])
+        return self._query(positions, return_uvw, _sdf_mode_to_id[mode], vertices)
 
 
 def floodfill(grid, check_bounds: bool = False):

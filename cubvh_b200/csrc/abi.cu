@@ -21,6 +21,9 @@ struct DevCopy {
     int device = -1;
     CNode* nodes = nullptr;
     CTri* tris = nullptr;
+    int32_t* face_vidx = nullptr;  // [F, 3] (meshes only), uploaded on first use
+    int32_t* face_slot = nullptr;  // [F] soup slot of each face id, -1 if none
+    float* node_box = nullptr;     // [n_nodes, 6] refit scratch
 };
 
 struct cubvh_bvh {
@@ -75,6 +78,30 @@ int device_copy(cubvh_bvh* h, DevCopy** out) {
     }
     h->dev.push_back(d);
     *out = &h->dev.back();
+    return CUBVH_OK;
+}
+
+// face -> vertex indices and face -> soup slot on the device (once).
+int grad_buffers(cubvh_bvh* h, DevCopy* d, bool need_vidx) {
+    std::lock_guard<std::mutex> lk(h->mu);
+    cudaError_t e;
+    const size_t nf = h->ids.size();
+    if (!d->face_slot) {
+        std::vector<int32_t> slot(nf, -1);
+        for (size_t s = 0; s < h->host.tris.size(); ++s) {
+            const int32_t id = h->host.tris[s].id;
+            if (id >= 0 && (size_t)id < nf) slot[(size_t)id] = (int32_t)s;
+        }
+        if ((e = cudaMalloc(&d->face_slot, nf * sizeof(int32_t))) != cudaSuccess) return cuda_fail(e, "cudaMalloc(face_slot)");
+        if ((e = cudaMemcpy(d->face_slot, slot.data(), nf * sizeof(int32_t), cudaMemcpyHostToDevice)) != cudaSuccess)
+            return cuda_fail(e, "upload(face_slot)");
+    }
+    if (need_vidx && !d->face_vidx) {
+        if (h->host.faces.empty()) return fail(CUBVH_ERR_INVALID, "this BVH was created from triangle records: it has no vertex indices");
+        if ((e = cudaMalloc(&d->face_vidx, nf * 3 * sizeof(int32_t))) != cudaSuccess) return cuda_fail(e, "cudaMalloc(face_vidx)");
+        if ((e = cudaMemcpy(d->face_vidx, h->host.faces.data(), nf * 3 * sizeof(int32_t), cudaMemcpyHostToDevice)) != cudaSuccess)
+            return cuda_fail(e, "upload(face_vidx)");
+    }
     return CUBVH_OK;
 }
 
@@ -166,7 +193,12 @@ int cubvh_bvh_destroy(cubvh_bvh* h) {
     int cur = 0;
     const bool have = cudaGetDevice(&cur) == cudaSuccess;
     for (auto& d : h->dev) {
-        if (cudaSetDevice(d.device) == cudaSuccess) { cudaFree(d.nodes); cudaFree(d.tris); }
+        if (cudaSetDevice(d.device) == cudaSuccess) {
+            cudaFree(d.nodes); cudaFree(d.tris);
+            if (d.face_vidx) cudaFree(d.face_vidx);
+            if (d.face_slot) cudaFree(d.face_slot);
+            if (d.node_box) cudaFree(d.node_box);
+        }
     }
     if (have && !h->dev.empty()) cudaSetDevice(cur);
     delete h;
@@ -330,6 +362,57 @@ int cubvh_floodfill_check(const void* workspace, int B, int H, int W, int D, voi
     if (e == cudaSuccess) e = cudaStreamSynchronize((cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(e, "floodfill status read");
     if (status != 0) return fail(CUBVH_ERR_DEVICE_BOUND, "floodfill: a union-find walk exceeded its step bound");
+    return CUBVH_OK;
+    CUBVH_GUARD_END
+}
+
+int cubvh_bvh_refit(cubvh_bvh* h, const float* vertices, int64_t n_vertices, void* stream) {
+    CUBVH_GUARD_BEGIN
+    if (!h || !vertices) return fail(CUBVH_ERR_INVALID, "bvh/vertices is null");
+    if (h->host.faces.empty()) return fail(CUBVH_ERR_INVALID, "refit needs a BVH created from vertices and faces");
+    if (n_vertices != h->host.n_vertices)
+        return fail(CUBVH_ERR_INVALID, "refit: vertex count differs from the mesh the BVH was built on");
+    DevCopy* d;
+    int rc = device_copy(h, &d);
+    if (rc != CUBVH_OK) return rc;
+    if ((rc = grad_buffers(h, d, true)) != CUBVH_OK) return rc;
+    cudaError_t e;
+    {
+        std::lock_guard<std::mutex> lk(h->mu);
+        if (!d->node_box && (e = cudaMalloc(&d->node_box, h->host.nodes.size() * 6 * sizeof(float))) != cudaSuccess)
+            return cuda_fail(e, "cudaMalloc(refit scratch)");
+    }
+    e = launch_refit((int64_t)h->host.tris.size(), d->tris, d->face_vidx, vertices, d->nodes, d->node_box,
+                     h->host.level_start.data(), (int)h->host.level_start.size() - 1, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "refit launch");
+    return CUBVH_OK;
+    CUBVH_GUARD_END
+}
+
+int cubvh_distance_backward(cubvh_bvh* h, const float* points, int64_t n, const int64_t* face_id,
+                            const float* grad_distances, const float* distances, const float* vertices,
+                            float* grad_points, float* grad_vertices, void* stream) {
+    CUBVH_GUARD_BEGIN
+    if (!h) return fail(CUBVH_ERR_INVALID, "bvh is null");
+    if (n < 0) return fail(CUBVH_ERR_INVALID, "negative query count");
+    if (n == 0) return CUBVH_OK;
+    if (!points || !face_id || !grad_distances || !distances)
+        return fail(CUBVH_ERR_INVALID, "points/face_id/grad_distances/distances is null");
+    if (grad_vertices && !vertices) return fail(CUBVH_ERR_INVALID, "grad_vertices needs the current vertices");
+    DevCopy* d;
+    int rc = device_copy(h, &d);
+    if (rc != CUBVH_OK) return rc;
+    if ((rc = grad_buffers(h, d, vertices != nullptr)) != CUBVH_OK) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int64_t nf = (int64_t)h->ids.size();
+    void* ws = nullptr;
+    cudaError_t e = cudaMallocAsync(&ws, backward_workspace_bytes(n, nf), s);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync(backward workspace)");
+    e = launch_backward(n, points, face_id, grad_distances, distances, vertices, vertices ? d->face_vidx : nullptr,
+                        d->face_slot, d->tris, nf, grad_points, grad_vertices, ws, s);
+    const cudaError_t e2 = cudaFreeAsync(ws, s);
+    if (e == cudaSuccess) e = e2;
+    if (e != cudaSuccess) return cuda_fail(e, "backward launch");
     return CUBVH_OK;
     CUBVH_GUARD_END
 }

@@ -255,6 +255,10 @@ bool build_bvh(const float* xyz, int64_t nf, HostBvh& out, std::string& err) {
         out.nodes[qi] = nd;
     }
     out.depth = max_depth;
+    out.level_start.assign(1, 0);
+    for (size_t qi = 1; qi < queue.size(); ++qi)
+        if (queue[qi].level != queue[qi - 1].level) out.level_start.push_back((int32_t)qi);
+    out.level_start.push_back((int32_t)queue.size());
     const Box& rb = B.nodes[root].box;
     for (int k = 0; k < 3; ++k) { out.lo[k] = rb.lo[k]; out.hi[k] = rb.hi[k]; }
     if (out.depth > kMaxDepth) {

@@ -12,6 +12,9 @@ struct HostBvh {
     std::vector<CNode> nodes;      // node 0 is the root
     std::vector<CTri> tris;        // leaf-ordered soup
     int depth = 0;                 // internal levels (root = 1)
+    // nodes are stored breadth first: level l (root = 0) is the index range
+    // [level_start[l], level_start[l + 1])
+    std::vector<int32_t> level_start;
     int64_t slot_of_face0 = 0;     // soup slot of original face 0
     float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};  // scene bounds
     // face -> vertex indices, for refit / vertex gradients (empty when the

@@ -71,7 +71,7 @@ __device__ __forceinline__ double seg_closest_d(d3 p, d3 p0, d3 p1, double* s_ou
 // Closest point on a triangle by Voronoi regions (Ericson, "Real-Time
 // Collision Detection", 2005, sec. 5.1.5) with a segment fallback for
 // degenerate triangles.  Returns the squared distance.
-__device__ __noinline__ double closest_on_tri_d(d3 p, d3 a, d3 b, d3 c, double bary[3], d3* cp_out) {
+static __device__ __noinline__ double closest_on_tri_d(d3 p, d3 a, d3 b, d3 c, double bary[3], d3* cp_out) {
     const d3 ab = dsub(b, a), ac = dsub(c, a), ap = dsub(p, a);
     double u, v, w;
     d3 cp;
@@ -123,7 +123,7 @@ done:
 
 // Ray-triangle in double (numerator form): hit iff det != 0, u >= 0, v >= 0,
 // u + v <= 1, 0 <= t < tmax.  Writes t = tn / det.
-__device__ __noinline__ bool ray_tri_d(d3 o, d3 d, d3 a, d3 b, d3 c, double tmax, double* t_out) {
+static __device__ __noinline__ bool ray_tri_d(d3 o, d3 d, d3 a, d3 b, d3 c, double tmax, double* t_out) {
     const d3 e1 = dsub(b, a), e2 = dsub(c, a);
     const d3 pv = dcross(d, e2);
     const double det = ddot(e1, pv);
@@ -224,8 +224,8 @@ __device__ __forceinline__ float exp2i(int e) { return __int_as_float((e + 127) 
 // Coefficients (-1)^k/(2k+1)! and (-1)^k/(2k)! by a fixed IEEE division
 // sequence (filled from the host by upload_constants(); this header is
 // compiled into one translation unit only).
-__constant__ double c_sin_coef[14];
-__constant__ double c_cos_coef[14];
+static __constant__ double c_sin_coef[14];
+static __constant__ double c_cos_coef[14];
 
 __device__ __forceinline__ void det_sincos(float phi, float* s, float* c) {
     const double x = (double)phi, x2 = dM(x, x);

@@ -25,6 +25,14 @@ cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts
 cudaError_t launch_ray(int64_t n, const float* ro, const float* rd, float* pos, int64_t* fid, float* depth,
                        const CNode* nodes, const CTri* tris, void* ws, cudaStream_t stream);
 
+// refit / backward (grad.cu)
+cudaError_t launch_refit(int64_t n_tris, CTri* tris, const int32_t* face_vidx, const float* V, CNode* nodes,
+                         float* node_box, const int32_t* level_start, int n_levels, cudaStream_t stream);
+size_t backward_workspace_bytes(int64_t n, int64_t nf);
+cudaError_t launch_backward(int64_t n, const float* pts, const int64_t* fid, const float* gout, const float* dist,
+                            const float* V, const int32_t* fv, const int32_t* fslot, const CTri* tris, int64_t nf,
+                            float* gpts, float* gV, void* ws, cudaStream_t stream);
+
 // floodfill (floodfill.cu)
 size_t floodfill_workspace_bytes(int B, int H, int W, int D);
 cudaError_t launch_floodfill(const uint8_t* grid, int B, int H, int W, int D, int32_t* labels,

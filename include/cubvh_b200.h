@@ -104,6 +104,30 @@ int cubvh_signed_distance(cubvh_bvh* bvh, const float* points, int64_t n, uint32
 int cubvh_ray_trace(cubvh_bvh* bvh, const float* rays_o, const float* rays_d, int64_t n, float* positions,
                     int64_t* face_id, float* depth, void* stream);
 
+/* Differentiable queries (no counterpart in the reference, whose cuBVH
+ * detaches the vertices: cubvh/api.py:16-17).
+ *
+ * cubvh_bvh_refit: move the BVH's vertices to `vertices` (device float32
+ * [n_vertices, 3], same count and faces as at creation) and refit the device
+ * copy on the current device: same tree, boxes recomputed bottom-up.  Needs a
+ * BVH created with cubvh_bvh_create.  The host copy (state_dict) keeps the
+ * creation-time geometry.
+ *
+ * cubvh_distance_backward: gradients of unsigned or signed distances.  For
+ * query i with face face_id[i], closest point c (recomputed in double on the
+ * current geometry: `vertices` if given, else the BVH's own triangles) and
+ * sign s of distances[i]:
+ *   grad_points[i]     = grad_distances[i] * s * (p - c) / |p - c|
+ *   grad_vertices[v_k] += -lambda_k * grad_distances[i] * s * (p - c) / |p - c|
+ * (lambda = barycentric weights of c).  grad_points (float32 [n, 3]) is
+ * overwritten; grad_vertices (float32 [n_vertices, 3], needs `vertices` and
+ * a BVH created from a mesh) is accumulated into.  Either may be NULL.
+ * Queries with distance 0 contribute nothing. */
+int cubvh_bvh_refit(cubvh_bvh* bvh, const float* vertices, int64_t n_vertices, void* stream);
+int cubvh_distance_backward(cubvh_bvh* bvh, const float* points, int64_t n, const int64_t* face_id,
+                            const float* grad_distances, const float* distances, const float* vertices,
+                            float* grad_points, float* grad_vertices, void* stream);
+
 /* Floodfill of a batch of boolean grids: grid uint8/bool [B, H, W, D]
  * (nonzero = occupied), labels int32 [B, H, W, D]: -1 for occupied voxels,
  * else the smallest global linear index of the voxel's 6-connected free

@@ -210,6 +210,19 @@ void orc_face_dist64(const float* V, const int64_t* F, const float* pts, const i
     }
 }
 
+// Distance from double points to double triangles (one triangle per point),
+// tri: [n, 9]; also the closest point's barycentric weights.  Used for the
+// finite-difference pins of the distance gradients.
+void orc_tri_dist64d(const double* tri, const double* pts, int64_t n, double* dist, double* bary_out) {
+    for (int64_t i = 0; i < n; ++i) {
+        const double* t = tri + 9 * i;
+        const Tri64 T{D3{t[0], t[1], t[2]}, D3{t[3], t[4], t[5]}, D3{t[6], t[7], t[8]}};
+        double bary[3]; D3 c;
+        dist[i] = std::sqrt(closest_on_tri(D3{pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]}, T, bary, &c));
+        if (bary_out) { bary_out[3 * i] = bary[0]; bary_out[3 * i + 1] = bary[1]; bary_out[3 * i + 2] = bary[2]; }
+    }
+}
+
 // Ray/triangle in double (Moller-Trumbore arrangement; same predicate as the
 // reference's Quilez test without its safe_divide clamp): hit iff det != 0,
 // u >= 0, v >= 0, u + v <= 1, 0 <= t < tmax.  Evaluated in numerator space.

@@ -85,6 +85,16 @@ def face_dist64(V, F, pts, fids):
     return dist, uvw
 
 
+def tri_dist64d(tri, pts):
+    """Distance from double points [n, 3] to double triangles [n, 3, 3]."""
+    tri = np.ascontiguousarray(tri, dtype=np.float64).reshape(-1, 9)
+    pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+    n = len(pts)
+    d = np.empty(n, np.float64); b = np.empty((n, 3), np.float64)
+    lib().orc_tri_dist64d(_p(tri), _p(pts), I64(n), _p(d), _p(b))
+    return d, b
+
+
 def ray64(V, F, ro, rd, tmax=1000.0, eps_b=1e-9, eps_g=1e-9, tie_eps=1e-7):
     """-> t (tmax on miss), fid (-1 on miss), flags (bit0 ambiguous, bit1 tie)."""
     V, F, ro, rd = _f32(V), _i64(F), _f32(ro), _f32(rd)
