@@ -72,12 +72,13 @@ def _peaks():
         return 6650.0, "fallback"
 
 
-def _profile_traffic(kernel: str, workload: str):
-    """DRAM bytes per launch of `kernel` from a committed ncu summary."""
+def _profile_traffic(op: str, workload: str):
+    """DRAM bytes (read + write) of one full-size call of `op`, from the
+    committed ncu summary profiles/traffic_<workload>.json."""
     path = os.path.join(ROOT, "profiles", f"traffic_{workload}.json")
     try:
         with open(path) as fh:
-            return float(json.load(fh)[kernel]["dram_bytes_per_full_launch"])
+            return float(json.load(fh)[op]["dram_bytes_per_full_launch"])
     except Exception:
         return None
 
@@ -282,7 +283,7 @@ def run_ours(args):
                     torch.empty(n, device=dev))
             fn = (lambda ro=ro, rd=rd, n=n, o=outs: check(
                 L.cubvh_ray_trace(h, P(ro), P(rd), n, P(o[0]), P(o[1]), P(o[2]), sp), "ray_trace"))
-            dev_ops.append((op, n, fn, "k_ray"))
+            dev_ops.append((op, n, fn, "ray: k_ray"))
         elif op in ("sdf_watertight", "udf", "udf_uvw"):
             p = torch.from_numpy(a[0]).to(dev)
             n = p.shape[0]
@@ -292,11 +293,11 @@ def run_ours(args):
             if op == "sdf_watertight":
                 fn = (lambda p=p, n=n, d=d, fid=fid: check(
                     L.cubvh_signed_distance(h, P(p), n, 0, P(d), P(fid), ctypes.c_void_p(0), sp), "sdf"))
-                kname = "k_distance<1,false>"
+                kname = "sdf_watertight: Morton bucketing + k_udf<0,1> + k_sign_watertight"
             else:
                 fn = (lambda p=p, n=n, d=d, fid=fid, u=uptr: check(
                     L.cubvh_unsigned_distance(h, P(p), n, P(d), P(fid), u, sp), "udf"))
-                kname = "k_distance<0,%s>" % ("true" if uvw is not None else "false")
+                kname = "%s: Morton bucketing + k_udf<%d,0>" % (op, 1 if uvw is not None else 0)
             dev_ops.append((op, n, fn, kname))
             if args.workload == "dense_tori":
                 occ_src = d
@@ -311,7 +312,7 @@ def run_ours(args):
             def fn(res=res, grid=grid, lab=lab, ws=ws, nb=nb.value):
                 torch.lt(occ_src.view(res, res, res), 2.0 / res, out=grid)
                 check(L.cubvh_floodfill(P(grid), 1, res, res, res, P(lab), P(ws), nb, sp), "floodfill")
-            dev_ops.append((op, 0, fn, "floodfill"))
+            dev_ops.append((op, 0, fn, "floodfill: 11 kernels"))
 
     q_per_step = sum(n for _, n, _, _ in dev_ops)
 
@@ -430,7 +431,7 @@ def run_ours(args):
                     "steps": e2e_steps},
             "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": _profile_traffic(kname, wl["name"]),
+                         "traffic": _profile_traffic(op, wl["name"]),
                          "algorithmic_bytes_per_launch": alg},
             "cpu_baseline": {"value": cpu_q / cpu_t, "unit": "queries/s", "cores": cpu_thr, "kind": "port",
                              "sample": cpu_desc},
