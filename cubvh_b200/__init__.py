@@ -10,5 +10,6 @@
 
 from ._lib import version
 from .api import cuBVH, floodfill
+from .arena import BVHArena
 
-__all__ = ["cuBVH", "floodfill", "version"]
+__all__ = ["cuBVH", "floodfill", "BVHArena", "version"]

@@ -39,6 +39,12 @@ _SIGS = {
     "cubvh_floodfill": [c_vp, c_int, c_int, c_int, c_int, c_vp, c_vp, c_sz, c_vp],
     "cubvh_floodfill_check": [c_vp, c_int, c_int, c_int, c_int, c_vp],
     "cubvh_bvh_refit": [c_vp, c_vp, c_i64, c_vp],
+    "cubvh_arena_create": [ctypes.c_int32, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(c_vp)],
+    "cubvh_arena_destroy": [c_vp],
+    "cubvh_arena_info": [c_vp, ctypes.POINTER(c_i32), ctypes.POINTER(c_i64), ctypes.POINTER(c_i64)],
+    "cubvh_arena_set_queries": [c_vp, c_vp, c_vp],
+    "cubvh_arena_distance": [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp],
+    "cubvh_arena_backward": [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp],
     "cubvh_distance_backward": [c_vp, c_vp, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp],
 }
 _STR_FUNCS = ("cubvh_version", "cubvh_last_error")

@@ -119,6 +119,11 @@ int finish_build(cubvh_bvh* h) {
 
 }  // namespace
 
+namespace cubvh {
+// Status + message of a failed call for cubvh_last_error() (other files).
+int set_error(int code, const std::string& msg) { return fail(code, msg); }
+}  // namespace cubvh
+
 #define CUBVH_GUARD_BEGIN try {
 #define CUBVH_GUARD_END                                                          \
     } catch (const std::bad_alloc&) {                                            \

@@ -48,6 +48,7 @@ struct Builder {
 
     static constexpr int kBins = 32;
     static constexpr float kTrav = 1.0f, kIsect = 1.0f;
+    int max_leaf = kMaxLeafTris;
 
     int make_leaf(int b, int e, const Box& box) {
         Node2 n; n.box = box; n.begin = b; n.count = e - b;
@@ -89,7 +90,7 @@ struct Builder {
         }
         const float parea = std::max(box.area(), 1e-30f);
         const float split_cost = kTrav + kIsect * best_cost / parea;
-        if (n <= kMaxLeafTris && (best_axis < 0 || kIsect * n <= split_cost))
+        if (n <= max_leaf && (best_axis < 0 || kIsect * n <= split_cost))
             return make_leaf(b, e, box);
 
         int mid;
@@ -171,14 +172,16 @@ Box tri_box(const CTri& t) {
 
 }  // namespace
 
-bool build_bvh(const float* xyz, int64_t nf, HostBvh& out, std::string& err) {
+bool build_bvh(const float* xyz, int64_t nf, HostBvh& out, std::string& err, int max_leaf) {
     if (nf <= 0) { err = "mesh has no faces"; return false; }
     if (nf > (int64_t)(1 << 28)) { err = "too many faces (limit 2^28)"; return false; }
     for (int64_t i = 0; i < nf * 9; ++i)
         if (!std::isfinite(xyz[i])) { err = "vertex coordinates must be finite"; return false; }
 
+    if (max_leaf < 1 || max_leaf > kMaxLeafTris) { err = "leaf size must be in [1, 4]"; return false; }
     Builder B;
     B.xyz = xyz;
+    B.max_leaf = max_leaf;
     B.pbox.resize(nf); B.cen.resize(3 * nf); B.idx.resize(nf);
     for (int64_t f = 0; f < nf; ++f) {
         Box b; b.grow(xyz + 9 * f); b.grow(xyz + 9 * f + 3); b.grow(xyz + 9 * f + 6);

@@ -206,6 +206,46 @@ __global__ void __launch_bounds__(256) k_backward(
     }
 }
 
+__device__ __forceinline__ int mesh_of_q(const int64_t* __restrict__ qoff, int M, int64_t i) {
+    int lo = 0, hi = M - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (qoff[mid] <= i) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Arena: gradients w.r.t. the query points only, one thread per query.
+__global__ void k_arena_backward_points(int64_t n, const float* __restrict__ pts, const int64_t* __restrict__ fid,
+                                        const float* __restrict__ gout, const float* __restrict__ dist,
+                                        const int64_t* __restrict__ qoff, int M, const int64_t* __restrict__ face_off,
+                                        const int32_t* __restrict__ gslot, const CTri* __restrict__ tris,
+                                        float* __restrict__ gpts) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const int m = mesh_of_q(qoff, M, i);
+        const int64_t f = fid[i];
+        const int64_t nfm = face_off[m + 1] - face_off[m];
+        const float g = gout[i], d = dist[i];
+        float gp[3] = {0.f, 0.f, 0.f};
+        if (f >= 0 && f < nfm && g != 0.f && d != 0.f) {
+            const int32_t s = gslot[face_off[m] + f];
+            if (s >= 0) {
+                const TriV t = load_tri(tris, s);
+                const d3 p = to_d3(load3g(pts, i));
+                double lam[3]; d3 cp;
+                const double d2 = closest_on_tri_d(p, to_d3(t.a), to_d3(t.b), to_d3(t.c), lam, &cp);
+                if (d2 > 0.0) {
+                    const double sc = (signbit(d) ? -(double)g : (double)g) / __dsqrt_rn(d2);
+                    const d3 r = dsub(p, cp);
+                    gp[0] = (float)(r.x * sc); gp[1] = (float)(r.y * sc); gp[2] = (float)(r.z * sc);
+                }
+            }
+        }
+        gpts[3 * i] = gp[0]; gpts[3 * i + 1] = gp[1]; gpts[3 * i + 2] = gp[2];
+    }
+}
+
 }  // namespace
 
 cudaError_t launch_refit(int64_t n_tris, CTri* tris, const int32_t* face_vidx, const float* V, CNode* nodes,
@@ -217,6 +257,15 @@ cudaError_t launch_refit(int64_t n_tris, CTri* tris, const int32_t* face_vidx, c
         if (l1 <= l0) continue;
         k_refit_level<<<(unsigned)((l1 - l0 + 63) / 64), 64, 0, stream>>>(l0, l1, nodes, tris, node_box);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_arena_backward(int64_t n, const float* pts, const int64_t* fid, const float* gout,
+                                  const float* dist, const int64_t* qoff, int M, const int64_t* face_off,
+                                  const int32_t* gslot, const CTri* tris, float* gpts, cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    k_arena_backward_points<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(n, pts, fid, gout, dist, qoff, M, face_off,
+                                                                             gslot, tris, gpts);
     return cudaGetLastError();
 }
 

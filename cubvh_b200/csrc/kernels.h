@@ -11,6 +11,34 @@ namespace cubvh {
 
 cudaError_t upload_constants();
 
+// Arena work descriptors (query.cu): a packet is up to 32 consecutive
+// positions of the (sorted) query order, all on one mesh.
+struct PacketDesc { int64_t start; int32_t count; int32_t mesh; };
+struct MeshDesc { int32_t root; int32_t slot0; int64_t qoff; };
+
+// Per-mesh Morton bucketing of an arena's queries: box of the mesh's
+// queries, bits per axis, first cell of the mesh in the global histogram.
+struct ArenaSortDesc { float lo[3], hi[3]; int32_t bits; int64_t cell_off; };
+
+// Everything one arena launch needs (device pointers unless noted).
+struct ArenaLaunch {
+    const CNode* nodes; const CTri* tris;
+    int32_t n_meshes;
+    int64_t n_queries;
+    const int64_t* qoff;               // [M + 1] first query of each mesh
+    const MeshDesc* meshes;            // [M]
+    const ArenaSortDesc* sort;         // [M]
+    int64_t n_cells;
+    const PacketDesc* packets; int64_t n_packets;        // every query
+    const PacketDesc* wt_packets; int64_t n_wt_packets;  // watertight meshes
+    const PacketDesc* rs_packets; int64_t n_rs_packets;  // raystab meshes
+    unsigned long long* counters;      // 256 bytes
+    uint32_t* order; uint32_t* hist; uint32_t* bsum; int32_t* slots;
+};
+cudaError_t launch_arena_distance(const ArenaLaunch& a, const float* pts, float* dist, int64_t* fid, float* uvw,
+                                  cudaStream_t stream);
+int cell_bits_for(int64_t n);
+
 // Point queries at least this many are visited in Morton-cell order.
 constexpr int64_t kSortMinQueries = 2048;
 
@@ -29,6 +57,9 @@ cudaError_t launch_ray(int64_t n, const float* ro, const float* rd, float* pos, 
 cudaError_t launch_refit(int64_t n_tris, CTri* tris, const int32_t* face_vidx, const float* V, CNode* nodes,
                          float* node_box, const int32_t* level_start, int n_levels, cudaStream_t stream);
 size_t backward_workspace_bytes(int64_t n, int64_t nf);
+cudaError_t launch_arena_backward(int64_t n, const float* pts, const int64_t* fid, const float* gout,
+                                  const float* dist, const int64_t* qoff, int M, const int64_t* face_off,
+                                  const int32_t* gslot, const CTri* tris, float* gpts, cudaStream_t stream);
 cudaError_t launch_backward(int64_t n, const float* pts, const int64_t* fid, const float* gout, const float* dist,
                             const float* V, const int32_t* fv, const int32_t* fslot, const CTri* tris, int64_t nf,
                             float* gpts, float* gV, void* ws, cudaStream_t stream);

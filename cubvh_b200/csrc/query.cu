@@ -122,10 +122,10 @@ __device__ __forceinline__ void leaf_range(int ref, int& s0, int& s1) {
 // drew cheap packets keep taking more and no SM idles while work remains.
 struct PacketQueue {
     unsigned long long* ctr;
-    int64_t n, grab, next, end;
-    __device__ __forceinline__ PacketQueue(unsigned long long* c, int64_t n_, int64_t g)
-        : ctr(c), n(n_), grab(g), next(0), end(0) {}
-    // base query index of the warp's next packet, or -1 when done
+    int64_t npk, grab, next, end;
+    __device__ __forceinline__ PacketQueue(unsigned long long* c, int64_t npk_, int64_t g)
+        : ctr(c), npk(npk_), grab(g), next(0), end(0) {}
+    // index of the warp's next packet, or -1 when done
     __device__ __forceinline__ int64_t take() {
         if (next == end) {
             unsigned long long b = 0;
@@ -133,9 +133,30 @@ struct PacketQueue {
             next = (int64_t)__shfl_sync(kFull, b, 0);
             end = next + grab;
         }
-        const int64_t base = next * 32;
-        ++next;
-        return base < n ? base : -1;
+        const int64_t p = next++;
+        return p < npk ? p : -1;
+    }
+};
+
+// What a launch works on: implicit 32-query packets over one BVH (root node
+// 0), or a table of packets, each up to 32 consecutive positions of the
+// query order on one mesh of an arena (root node, face-0 slot and first
+// query index of that mesh).
+struct Work {
+    const PacketDesc* table;  // nullptr: implicit packets
+    const MeshDesc* meshes;
+    int64_t n;                // implicit: queries; table: packets
+    int slot0;                // implicit: face-0 slot of the single BVH
+    __device__ __forceinline__ int64_t packets() const { return table ? n : (n + 31) >> 5; }
+    __device__ __forceinline__ void get(int64_t p, int64_t& start, int& count, int& root, int& s0,
+                                        int64_t& qoff) const {
+        if (table) {
+            const PacketDesc d = table[p];
+            const MeshDesc m = meshes[d.mesh];
+            start = d.start; count = d.count; root = m.root; s0 = m.slot0; qoff = m.qoff;
+        } else {
+            start = p * 32; count = (int)min((int64_t)32, n - start); root = 0; s0 = slot0; qoff = 0;
+        }
     }
 };
 
@@ -187,17 +208,20 @@ constexpr int kCand = 8;  // per-lane candidate list of the distance search
 // the end every lane evaluates its surviving candidates in double: the
 // minimum (ties -> lowest face index) is the exact nearest triangle.
 template <bool UVW, bool SLOT>
-__global__ void __launch_bounds__(kQBlock) k_udf(int64_t n, const uint32_t* __restrict__ order,
+__global__ void __launch_bounds__(kQBlock) k_udf(Work w, const uint32_t* __restrict__ order,
                                                  const float* __restrict__ pts, float* __restrict__ dist,
                                                  int64_t* __restrict__ face_id, float* __restrict__ uvw,
                                                  int32_t* __restrict__ slot_out, const CNode* __restrict__ nodes,
-                                                 const CTri* __restrict__ tris, int slot_face0,
+                                                 const CTri* __restrict__ tris,
                                                  unsigned long long* __restrict__ ctr, int64_t grab) {
     const int lane = threadIdx.x & 31;
-    PacketQueue pq(ctr, n, grab);
-    for (int64_t base = pq.take(); base >= 0; base = pq.take()) {
-        const int64_t qi = base + lane;
-        const bool act = qi < n;
+    PacketQueue pq(ctr, w.packets(), grab);
+    for (int64_t pk = pq.take(); pk >= 0; pk = pq.take()) {
+        int64_t start, qoff;
+        int cnt, root, slot_face0;
+        w.get(pk, start, cnt, root, slot_face0, qoff);
+        const int64_t qi = start + lane;
+        const bool act = lane < cnt;
         const int64_t idx = act ? (order ? (int64_t)order[qi] : qi) : 0;
         const float3 p = act ? load3(pts, idx) : make_float3(0.f, 0.f, 0.f);
         const d3 pd = to_d3(p);
@@ -219,9 +243,9 @@ __global__ void __launch_bounds__(kQBlock) k_udf(int64_t n, const uint32_t* __re
             }
             nc = 0;
         };
-        uint32_t cullmax = __reduce_max_sync(kFull, __float_as_uint(fmaxf(cull, 0.f)) | (act ? 0u : 0u));
+        uint32_t cullmax = __reduce_max_sync(kFull, __float_as_uint(fmaxf(cull, 0.f)));
         WarpStack st;
-        int cur = 0;
+        int cur = root;
         bool live = __any_sync(kFull, act);
         while (live) {
             if (cur >= 0) {
@@ -297,7 +321,7 @@ __global__ void __launch_bounds__(kQBlock) k_udf(int64_t n, const uint32_t* __re
 // Sum of unit normals of every triangle whose squared distance to cp is
 // below 1e-6 (src/bvh.cu:356-396; the division by the count does not change
 // the sign and is omitted).
-__device__ d3 normal_sum(const CNode* __restrict__ nodes, const CTri* __restrict__ tris, d3 cp) {
+__device__ d3 normal_sum(const CNode* __restrict__ nodes, const CTri* __restrict__ tris, d3 cp, int root) {
     const float3 cf = make_float3(__double2float_rn(cp.x), __double2float_rn(cp.y), __double2float_rn(cp.z));
     const float cinf = f3inf(cf);
     const float r = 1e-3f + 4e-7f * (1.f + cinf);
@@ -306,7 +330,7 @@ __device__ d3 normal_sum(const CNode* __restrict__ nodes, const CTri* __restrict
     d3 sum{0.0, 0.0, 0.0};
     int st[kStack];
     int sp = 0;
-    st[sp++] = 0;
+    st[sp++] = root;
     while (sp > 0) {
         const int ref = st[--sp];
         if (ref >= 0) {
@@ -339,23 +363,26 @@ __device__ d3 normal_sum(const CNode* __restrict__ nodes, const CTri* __restrict
     return sum;
 }
 
-__global__ void __launch_bounds__(kQBlock) k_sign_watertight(int64_t n, const uint32_t* __restrict__ order,
+__global__ void __launch_bounds__(kQBlock) k_sign_watertight(Work w, const uint32_t* __restrict__ order,
                                                              const float* __restrict__ pts,
                                                              float* __restrict__ dist,
                                                              const int32_t* __restrict__ slots,
                                                              const CNode* __restrict__ nodes,
                                                              const CTri* __restrict__ tris,
                                                              unsigned long long* __restrict__ ctr, int64_t grab) {
-    PacketQueue pq(ctr, n, grab);
-    for (int64_t base = pq.take(); base >= 0; base = pq.take()) {
-        const int64_t q = base + (threadIdx.x & 31);
-        if (q >= n) continue;
+    PacketQueue pq(ctr, w.packets(), grab);
+    for (int64_t pk = pq.take(); pk >= 0; pk = pq.take()) {
+        int64_t start, qoff;
+        int cnt, root, s0;
+        w.get(pk, start, cnt, root, s0, qoff);
+        if ((int)(threadIdx.x & 31) >= cnt) continue;
+        const int64_t q = start + (threadIdx.x & 31);
         const int64_t idx = order ? (int64_t)order[q] : q;
         const d3 pd = to_d3(load3(pts, idx));
         const TriV t = load_tri(tris, slots[idx]);
         double bary[3]; d3 cp;
         closest_on_tri_d(pd, to_d3(t.a), to_d3(t.b), to_d3(t.c), bary, &cp);
-        const d3 ns = normal_sum(nodes, tris, cp);
+        const d3 ns = normal_sum(nodes, tris, cp, root);
         // copysign(distance, avg_normal . (p - cp))
         const double s = ddot(ns, dsub(pd, cp));
         const float d = dist[idx];
@@ -365,15 +392,15 @@ __global__ void __launch_bounds__(kQBlock) k_sign_watertight(int64_t n, const ui
 
 // --------------------------------------------------------------- raystab
 // Any hit with 0 <= t < tmax (FP32 filter, FP64 for undecided triangles).
-__device__ bool any_hit(const CNode* __restrict__ nodes, const CTri* __restrict__ tris, float3 o, float3 d,
-                        double tmax) {
+__device__ bool any_hit(const CNode* __restrict__ nodes, const CTri* __restrict__ tris, int root, float3 o,
+                        float3 d, double tmax) {
     const float3 inv = make_float3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
     const float dinf = f3inf(d);
     const float tmaxf = (float)tmax;
     const float cull = cull_of(tmax);
     int st[kStack];
     int sp = 0;
-    st[sp++] = 0;
+    st[sp++] = root;
     while (sp > 0) {
         const int ref = st[--sp];
         if (ref >= 0) {
@@ -409,23 +436,27 @@ __device__ bool any_hit(const CNode* __restrict__ nodes, const CTri* __restrict_
 // within [0, 1000) (src/bvh.cu:408-427); the first miss ends the query.
 // Queries are visited in Morton-cell order so neighbouring lanes trace
 // neighbouring origins.
-__global__ void __launch_bounds__(kQBlock) k_sign_raystab(int64_t n, const uint32_t* __restrict__ order,
+__global__ void __launch_bounds__(kQBlock) k_sign_raystab(Work w, const uint32_t* __restrict__ order,
                                                           const float* __restrict__ pts, float* __restrict__ dist,
                                                           const CNode* __restrict__ nodes,
                                                           const CTri* __restrict__ tris,
                                                           unsigned long long* __restrict__ ctr, int64_t grab) {
-    PacketQueue pq(ctr, n, grab);
-    for (int64_t base = pq.take(); base >= 0; base = pq.take()) {
-        const int64_t q = base + (threadIdx.x & 31);
-        if (q >= n) continue;
+    PacketQueue pq(ctr, w.packets(), grab);
+    for (int64_t pk = pq.take(); pk >= 0; pk = pq.take()) {
+        int64_t start, qoff;
+        int cnt, root, s0;
+        w.get(pk, start, cnt, root, s0, qoff);
+        if ((int)(threadIdx.x & 31) >= cnt) continue;
+        const int64_t q = start + (threadIdx.x & 31);
         const int64_t idx = order ? (int64_t)order[q] : q;
         const float3 p = load3(pts, idx);
-        const float2 off = stab_offset((uint32_t)idx);
+        // the stab stream of a query is its index within its own call / mesh
+        const float2 off = stab_offset((uint32_t)(idx - qoff));
         bool inside = true;
         for (uint32_t k = 0; k < 32 && inside; ++k) {
             const float3 dir = stab_dir(k, off);
-            if (!any_hit(nodes, tris, p, make_float3(-dir.x, -dir.y, -dir.z), 1000.0) ||
-                !any_hit(nodes, tris, p, dir, 1000.0))
+            if (!any_hit(nodes, tris, root, p, make_float3(-dir.x, -dir.y, -dir.z), 1000.0) ||
+                !any_hit(nodes, tris, root, p, dir, 1000.0))
                 inside = false;
         }
         if (inside) dist[idx] = -dist[idx];
@@ -446,9 +477,9 @@ __global__ void __launch_bounds__(kQBlock) k_ray(int64_t n, const float* __restr
                                                  const CNode* __restrict__ nodes, const CTri* __restrict__ tris,
                                                  unsigned long long* __restrict__ ctr, int64_t grab) {
     const int lane = threadIdx.x & 31;
-    PacketQueue pq(ctr, n, grab);
-    for (int64_t base = pq.take(); base >= 0; base = pq.take()) {
-        const int64_t q = base + lane;
+    PacketQueue pq(ctr, (n + 31) >> 5, grab);
+    for (int64_t pk = pq.take(); pk >= 0; pk = pq.take()) {
+        const int64_t q = pk * 32 + lane;
         const bool act = q < n;
         const float3 o = act ? load3(ro, q) : make_float3(0.f, 0.f, 0.f);
         const float3 d = act ? load3(rd, q) : make_float3(1.f, 1.f, 1.f);
@@ -682,18 +713,19 @@ cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts
         k_cell_scatter<<<g, 256, 0, stream>>>(n, pts, box, bits, hist, order);
     }
     int32_t* slots = mode != 0 ? reinterpret_cast<int32_t*>(w) : nullptr;
+    const Work work{nullptr, nullptr, n, slot_face0};
 #define CUBVH_L(U, S) do { const unsigned g_ = persistent_grid(k_udf<U, S>, n); \
-        k_udf<U, S><<<g_, kQBlock, 0, stream>>>(n, order, pts, dist, fid, uvw, slots, nodes, tris, slot_face0, \
+        k_udf<U, S><<<g_, kQBlock, 0, stream>>>(work, order, pts, dist, fid, uvw, slots, nodes, tris, \
                                                 ctr, grab_for(n, g_)); } while (0)
     if (mode == 0) { if (want_uvw) CUBVH_L(true, false); else CUBVH_L(false, false); }
     else { if (want_uvw) CUBVH_L(true, true); else CUBVH_L(false, true); }
 #undef CUBVH_L
     if (mode == 1) {
         const unsigned g = persistent_grid(k_sign_watertight, n);
-        k_sign_watertight<<<g, kQBlock, 0, stream>>>(n, order, pts, dist, slots, nodes, tris, ctr + 1, grab_for(n, g));
+        k_sign_watertight<<<g, kQBlock, 0, stream>>>(work, order, pts, dist, slots, nodes, tris, ctr + 1, grab_for(n, g));
     } else if (mode == 2) {
         const unsigned g = persistent_grid(k_sign_raystab, n);
-        k_sign_raystab<<<g, kQBlock, 0, stream>>>(n, order, pts, dist, nodes, tris, ctr + 1, grab_for(n, g));
+        k_sign_raystab<<<g, kQBlock, 0, stream>>>(work, order, pts, dist, nodes, tris, ctr + 1, grab_for(n, g));
     }
     return cudaGetLastError();
 }
@@ -708,6 +740,77 @@ cudaError_t launch_ray(int64_t n, const float* ro, const float* rd, float* pos, 
     k_ray<<<g, kQBlock, 0, stream>>>(n, ro, rd, pos, fid, depth, nodes, tris, ctr, grab_for(n, g));
     return cudaGetLastError();
 }
+
+// ------------------------------------------------------------------ arena
+// Query -> mesh: binary search over the meshes' first query indices.
+__device__ __forceinline__ int mesh_of(const int64_t* __restrict__ qoff, int M, int64_t i) {
+    int lo = 0, hi = M - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (qoff[mid] <= i) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+__device__ __forceinline__ uint32_t arena_cell(float3 p, const ArenaSortDesc& s) {
+    const float side = (float)(1 << s.bits), m = side - 1.f;
+    const float c[3] = {p.x, p.y, p.z};
+    uint32_t g[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float sc = s.hi[k] > s.lo[k] ? side / (s.hi[k] - s.lo[k]) : 0.f;
+        const float v = (c[k] - s.lo[k]) * sc;
+        g[k] = (uint32_t)fminf(fmaxf(v == v ? v : 0.f, 0.f), m);
+    }
+    return (uint32_t)s.cell_off + (spread3(g[0]) | (spread3(g[1]) << 1) | (spread3(g[2]) << 2));
+}
+__global__ void k_arena_hist(int64_t n, const float* __restrict__ pts, const int64_t* __restrict__ qoff, int M,
+                             const ArenaSortDesc* __restrict__ sd, uint32_t* __restrict__ hist) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        atomicAdd(&hist[arena_cell(load3(pts, i), sd[mesh_of(qoff, M, i)])], 1u);
+}
+__global__ void k_arena_scatter(int64_t n, const float* __restrict__ pts, const int64_t* __restrict__ qoff, int M,
+                                const ArenaSortDesc* __restrict__ sd, uint32_t* __restrict__ offs,
+                                uint32_t* __restrict__ order) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        order[atomicAdd(&offs[arena_cell(load3(pts, i), sd[mesh_of(qoff, M, i)])], 1u)] = (uint32_t)i;
+}
+
+cudaError_t launch_arena_distance(const ArenaLaunch& a, const float* pts, float* dist, int64_t* fid, float* uvw,
+                                  cudaStream_t stream) {
+    if (a.n_queries <= 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(a.counters, 0, 256, stream);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(a.hist, 0, sizeof(uint32_t) * (a.n_cells + 1), stream)) != cudaSuccess) return e;
+    const unsigned g = (unsigned)sm_count() * 8;
+    k_arena_hist<<<g, 256, 0, stream>>>(a.n_queries, pts, a.qoff, a.n_meshes, a.sort, a.hist);
+    scan::exclusive(a.hist, a.bsum, a.n_cells, stream);
+    k_arena_scatter<<<g, 256, 0, stream>>>(a.n_queries, pts, a.qoff, a.n_meshes, a.sort, a.hist, a.order);
+    const bool signed_any = a.n_wt_packets > 0 || a.n_rs_packets > 0;
+    const Work all{a.packets, a.meshes, a.n_packets, 0};
+#define CUBVH_L(U, S) do { const unsigned g_ = persistent_grid(k_udf<U, S>, a.n_queries); \
+        k_udf<U, S><<<g_, kQBlock, 0, stream>>>(all, a.order, pts, dist, fid, uvw, a.slots, a.nodes, a.tris, \
+                                                a.counters, grab_for(a.n_queries, g_)); } while (0)
+    if (uvw) { if (signed_any) CUBVH_L(true, true); else CUBVH_L(true, false); }
+    else { if (signed_any) CUBVH_L(false, true); else CUBVH_L(false, false); }
+#undef CUBVH_L
+    if (a.n_wt_packets > 0) {
+        const Work w{a.wt_packets, a.meshes, a.n_wt_packets, 0};
+        const unsigned gw = persistent_grid(k_sign_watertight, 32 * a.n_wt_packets);
+        k_sign_watertight<<<gw, kQBlock, 0, stream>>>(w, a.order, pts, dist, a.slots, a.nodes, a.tris,
+                                                      a.counters + 1, grab_for(32 * a.n_wt_packets, gw));
+    }
+    if (a.n_rs_packets > 0) {
+        const Work w{a.rs_packets, a.meshes, a.n_rs_packets, 0};
+        const unsigned gr = persistent_grid(k_sign_raystab, 32 * a.n_rs_packets);
+        k_sign_raystab<<<gr, kQBlock, 0, stream>>>(w, a.order, pts, dist, a.nodes, a.tris, a.counters + 2,
+                                                   grab_for(32 * a.n_rs_packets, gr));
+    }
+    return cudaGetLastError();
+}
+
+int cell_bits_for(int64_t n) { return cell_bits(n); }
 
 cudaError_t upload_constants() {
     double s[14], c[14];

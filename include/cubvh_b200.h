@@ -128,6 +128,34 @@ int cubvh_distance_backward(cubvh_bvh* bvh, const float* points, int64_t n, cons
                             const float* grad_distances, const float* distances, const float* vertices,
                             float* grad_points, float* grad_vertices, void* stream);
 
+/* Batched queries over many meshes in one launch (no counterpart in the
+ * reference, which serves one mesh per cuBVH object and one launch per call).
+ *
+ * cubvh_arena_create: build every mesh (host, in parallel) into one arena;
+ * vertices[m] float32 [n_vertices[m], 3], faces[m] int64 [n_faces[m], 3]
+ * (host); max_leaf[m] in [1, 4] (NULL = 4) is the leaf size of mesh m.
+ * cubvh_arena_set_queries: fix the query layout: the queries of mesh m are
+ * rows [query_offsets[m], query_offsets[m + 1]) of one points array (host
+ * int64 [M + 1]); modes[m] (host uint32 [M]) is 0 unsigned, 1 watertight,
+ * 2 raystab (stab streams use the query's index within its mesh).  Uploads
+ * the layout and sizes its workspace (synchronous; call before capture).
+ * cubvh_arena_distance: all queries of all meshes; face_id is the face index
+ * within the query's mesh; uvw may be NULL.  Only stream-ordered work: can be
+ * captured in a CUDA graph; calls on one arena must not overlap on the GPU.
+ * cubvh_arena_backward: gradients w.r.t. the query points (as
+ * cubvh_distance_backward; grad_points overwritten). */
+typedef struct cubvh_arena cubvh_arena;
+int cubvh_arena_create(int32_t n_meshes, const float* const* vertices, const int64_t* n_vertices,
+                       const int64_t* const* faces, const int64_t* n_faces, const int32_t* max_leaf,
+                       cubvh_arena** out);
+int cubvh_arena_destroy(cubvh_arena* arena);
+int cubvh_arena_info(const cubvh_arena* arena, int32_t* n_meshes, int64_t* n_faces, int64_t* n_nodes);
+int cubvh_arena_set_queries(cubvh_arena* arena, const int64_t* query_offsets, const uint32_t* modes);
+int cubvh_arena_distance(cubvh_arena* arena, const float* points, float* distances, int64_t* face_id, float* uvw,
+                         void* stream);
+int cubvh_arena_backward(cubvh_arena* arena, const float* points, const int64_t* face_id,
+                         const float* grad_distances, const float* distances, float* grad_points, void* stream);
+
 /* Floodfill of a batch of boolean grids: grid uint8/bool [B, H, W, D]
  * (nonzero = occupied), labels int32 [B, H, W, D]: -1 for occupied voxels,
  * else the smallest global linear index of the voxel's 6-connected free
