@@ -155,6 +155,13 @@ def build_workload(name: str, res: int = 2048, sdf_points: int = 8 << 20):
         g = W.dense_grid(w["grid_res"])
         return dict(name=name, vertices=w["vertices"], faces=w["faces"], ops=[("udf", (g,)), ("floodfill", (512,))],
                     desc="12 tori (174,778 faces, 10% removed); UDF on the 512^3 grid + floodfill of udf < 2/512")
+    if name == "grad_displaced":
+        w = W.grad_displaced()
+        return dict(name=name, vertices=w["vertices"], faces=w["faces"], ops=[("udf", (w["points"],))],
+                    desc="displaced icosphere L6 (81,920 faces); 4,194,304 points (half U[-1,1]^3, half "
+                         "+-0.05 of the surface); fwd + bwd w.r.t. points and vertices")
+    if name == "batch_256":
+        raise SystemExit("batch_256 has no single-mesh CPU view")
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -445,6 +452,174 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
 
 
+# ------------------------------------------------- forward + backward arms
+def _timed(fn, steps, stream):
+    import torch
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0.record(stream)
+    for _ in range(steps):
+        fn()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    return t0.elapsed_time(t1) / steps
+
+
+def run_ours_fwd_bwd(args):
+    """grad_displaced: distance + backward w.r.t. points and vertices (and the
+    200-step Adam sphere fit); batch_256: 256 meshes in one arena launch vs
+    one cuBVH call per mesh, forward + backward w.r.t. the points."""
+    import torch
+    rank, world, local = _rank_info()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    import cubvh_b200 as cubvh
+    from cubvh_b200 import workloads as W
+    stream = torch.cuda.current_stream(dev)
+    extra = {}
+    if args.workload == "grad_displaced":
+        w = W.grad_displaced()
+        bvh = cubvh.cuBVH(w["vertices"], w["faces"])
+        pts = torch.from_numpy(w["points"]).to(dev)
+        wts = torch.from_numpy(w["weights"]).to(dev)
+        V = torch.from_numpy(w["vertices"]).to(dev)
+        nq = pts.shape[0]
+
+        def step():
+            p = pts.detach().requires_grad_()
+            v = V.detach().requires_grad_()
+            d, _, _ = bvh.unsigned_distance(p, vertices=v)
+            (wts * d).sum().backward()
+
+        desc = ("displaced icosphere L6 (81,920 faces); 4,194,304 points; loss sum(w*udf); "
+                "grads w.r.t. points and vertices")
+        kname = "fwd_bwd: Morton bucketing + k_udf + face counting sort + k_backward"
+        # Adam: fit a level-5 sphere's vertices to samples of this mesh's surface
+        rng = np.random.default_rng(3)
+        samples = torch.from_numpy(W.surface_points(w["vertices"], w["faces"], nq, 0.0, rng)).to(dev)
+        v5, f5 = W.icosphere(5, 0.5)
+        fit = cubvh.cuBVH(v5, f5)
+        vv = torch.from_numpy(v5).to(dev).requires_grad_()
+        opt = torch.optim.Adam([vv], lr=2e-3)
+
+        def adam_step():
+            opt.zero_grad(set_to_none=True)
+            d, _, _ = fit.unsigned_distance(samples, vertices=vv)
+            loss = d.mean()
+            loss.backward()
+            opt.step()
+            return loss
+
+        l0 = float(adam_step().item())
+        ams = _timed(adam_step, max(1, args.adam_steps - 1), stream)
+        l1 = float(adam_step().item())
+        extra["adam_fit"] = {"steps": args.adam_steps, "ms_per_step": ams, "loss_first": l0, "loss_last": l1,
+                             "fwd_bwd_queries_per_s": nq / (ams / 1e3),
+                             "sphere": "icosphere L5 (20,480 faces)", "samples": nq}
+    else:
+        from cubvh_b200.autotune import autotune_leaf_sizes
+        ms = W.batch_256(n_meshes=args.meshes)
+        meshes = [(m["vertices"], m["faces"]) for m in ms]
+        qs = [m["points"] for m in ms]
+        modes = ["unsigned" if i % 2 == 0 else "raystab" for i in range(len(ms))]
+        leaves, report = autotune_leaf_sizes(meshes, qs, modes, sample=32768, repeats=2, device=dev)
+        arena = cubvh.BVHArena(meshes, leaf_sizes=leaves)
+        counts = [len(q) for q in qs]
+        arena.set_queries(counts, modes, device=dev)
+        pts = torch.from_numpy(np.concatenate(qs)).to(dev)
+        nq = pts.shape[0]
+
+        def step():
+            p = pts.detach().requires_grad_()
+            d, _, _ = arena.distance(p)
+            d.sum().backward()
+
+        # the same work as one cuBVH per mesh, one call (and backward) each
+        bvhs = [cubvh.cuBVH(v, f) for v, f in meshes]
+        off = np.concatenate([[0], np.cumsum(counts)])
+        views = [pts[off[i]:off[i + 1]] for i in range(len(ms))]
+
+        def per_call():
+            for b_, q_, mode in zip(bvhs, views, modes):
+                p = q_.detach().requires_grad_()
+                d = b_.unsigned_distance(p)[0] if mode == "unsigned" else b_.signed_distance(p, mode=mode)[0]
+                d.sum().backward()
+
+        per_call()
+        pc_ms = _timed(per_call, 1, stream)
+        desc = (f"{len(ms)} meshes (displaced icospheres L2-7 / tori, {sum(len(f) for _, f in meshes):,} faces), "
+                f"{nq:,} queries (10k-2M per mesh, log-uniform), even meshes unsigned, odd raystab; fwd + bwd")
+        kname = "batched fwd_bwd: arena bucketing + k_udf + k_sign_raystab + k_arena_backward_points"
+        extra["per_call"] = {"ms_per_step": pc_ms, "queries_per_s": nq / (pc_ms / 1e3)}
+        extra["autotune"] = {str(k): v for k, v in report.items()}
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ms_step = _timed(step, args.steps, stream)
+    ms_step = max_over_ranks(ms_step, dev)
+    value = world * nq / (ms_step / 1e3)
+    if args.workload == "batch_256":
+        extra["speedup_vs_per_call"] = extra["per_call"]["ms_per_step"] / ms_step
+    # e2e: host points in, gradients and distances back
+    hp = pts.detach().cpu().pin_memory()
+    hd = torch.empty(nq, pin_memory=True)
+    hg = torch.empty(nq, 3, pin_memory=True)
+
+    def e2e():
+        p = hp.to(dev, non_blocking=True).requires_grad_()
+        if args.workload == "batch_256":
+            d, _, _ = arena.distance(p)
+        else:
+            d, _, _ = bvh.unsigned_distance(p, vertices=V.detach().requires_grad_())
+        d.sum().backward()
+        hd.copy_(d.detach(), non_blocking=True)
+        hg.copy_(p.grad, non_blocking=True)
+
+    for _ in range(2):
+        e2e()
+    torch.cuda.synchronize()
+    w0 = time.perf_counter()
+    for _ in range(max(2, min(args.steps, 3))):
+        e2e()
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks((time.perf_counter() - w0) * 1e3 / max(2, min(args.steps, 3)), dev)
+    if rank == 0:
+        peak, peak_kind = _peaks()
+        # algorithmic bytes per fwd+bwd query: forward query I/O (12 in, 12
+        # out) + backward (12 p, 8 face, 4 grad, 4 dist read, 12 grad written)
+        io = 24 + 40
+        achieved = nq * io / (ms_step / 1e3) / 1e9
+        line = {
+            "metric": "mesh queries/s, forward + backward", "value": value, "unit": "queries/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded meshes and queries)",
+            "config": {"workload": args.workload, "description": desc, "queries_per_step": nq,
+                       "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
+            "e2e": {"value": world * nq / (e2e_ms / 1e3), "unit": "queries/s",
+                    "h2d_bytes_per_step": nq * 12, "d2h_bytes_per_step": nq * 16},
+            "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                         "algorithmic_bytes_per_launch": nq * io,
+                         "note": "query I/O bytes only (no traversal bytes) for the fwd+bwd workloads"},
+            "cpu_baseline": None, "gpu_launches": None, "clocks": clk.summary(), "ops": extra,
+        }
+        if args.workload == "grad_displaced":
+            wl = build_workload("grad_displaced")
+            cq, ct, cthr, cdesc = cpu_time_sample(wl, 4 << 20)
+            line["cpu_baseline"] = {"value": cq / ct, "unit": "queries/s", "cores": cthr, "kind": "port",
+                                    "sample": cdesc + " (forward only: the reference has no backward)"}
+            line["gpu_launches"] = args.steps * 9
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -452,7 +627,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="rays_displaced",
-                    choices=["rays_displaced", "udf_icosphere", "dense_tori"])
+                    choices=["rays_displaced", "udf_icosphere", "dense_tori", "grad_displaced", "batch_256"])
+    ap.add_argument("--adam-steps", type=int, default=200, help="grad_displaced: sphere-fitting steps")
+    ap.add_argument("--meshes", type=int, default=256, help="batch_256: number of meshes")
     ap.add_argument("--res", type=int, default=2048, help="camera resolution (rays_displaced)")
     ap.add_argument("--sdf-points", type=int, default=8 << 20, help="SDF queries (rays_displaced)")
     args = ap.parse_args()
@@ -460,6 +637,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload in ("grad_displaced", "batch_256"):
+        run_ours_fwd_bwd(args)
     else:
         run_ours(args)
 

@@ -26,6 +26,7 @@ which is what gives the ~180k-face total of the dense-grid workload.
 
 from __future__ import annotations
 
+import functools
 import math
 
 import numpy as np
@@ -42,6 +43,12 @@ __all__ = [
 # --------------------------------------------------------------------------
 def icosphere(level: int, radius: float = 1.0):
     """Subdivided icosahedron: 10*4^level + 2 vertices, 20*4^level faces."""
+    v, f = _unit_icosphere(level)
+    return (v * radius).astype(np.float32), f.copy()
+
+
+@functools.lru_cache(maxsize=None)
+def _unit_icosphere(level: int):
     t = (1.0 + 5.0 ** 0.5) / 2.0
     v = np.array([
         [-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0],
@@ -69,7 +76,10 @@ def icosphere(level: int, radius: float = 1.0):
         f = np.concatenate([
             np.stack([f0, m01, m20], 1), np.stack([f1, m12, m01], 1),
             np.stack([f2, m20, m12], 1), np.stack([m01, m12, m20], 1)], axis=0)
-    return (v * radius).astype(np.float32), f.astype(np.int64)
+    v.setflags(write=False)
+    f = f.astype(np.int64)
+    f.setflags(write=False)
+    return v, f
 
 
 def displaced_icosphere(level: int, seed: int, radius: float = 0.7, amp: float = 0.08,
