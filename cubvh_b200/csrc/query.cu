@@ -101,14 +101,63 @@ __device__ __forceinline__ float box_d2(float3 p, float3 lo, float3 hi) {
 }
 // Conservative slab interval: computed bounds widened by 1e-6 relative
 // (each bound carries at most three roundings).
+// SAFE: for rays with a zero direction component (inv = +-inf).  A ray with
+// d.x == 0 stays in the x slab of a box for every t if lo.x <= o.x <= hi.x
+// and never otherwise; (lo.x - o.x) * inv.x is +-inf except when the origin
+// lies on the plane (0 * inf = NaN), which then counts as inside the slab.
+template <bool SAFE = false>
 __device__ __forceinline__ void box_ray(float3 o, float3 inv, float3 lo, float3 hi, float& tn, float& tf) {
-    const float t0x = (lo.x - o.x) * inv.x, t1x = (hi.x - o.x) * inv.x;
-    const float t0y = (lo.y - o.y) * inv.y, t1y = (hi.y - o.y) * inv.y;
-    const float t0z = (lo.z - o.z) * inv.z, t1z = (hi.z - o.z) * inv.z;
+    float t0x = (lo.x - o.x) * inv.x, t1x = (hi.x - o.x) * inv.x;
+    float t0y = (lo.y - o.y) * inv.y, t1y = (hi.y - o.y) * inv.y;
+    float t0z = (lo.z - o.z) * inv.z, t1z = (hi.z - o.z) * inv.z;
+    if (SAFE) {
+        if (t0x != t0x) t0x = -inv.x;
+        if (t1x != t1x) t1x = inv.x;
+        if (t0y != t0y) t0y = -inv.y;
+        if (t1y != t1y) t1y = inv.y;
+        if (t0z != t0z) t0z = -inv.z;
+        if (t1z != t1z) t1z = inv.z;
+    }
     tn = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fminf(t0z, t1z));
     tf = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fmaxf(t0z, t1z));
     tn -= 1e-6f * fabsf(tn);
     tf += 1e-6f * fabsf(tf);
+}
+// 1/d per axis for box_ray; a ray with an infinite reciprocal (a zero or
+// subnormal direction component) must use box_ray<true>.
+__device__ __forceinline__ float3 ray_inv(float3 d) { return make_float3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z); }
+__device__ __forceinline__ bool ray_degenerate(float3 inv) { return isinf(inv.x) || isinf(inv.y) || isinf(inv.z); }
+
+// Any-hit traversal step: push the children of node nd that the ray (o, inv)
+// enters within [0, cull].
+template <bool SAFE>
+__device__ __forceinline__ void push_ray_children(const NodeView& nd, float3 o, float3 inv, float cull, int* st,
+                                                  int& sp) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const uint32_t m = meta_of(nd, j);
+        float3 lo, hi;
+        child_box(nd, j, lo, hi);
+        float tn, tf;
+        box_ray<SAFE>(o, inv, lo, hi, tn, tf);
+        if (m != kEmpty && tn <= tf && tf >= 0.f && tn <= cull) st[sp++] = child_ref(nd, m);
+    }
+}
+
+// Entry distance (as ordered bits) of the ray into each child of nd, kFull
+// where the ray does not need the child.
+template <bool SAFE>
+__device__ __forceinline__ void ray_child_keys(const NodeView& nd, float3 o, float3 inv, float cull, uint32_t k[8]) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        float3 lo, hi;
+        child_box(nd, j, lo, hi);
+        float tn, tf;
+        box_ray<SAFE>(o, inv, lo, hi, tn, tf);
+        const float key = fmaxf(tn, 0.f);
+        const bool need = meta_of(nd, j) != kEmpty && tn <= tf && tf >= 0.f && key <= cull;
+        k[j] = need ? __float_as_uint(key) : kFull;
+    }
 }
 __device__ __forceinline__ float cull_of(double best) { return __double2float_ru(dM(best, 1.000001)); }
 __device__ __forceinline__ void leaf_range(int ref, int& s0, int& s1) {
@@ -391,56 +440,22 @@ __global__ void __launch_bounds__(kQBlock) k_sign_watertight(Work w, const uint3
 }
 
 // --------------------------------------------------------------- raystab
-// Any hit with 0 <= t < tmax (FP32 filter, FP64 for undecided triangles).
-__device__ bool any_hit(const CNode* __restrict__ nodes, const CTri* __restrict__ tris, int root, float3 o,
-                        float3 d, double tmax) {
-    const float3 inv = make_float3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
-    const float dinf = f3inf(d);
-    const float tmaxf = (float)tmax;
-    const float cull = cull_of(tmax);
-    int st[kStack];
-    int sp = 0;
-    st[sp++] = root;
-    while (sp > 0) {
-        const int ref = st[--sp];
-        if (ref >= 0) {
-            const NodeView nd = load_node(nodes, ref);
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const uint32_t m = meta_of(nd, j);
-                float3 lo, hi;
-                child_box(nd, j, lo, hi);
-                float tn, tf;
-                box_ray(o, inv, lo, hi, tn, tf);
-                if (m != kEmpty && tn <= tf && tf >= 0.f && tn <= cull) st[sp++] = child_ref(nd, m);
-            }
-        } else {
-            int s0, s1;
-            leaf_range(ref, s0, s1);
-            for (int s = s0; s < s1; ++s) {
-                const TriV t = load_tri(tris, s);
-                float tt, terr;
-                const int r = ray_tri_f(o, d, dinf, t, tmaxf, &tt, &terr);
-                if (r == 1) return true;
-                if (r < 0) {
-                    double t64;
-                    if (ray_tri_d(to_d3(o), to_d3(d), to_d3(t.a), to_d3(t.b), to_d3(t.c), tmax, &t64)) return true;
-                }
-            }
-        }
-    }
-    return false;
-}
-
 // Negative iff all 64 stab rays (for k = 0..31: -d_k, then +d_k) hit the mesh
 // within [0, 1000) (src/bvh.cu:408-427); the first miss ends the query.
-// Queries are visited in Morton-cell order so neighbouring lanes trace
-// neighbouring origins.
+// Whether all rays hit does not depend on the order they are traced in.
+//
+// One loop walks the stack entries of all the query's rays: when a ray hits,
+// the lane starts its next ray in the same iteration, so lanes of a warp do
+// not wait for one another at the end of every ray (stab directions differ
+// from lane to lane, so the rays' lengths in steps do too).  Queries are
+// visited in Morton-cell order so neighbouring lanes share cached nodes.
 __global__ void __launch_bounds__(kQBlock) k_sign_raystab(Work w, const uint32_t* __restrict__ order,
                                                           const float* __restrict__ pts, float* __restrict__ dist,
                                                           const CNode* __restrict__ nodes,
                                                           const CTri* __restrict__ tris,
                                                           unsigned long long* __restrict__ ctr, int64_t grab) {
+    const float tmaxf = 1000.0f;
+    const float cull = cull_of(1000.0);
     PacketQueue pq(ctr, w.packets(), grab);
     for (int64_t pk = pq.take(); pk >= 0; pk = pq.take()) {
         int64_t start, qoff;
@@ -452,12 +467,48 @@ __global__ void __launch_bounds__(kQBlock) k_sign_raystab(Work w, const uint32_t
         const float3 p = load3(pts, idx);
         // the stab stream of a query is its index within its own call / mesh
         const float2 off = stab_offset((uint32_t)(idx - qoff));
+        uint32_t r = 0;  // ray r: -d_{r/2} for even r, +d_{r/2} for odd r
+        float3 sd = stab_dir(0, off);
+        float3 d = make_float3(-sd.x, -sd.y, -sd.z);
+        float3 inv = ray_inv(d);
+        bool degen = ray_degenerate(inv);
+        float dinf = f3inf(d);
+        int st[kStack];
+        int sp = 0;
+        st[sp++] = root;
         bool inside = true;
-        for (uint32_t k = 0; k < 32 && inside; ++k) {
-            const float3 dir = stab_dir(k, off);
-            if (!any_hit(nodes, tris, root, p, make_float3(-dir.x, -dir.y, -dir.z), 1000.0) ||
-                !any_hit(nodes, tris, root, p, dir, 1000.0))
-                inside = false;
+        while (true) {
+            if (sp == 0) { inside = false; break; }  // ray r missed
+            const int ref = st[--sp];
+            bool hit = false;
+            if (ref >= 0) {
+                const NodeView nd = load_node(nodes, ref);
+                if (degen) push_ray_children<true>(nd, p, inv, cull, st, sp);
+                else push_ray_children<false>(nd, p, inv, cull, st, sp);
+            } else {
+                int a, b;
+                leaf_range(ref, a, b);
+                for (int s = a; s < b && !hit; ++s) {
+                    const TriV t = load_tri(tris, s);
+                    float tt, terr;
+                    const int c = ray_tri_f(p, d, dinf, t, tmaxf, &tt, &terr);
+                    if (c == 1) hit = true;
+                    else if (c < 0) {
+                        double t64;
+                        hit = ray_tri_d(to_d3(p), to_d3(d), to_d3(t.a), to_d3(t.b), to_d3(t.c), 1000.0, &t64);
+                    }
+                }
+            }
+            if (hit) {
+                if (++r == 64) break;
+                if (r & 1) d = sd;
+                else { sd = stab_dir(r >> 1, off); d = make_float3(-sd.x, -sd.y, -sd.z); }
+                inv = ray_inv(d);
+                degen = ray_degenerate(inv);
+                dinf = f3inf(d);
+                sp = 0;
+                st[sp++] = root;
+            }
         }
         if (inside) dist[idx] = -dist[idx];
     }
@@ -483,7 +534,8 @@ __global__ void __launch_bounds__(kQBlock) k_ray(int64_t n, const float* __restr
         const bool act = q < n;
         const float3 o = act ? load3(ro, q) : make_float3(0.f, 0.f, 0.f);
         const float3 d = act ? load3(rd, q) : make_float3(1.f, 1.f, 1.f);
-        const float3 inv = make_float3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+        const float3 inv = ray_inv(d);
+        const bool degen = __any_sync(kFull, act && ray_degenerate(inv));  // warp-uniform
         const float dinf = f3inf(d);
         const d3 od = to_d3(o), dd = to_d3(d);
         float U = act ? 1000.0f : -1.f;             // MAX_DIST
@@ -511,15 +563,11 @@ __global__ void __launch_bounds__(kQBlock) k_ray(int64_t n, const float* __restr
             if (cur >= 0) {
                 const NodeView nd = load_node(nodes, cur);
                 uint32_t k[8];
+                if (degen) ray_child_keys<true>(nd, o, inv, cull, k);
+                else ray_child_keys<false>(nd, o, inv, cull, k);
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
-                    float3 lo, hi;
-                    child_box(nd, j, lo, hi);
-                    float tn, tf;
-                    box_ray(o, inv, lo, hi, tn, tf);
-                    const float key = fmaxf(tn, 0.f);
-                    const bool need = meta_of(nd, j) != kEmpty && tn <= tf && tf >= 0.f && key <= cull;
-                    const uint32_t kmin = __reduce_min_sync(kFull, need ? __float_as_uint(key) : kFull);
+                    const uint32_t kmin = __reduce_min_sync(kFull, k[j]);
                     k[j] = kmin != kFull ? ((kmin & ~7u) | (uint32_t)j) : kFull;
                 }
                 sort8(k);

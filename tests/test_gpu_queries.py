@@ -139,6 +139,29 @@ def test_ray_trace_inside_and_random(oracle, dev):
     assert out[0].shape == (6000, 3)
 
 
+def test_ray_trace_in_face_planes(oracle, dev):
+    """Rays with a zero direction component whose origin lies exactly on a
+    face plane of an axis-aligned cube (and so on a child box plane): they run
+    along the box face and hit the edges of the triangles there."""
+    v = np.array([[x, y, z] for x in (-1, 1) for y in (-1, 1) for z in (-1, 1)], np.float32)
+    quads = [(0, 1, 3, 2), (4, 6, 7, 5), (0, 4, 5, 1), (2, 3, 7, 6), (0, 2, 6, 4), (1, 5, 7, 3)]
+    f = np.array([t for a, b, c, d in quads for t in ((a, b, c), (a, c, d))], np.int64)
+    ro, rd = [], []
+    for ax in range(3):
+        u, w = (ax + 1) % 3, (ax + 2) % 3
+        for side in (-1.0, 1.0):
+            for x in np.linspace(-1.5, 1.5, 13):
+                for dirn in ((0.0, 1.0), (0.6, 0.8), (-0.28, 0.96)):
+                    o = np.zeros(3); o[ax] = side; o[u] = x; o[w] = -3.0
+                    d = np.zeros(3); d[u], d[w] = dirn
+                    ro.append(o); rd.append(d)
+    ro, rd = np.array(ro, np.float32), np.array(rd, np.float32)
+    bvh = cubvh.cuBVH(v, f)
+    out = bvh.ray_trace(torch.from_numpy(ro).to(dev), torch.from_numpy(rd).to(dev))
+    check_rays(oracle, v, f, ro, rd, out)
+    assert (_np(out[1]) >= 0).mean() > 0.3
+
+
 def check_sdf(got, sd_o, fid_o, what):
     d, fid, _ = (_np(x) if x is not None else None for x in got)
     assert np.array_equal(fid, fid_o), f"{what}: face ids differ at {(fid != fid_o).sum()} points"
