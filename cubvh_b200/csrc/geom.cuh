@@ -226,6 +226,10 @@ __device__ __forceinline__ float exp2i(int e) { return __int_as_float((e + 127) 
 // compiled into one translation unit only).
 static __constant__ double c_sin_coef[14];
 static __constant__ double c_cos_coef[14];
+// Lattice terms of direction k: (k + 1.33) / (31 + 2 * 1.33) at [k] and
+// k / golden ratio at [32 + k], float IEEE divisions done by the host (the
+// same values as computing them here); read per lane through L1.
+static __device__ float g_lattice[64];
 
 __device__ __forceinline__ void det_sincos(float phi, float* s, float* c) {
     const double x = (double)phi, x2 = dM(x, x);
@@ -263,11 +267,9 @@ __device__ __forceinline__ float2 stab_offset(uint32_t i) {
 }
 // Direction k of the 32-ray Fibonacci lattice (epsilon 1.33) with offset.
 __device__ __forceinline__ float3 stab_dir(uint32_t k, float2 off) {
-    const float eps = 1.33f;
-    const float den = __fadd_rn(31.0f, __fmul_rn(2.0f, eps));
-    float a = __fadd_rn(__fdiv_rn(__fadd_rn((float)k, eps), den), off.x);
+    float a = __fadd_rn(__ldg(&g_lattice[k]), off.x);
     a = __fsub_rn(a, floorf(a));
-    float b = __fadd_rn(__fdiv_rn((float)k, 1.6180339887498948482045868343656f), off.y);
+    float b = __fadd_rn(__ldg(&g_lattice[32 + k]), off.y);
     b = __fsub_rn(b, floorf(b));
     const float cos_t = __fadd_rn(__fmul_rn(-2.0f, a), 1.0f);
     const float phi = __fmul_rn(__fmul_rn(2.0f, 3.14159265358979323846f), __fsub_rn(b, 0.5f));

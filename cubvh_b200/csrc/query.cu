@@ -127,6 +127,17 @@ __device__ __forceinline__ void box_ray(float3 o, float3 inv, float3 lo, float3 
 // subnormal direction component) must use box_ray<true>.
 __device__ __forceinline__ float3 ray_inv(float3 d) { return make_float3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z); }
 __device__ __forceinline__ bool ray_degenerate(float3 inv) { return isinf(inv.x) || isinf(inv.y) || isinf(inv.z); }
+// 1/d with the hardware approximation (at most 1 ulp off: box_ray's 1e-6
+// widening covers it) for unit directions; zero and subnormal components
+// give +-inf, as ray_inv.
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float3 ray_inv_approx(float3 d) {
+    return make_float3(rcp_approx(d.x), rcp_approx(d.y), rcp_approx(d.z));
+}
 
 // Any-hit traversal step: push the children of node nd that the ray (o, inv)
 // enters within [0, cull].
@@ -184,6 +195,14 @@ struct PacketQueue {
         }
         const int64_t p = next++;
         return p < npk ? p : -1;
+    }
+    // the warp's next range of packets [b, e), false when done (warp-collective)
+    __device__ __forceinline__ bool take_range(int64_t& b, int64_t& e) {
+        unsigned long long v = 0;
+        if ((threadIdx.x & 31) == 0) v = atomicAdd(ctr, (unsigned long long)grab);
+        b = (int64_t)__shfl_sync(kFull, v, 0);
+        e = b + grab < npk ? b + grab : npk;
+        return b < npk;
     }
 };
 
@@ -444,41 +463,78 @@ __global__ void __launch_bounds__(kQBlock) k_sign_watertight(Work w, const uint3
 // within [0, 1000) (src/bvh.cu:408-427); the first miss ends the query.
 // Whether all rays hit does not depend on the order they are traced in.
 //
-// One loop walks the stack entries of all the query's rays: when a ray hits,
-// the lane starts its next ray in the same iteration, so lanes of a warp do
-// not wait for one another at the end of every ray (stab directions differ
-// from lane to lane, so the rays' lengths in steps do too).  Queries are
-// visited in Morton-cell order so neighbouring lanes share cached nodes.
+// Work is per lane, not per warp: a warp takes a chunk of packets (queries in
+// Morton-cell order) and each lane takes the chunk's next query from a
+// shared-memory counter whenever its own query ends, and starts its next
+// stab ray as soon as the current one hits.  Stab directions differ from
+// lane to lane and inside queries need 64 rays where outside ones end after a
+// few, so lanes never wait for one another except at the end of a chunk.
+// The per-query setup (query index, stab stream offset, root) is computed by
+// the whole warp in lockstep when the chunk is taken.
+constexpr int kChunkMax = 2;  // packets per raystab chunk
 __global__ void __launch_bounds__(kQBlock) k_sign_raystab(Work w, const uint32_t* __restrict__ order,
                                                           const float* __restrict__ pts, float* __restrict__ dist,
                                                           const CNode* __restrict__ nodes,
                                                           const CTri* __restrict__ tris,
                                                           unsigned long long* __restrict__ ctr, int64_t grab) {
+    __shared__ int s_next[kQBlock / 32];
+    __shared__ uint4 s_q[kQBlock / 32][kChunkMax * 32];  // query index, offset x/y bits, root (-1: none)
+    const int wib = threadIdx.x >> 5;
     const float tmaxf = 1000.0f;
     const float cull = cull_of(1000.0);
     PacketQueue pq(ctr, w.packets(), grab);
-    for (int64_t pk = pq.take(); pk >= 0; pk = pq.take()) {
-        int64_t start, qoff;
-        int cnt, root, s0;
-        w.get(pk, start, cnt, root, s0, qoff);
-        if ((int)(threadIdx.x & 31) >= cnt) continue;
-        const int64_t q = start + (threadIdx.x & 31);
-        const int64_t idx = order ? (int64_t)order[q] : q;
-        const float3 p = load3(pts, idx);
-        // the stab stream of a query is its index within its own call / mesh
-        const float2 off = stab_offset((uint32_t)(idx - qoff));
-        uint32_t r = 0;  // ray r: -d_{r/2} for even r, +d_{r/2} for odd r
-        float3 sd = stab_dir(0, off);
-        float3 d = make_float3(-sd.x, -sd.y, -sd.z);
-        float3 inv = ray_inv(d);
-        bool degen = ray_degenerate(inv);
-        float dinf = f3inf(d);
+    int64_t pk0, pk1;
+    while (pq.take_range(pk0, pk1)) {
+        const int total = (int)(pk1 - pk0) * 32;
+        for (int i = threadIdx.x & 31; i < total; i += 32) {
+            int64_t start, qoff;
+            int cnt, rt, s0;
+            w.get(pk0 + (i >> 5), start, cnt, rt, s0, qoff);
+            uint4 e = make_uint4(0u, 0u, 0u, 0xFFFFFFFFu);
+            if ((i & 31) < cnt) {
+                const int64_t qi = start + (i & 31);
+                const int64_t id = order ? (int64_t)order[qi] : qi;
+                // the stab stream of a query is its index within its own call / mesh
+                const float2 o2 = stab_offset((uint32_t)(id - qoff));
+                e = make_uint4((uint32_t)id, __float_as_uint(o2.x), __float_as_uint(o2.y), (uint32_t)rt);
+            }
+            s_q[wib][i] = e;
+        }
+        if ((threadIdx.x & 31) == 0) s_next[wib] = 0;
+        __syncwarp();
+        int64_t idx = -1;  // current query, -1: none
+        int root = 0;
+        float3 p = make_float3(0.f, 0.f, 0.f), sd = p, d = p, inv = p;
+        float2 off = make_float2(0.f, 0.f);
+        float dinf = 0.f;
+        bool degen = false;
+        uint32_t r = 0;    // ray r: -d_{r/2} for even r, +d_{r/2} for odd r
         int st[kStack];
         int sp = 0;
-        st[sp++] = root;
-        bool inside = true;
         while (true) {
-            if (sp == 0) { inside = false; break; }  // ray r missed
+            if (idx < 0) {
+                int i;
+                while ((i = atomicAdd(&s_next[wib], 1)) < total) {
+                    const uint4 e = s_q[wib][i];
+                    if (e.w != 0xFFFFFFFFu) {
+                        idx = e.x;
+                        off = make_float2(__uint_as_float(e.y), __uint_as_float(e.z));
+                        root = (int)e.w;
+                        break;
+                    }
+                }
+                if (idx < 0) break;
+                p = load3(pts, idx);
+                r = 0;
+                sd = stab_dir(0, off);
+                d = make_float3(-sd.x, -sd.y, -sd.z);
+                inv = ray_inv_approx(d);
+                degen = ray_degenerate(inv);
+                dinf = f3inf(d);
+                sp = 0;
+                st[sp++] = root;
+            }
+            if (sp == 0) { idx = -1; continue; }  // ray r missed: outside
             const int ref = st[--sp];
             bool hit = false;
             if (ref >= 0) {
@@ -500,17 +556,21 @@ __global__ void __launch_bounds__(kQBlock) k_sign_raystab(Work w, const uint32_t
                 }
             }
             if (hit) {
-                if (++r == 64) break;
+                if (++r == 64) {  // every ray hit: inside
+                    dist[idx] = -dist[idx];
+                    idx = -1;
+                    continue;
+                }
                 if (r & 1) d = sd;
                 else { sd = stab_dir(r >> 1, off); d = make_float3(-sd.x, -sd.y, -sd.z); }
-                inv = ray_inv(d);
+                inv = ray_inv_approx(d);
                 degen = ray_degenerate(inv);
                 dinf = f3inf(d);
                 sp = 0;
                 st[sp++] = root;
             }
         }
-        if (inside) dist[idx] = -dist[idx];
+        __syncwarp();
     }
 }
 
@@ -733,6 +793,15 @@ int64_t grab_for(int64_t n, unsigned grid) {
     const int64_t g = packets / (warps * 64);
     return g < 1 ? 1 : g;
 }
+// raystab chunk: kChunkMax packets (64 queries for 32 lanes: a lane whose
+// query ends early takes another one; larger chunks cost more in lane-by-lane
+// query setup than they save), one packet when the launch has fewer than two
+// packets per warp
+int64_t chunk_for(int64_t n, unsigned grid) {
+    const int64_t packets = (n + 31) / 32;
+    const int64_t warps = (int64_t)grid * (kQBlock / 32);
+    return packets >= (int64_t)kChunkMax * warps ? kChunkMax : 1;
+}
 }  // namespace
 
 cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts, float* dist, int64_t* fid,
@@ -773,7 +842,7 @@ cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts
         k_sign_watertight<<<g, kQBlock, 0, stream>>>(work, order, pts, dist, slots, nodes, tris, ctr + 1, grab_for(n, g));
     } else if (mode == 2) {
         const unsigned g = persistent_grid(k_sign_raystab, n);
-        k_sign_raystab<<<g, kQBlock, 0, stream>>>(work, order, pts, dist, nodes, tris, ctr + 1, grab_for(n, g));
+        k_sign_raystab<<<g, kQBlock, 0, stream>>>(work, order, pts, dist, nodes, tris, ctr + 1, chunk_for(n, g));
     }
     return cudaGetLastError();
 }
@@ -853,7 +922,7 @@ cudaError_t launch_arena_distance(const ArenaLaunch& a, const float* pts, float*
         const Work w{a.rs_packets, a.meshes, a.n_rs_packets, 0};
         const unsigned gr = persistent_grid(k_sign_raystab, 32 * a.n_rs_packets);
         k_sign_raystab<<<gr, kQBlock, 0, stream>>>(w, a.order, pts, dist, a.nodes, a.tris, a.counters + 2,
-                                                   grab_for(32 * a.n_rs_packets, gr));
+                                                   chunk_for(32 * a.n_rs_packets, gr));
     }
     return cudaGetLastError();
 }
@@ -867,9 +936,17 @@ cudaError_t upload_constants() {
         s[k] = -s[k - 1] / (double)((2 * k) * (2 * k + 1));
         c[k] = -c[k - 1] / (double)((2 * k - 1) * (2 * k));
     }
+    float lat[64];
+    const volatile float eps = 1.33f, phi = 1.6180339887498948482045868343656f;
+    const float den = 31.0f + 2.0f * eps;
+    for (int k = 0; k < 32; ++k) {
+        lat[k] = ((float)k + eps) / den;
+        lat[32 + k] = (float)k / phi;
+    }
     cudaError_t e = cudaMemcpyToSymbol(c_sin_coef, s, sizeof(s));
-    if (e != cudaSuccess) return e;
-    return cudaMemcpyToSymbol(c_cos_coef, c, sizeof(c));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_cos_coef, c, sizeof(c));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_lattice, lat, sizeof(lat));
+    return e;
 }
 
 }  // namespace cubvh
