@@ -57,7 +57,13 @@ __device__ __forceinline__ NodeView load_node(const CNode* __restrict__ nodes, i
     n.hy0 = w4.x; n.hy1 = w4.y; n.hz0 = w4.z; n.hz1 = w4.w;
     return n;
 }
-__device__ __forceinline__ uint32_t meta_of(const NodeView& n, int j) {
+// A node's links (what a warp-uniform traversal needs besides the boxes).
+struct NodeLinks {
+    int child_base, tri_base;
+    uint32_t meta0, meta1;
+};
+template <class N>
+__device__ __forceinline__ uint32_t meta_of(const N& n, int j) {
     return ((j < 4 ? n.meta0 : n.meta1) >> (8 * (j & 3))) & 0xFFu;
 }
 // byte k of w as a float: 0x4B0000qq is 2^23 + q, minus 2^23 is q exactly
@@ -76,9 +82,47 @@ __device__ __forceinline__ void child_box(const NodeView& n, int j, float3& lo, 
     hi.z = fmaf(qbyte(h ? n.hz1 : n.hz0, b), n.sz, n.oz);
 }
 // >= 0: internal node index; < 0: leaf, -(slot * 4 + count - 1) - 1
-__device__ __forceinline__ int child_ref(const NodeView& n, uint32_t m) {
+template <class N>
+__device__ __forceinline__ int child_ref(const N& n, uint32_t m) {
     if (m & 0x80u) return n.child_base + (int)(m & 7u);
     return -((((n.tri_base + (int)(m & 31u)) << 2) | (int)((m >> 5) & 3u)) + 1);
+}
+
+// Cooperative decode for warp-uniform traversals (every lane visits the same
+// node): lane l < 12 loads word l of the quantised bytes (coordinate l / 2 =
+// lo x, y, z, hi x, y, z of children 4 * (l % 2) .. + 3), decodes it as
+// child_box does and stores the floats in the warp's box table s (64 floats,
+// 16-byte aligned): child j at s[8j .. 8j + 7] = lo.xyz, -, hi.xyz, -.  The
+// whole warp then reads the boxes with broadcast loads instead of decoding
+// all 48 bounds in every lane.  Called by all lanes.
+__device__ __forceinline__ NodeLinks decode_node_warp(const CNode* __restrict__ nodes, int i, float* s) {
+    const int lane = threadIdx.x & 31;
+    const uint4* p = reinterpret_cast<const uint4*>(nodes + i);
+    const uint4 l = __ldg(p + 1);
+    uint4 h = make_uint4(0u, 0u, 0u, 0u);
+    uint32_t q = 0u;
+    if (lane < 12) {  // loads first: they do not wait for the table to be free
+        h = __ldg(p);
+        q = __ldg(reinterpret_cast<const uint32_t*>(p + 2) + lane);
+    }
+    __syncwarp();  // the previous node's boxes have been read
+    if (lane < 12) {
+        const int c = lane >> 1;
+        const int ax = c < 3 ? c : c - 3;
+        const float o = __uint_as_float(ax == 0 ? h.x : (ax == 1 ? h.y : h.z));
+        const float sc = exp2i((int)(int8_t)((h.w >> (8 * ax)) & 0xFFu));
+        float* d = s + 32 * (lane & 1) + (c < 3 ? c : c + 1);
+#pragma unroll
+        for (int b = 0; b < 4; ++b) d[8 * b] = fmaf(qbyte(q, b), sc, o);
+    }
+    __syncwarp();
+    return NodeLinks{(int)l.x, (int)l.y, l.z, l.w};
+}
+__device__ __forceinline__ void warp_box(const float* s, int j, float3& lo, float3& hi) {
+    const float4 a = *reinterpret_cast<const float4*>(s + 8 * j);
+    const float4 b = *reinterpret_cast<const float4*>(s + 8 * j + 4);
+    lo = make_float3(a.x, a.y, a.z);
+    hi = make_float3(b.x, b.y, b.z);
 }
 
 // Batcher odd-even merge sort network for 8 keys (19 comparators), ascending.
@@ -158,11 +202,12 @@ __device__ __forceinline__ void push_ray_children(const NodeView& nd, float3 o, 
 // Entry distance (as ordered bits) of the ray into each child of nd, kFull
 // where the ray does not need the child.
 template <bool SAFE>
-__device__ __forceinline__ void ray_child_keys(const NodeView& nd, float3 o, float3 inv, float cull, uint32_t k[8]) {
+__device__ __forceinline__ void ray_child_keys(const NodeLinks& nd, const float* sb, float3 o, float3 inv, float cull,
+                                               uint32_t k[8]) {
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         float3 lo, hi;
-        child_box(nd, j, lo, hi);
+        warp_box(sb, j, lo, hi);
         float tn, tf;
         box_ray<SAFE>(o, inv, lo, hi, tn, tf);
         const float key = fmaxf(tn, 0.f);
@@ -283,6 +328,8 @@ __global__ void __launch_bounds__(kQBlock) k_udf(Work w, const uint32_t* __restr
                                                  const CTri* __restrict__ tris,
                                                  unsigned long long* __restrict__ ctr, int64_t grab) {
     const int lane = threadIdx.x & 31;
+    __shared__ __align__(16) float s_box[kQBlock / 32][64];
+    float* sb = s_box[threadIdx.x >> 5];
     PacketQueue pq(ctr, w.packets(), grab);
     for (int64_t pk = pq.take(); pk >= 0; pk = pq.take()) {
         int64_t start, qoff;
@@ -292,7 +339,6 @@ __global__ void __launch_bounds__(kQBlock) k_udf(Work w, const uint32_t* __restr
         const bool act = lane < cnt;
         const int64_t idx = act ? (order ? (int64_t)order[qi] : qi) : 0;
         const float3 p = act ? load3(pts, idx) : make_float3(0.f, 0.f, 0.f);
-        const d3 pd = to_d3(p);
         // U: upper bound of the lane's nearest squared distance (MAX_DIST^2)
         float U = act ? 1e6f : -1.f;
         float cull = act ? U * 1.000002f : -1.f;
@@ -306,7 +352,7 @@ __global__ void __launch_bounds__(kQBlock) k_udf(Work w, const uint32_t* __restr
                 if (final_pass && cl[i] > U) continue;
                 const TriV t = load_tri(tris, cs[i]);
                 double bary[3]; d3 cp;
-                const double e = closest_on_tri_d(pd, to_d3(t.a), to_d3(t.b), to_d3(t.c), bary, &cp);
+                const double e = closest_on_tri_d(to_d3(p), to_d3(t.a), to_d3(t.b), to_d3(t.c), bary, &cp);
                 if (e < bx || (e == bx && (sx < 0 || t.id < ix))) { bx = e; sx = cs[i]; ix = t.id; }
             }
             nc = 0;
@@ -317,12 +363,12 @@ __global__ void __launch_bounds__(kQBlock) k_udf(Work w, const uint32_t* __restr
         bool live = __any_sync(kFull, act);
         while (live) {
             if (cur >= 0) {
-                const NodeView nd = load_node(nodes, cur);
+                const NodeLinks nd = decode_node_warp(nodes, cur, sb);
                 uint32_t k[8];
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
                     float3 lo, hi;
-                    child_box(nd, j, lo, hi);
+                    warp_box(sb, j, lo, hi);
                     const float d2 = box_d2(p, lo, hi);
                     const bool need = meta_of(nd, j) != kEmpty && d2 <= cull;
                     const uint32_t kmin = __reduce_min_sync(kFull, need ? __float_as_uint(d2) : kFull);
@@ -377,7 +423,7 @@ __global__ void __launch_bounds__(kQBlock) k_udf(Work w, const uint32_t* __restr
         if (UVW) {
             const TriV t = load_tri(tris, sx);
             double bary[3]; d3 cp;
-            closest_on_tri_d(pd, to_d3(t.a), to_d3(t.b), to_d3(t.c), bary, &cp);
+            closest_on_tri_d(to_d3(p), to_d3(t.a), to_d3(t.b), to_d3(t.c), bary, &cp);
             uvw[3 * idx] = __double2float_rn(bary[0]);
             uvw[3 * idx + 1] = __double2float_rn(bary[1]);
             uvw[3 * idx + 2] = __double2float_rn(bary[2]);
@@ -588,6 +634,8 @@ __global__ void __launch_bounds__(kQBlock) k_ray(int64_t n, const float* __restr
                                                  const CNode* __restrict__ nodes, const CTri* __restrict__ tris,
                                                  unsigned long long* __restrict__ ctr, int64_t grab) {
     const int lane = threadIdx.x & 31;
+    __shared__ __align__(16) float s_box[kQBlock / 32][64];
+    float* sb = s_box[threadIdx.x >> 5];
     PacketQueue pq(ctr, (n + 31) >> 5, grab);
     for (int64_t pk = pq.take(); pk >= 0; pk = pq.take()) {
         const int64_t q = pk * 32 + lane;
@@ -621,10 +669,10 @@ __global__ void __launch_bounds__(kQBlock) k_ray(int64_t n, const float* __restr
         bool live = __any_sync(kFull, act);
         while (live) {
             if (cur >= 0) {
-                const NodeView nd = load_node(nodes, cur);
+                const NodeLinks nd = decode_node_warp(nodes, cur, sb);
                 uint32_t k[8];
-                if (degen) ray_child_keys<true>(nd, o, inv, cull, k);
-                else ray_child_keys<false>(nd, o, inv, cull, k);
+                if (degen) ray_child_keys<true>(nd, sb, o, inv, cull, k);
+                else ray_child_keys<false>(nd, sb, o, inv, cull, k);
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
                     const uint32_t kmin = __reduce_min_sync(kFull, k[j]);
