@@ -118,6 +118,29 @@ __device__ __forceinline__ NodeLinks decode_node_warp(const CNode* __restrict__ 
     __syncwarp();
     return NodeLinks{(int)l.x, (int)l.y, l.z, l.w};
 }
+// Cooperative load of a leaf's triangles (slots s0 .. s1 - 1, at most four,
+// contiguous) into the warp's table: lane l < 3 * count loads 16-byte word l,
+// so the leaf costs one memory latency instead of one per triangle.  Called
+// by all lanes; the table is the box table (the two are used in turn).
+__device__ __forceinline__ void load_leaf_warp(const CTri* __restrict__ tris, int s0, int s1, float* s) {
+    const int lane = threadIdx.x & 31;
+    const bool ld = lane < 3 * (s1 - s0);
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (ld) v = __ldg(reinterpret_cast<const float4*>(tris + s0) + lane);
+    __syncwarp();  // the previous contents have been read
+    if (ld) reinterpret_cast<float4*>(s)[lane] = v;
+    __syncwarp();
+}
+// triangle i of the leaf in the warp's table
+__device__ __forceinline__ TriV warp_tri(const float* s, int i) {
+    const float4* p = reinterpret_cast<const float4*>(s) + 3 * i;
+    const float4 w0 = p[0], w1 = p[1], w2 = p[2];
+    TriV t;
+    t.a = make_float3(w0.x, w0.y, w0.z); t.id = __float_as_int(w0.w);
+    t.b = make_float3(w1.x, w1.y, w1.z); t.e2 = w1.w;
+    t.c = make_float3(w2.x, w2.y, w2.z); t.einf = w2.w;
+    return t;
+}
 __device__ __forceinline__ void warp_box(const float* s, int j, float3& lo, float3& hi) {
     const float4 a = *reinterpret_cast<const float4*>(s + 8 * j);
     const float4 b = *reinterpret_cast<const float4*>(s + 8 * j + 4);
@@ -383,8 +406,9 @@ __global__ void __launch_bounds__(kQBlock) k_udf(Work w, const uint32_t* __restr
             } else {
                 int s0, s1;
                 leaf_range(cur, s0, s1);
+                load_leaf_warp(tris, s0, s1, sb);
                 for (int s = s0; s < s1; ++s) {
-                    const TriV t = load_tri(tris, s);
+                    const TriV t = warp_tri(sb, s - s0);
                     float err;
                     const float e32 = tri_d2_f(p, t, &err);
                     const float lb = e32 - err;
@@ -687,8 +711,9 @@ __global__ void __launch_bounds__(kQBlock) k_ray(int64_t n, const float* __restr
             } else {
                 int s0, s1;
                 leaf_range(cur, s0, s1);
+                load_leaf_warp(tris, s0, s1, sb);
                 for (int s = s0; s < s1; ++s) {
-                    const TriV t = load_tri(tris, s);
+                    const TriV t = warp_tri(sb, s - s0);
                     float tt, terr;
                     const int r = ray_tri_f(o, d, dinf, t, 1000.0f, &tt, &terr);
                     const float lb = tt - terr;
