@@ -236,6 +236,8 @@ int cubvh_arena_set_queries(cubvh_arena* a, const int64_t* query_offsets, const 
     const size_t o_hist = off; off += al(sizeof(uint32_t) * (cells + 1));
     const size_t o_bsum = off; off += al(sizeof(uint32_t) * (scan::num_chunks(cells) + 1));
     const size_t o_slots = off; off += al(sizeof(int32_t) * std::max<int64_t>(Q, 1));
+    const int64_t hcap = heavy_cap_for(std::max<int64_t>(Q, 1));
+    const size_t o_heavy = off; off += al(sizeof(uint2) * hcap);
     std::lock_guard<std::mutex> lk(a->mu);
     if (a->d_layout) { cudaFree(a->d_layout); a->d_layout = nullptr; a->has_layout = false; }
     cudaError_t e = cudaMalloc(&a->d_layout, off);
@@ -266,6 +268,8 @@ int cubvh_arena_set_queries(cubvh_arena* a, const int64_t* query_offsets, const 
     L.hist = reinterpret_cast<uint32_t*>(base + o_hist);
     L.bsum = reinterpret_cast<uint32_t*>(base + o_bsum);
     L.slots = reinterpret_cast<int32_t*>(base + o_slots);
+    L.heavy = reinterpret_cast<uint2*>(base + o_heavy);
+    L.heavy_cap = hcap;
     a->n_queries = Q;
     a->has_layout = true;
     return CUBVH_OK;

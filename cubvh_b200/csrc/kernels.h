@@ -34,10 +34,12 @@ struct ArenaLaunch {
     const PacketDesc* rs_packets; int64_t n_rs_packets;  // raystab meshes
     unsigned long long* counters;      // 256 bytes
     uint32_t* order; uint32_t* hist; uint32_t* bsum; int32_t* slots;
+    uint2* heavy; int64_t heavy_cap;   // heavy-query list (heavy_cap_for(n_queries) entries)
 };
 cudaError_t launch_arena_distance(const ArenaLaunch& a, const float* pts, float* dist, int64_t* fid, float* uvw,
                                   cudaStream_t stream);
 int cell_bits_for(int64_t n);
+int64_t heavy_cap_for(int64_t n);
 
 // Point queries at least this many are visited in Morton-cell order.
 constexpr int64_t kSortMinQueries = 2048;

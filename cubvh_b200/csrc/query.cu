@@ -23,8 +23,10 @@
 //  * children are visited nearest-first (8 keys sorted as packed 32-bit
 //    integers); the nearest child is descended directly, the rest pushed on
 //    a local-memory stack with their lower-bound key, re-checked on pop.
+#include <climits>
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <math_constants.h>
 
 #include "geom.cuh"
 #include "kernels.h"
@@ -332,7 +334,9 @@ struct WarpStack {
     }
 };
 
-constexpr int kCand = 8;  // per-lane candidate list of the distance search
+constexpr int kCand = 8;         // per-lane candidate list of the distance search
+constexpr int kHeavyMinWork = 256;  // a packet is never handed off below this many visits
+
 
 // Exact nearest triangle of 32 Morton-adjacent points per warp (a packet):
 // the warp walks the union of the lanes' search paths with warp-uniform
@@ -343,13 +347,30 @@ constexpr int kCand = 8;  // per-lane candidate list of the distance search
 // bound), and a short list of triangles whose lower bound is within U.  At
 // the end every lane evaluates its surviving candidates in double: the
 // minimum (ties -> lowest face index) is the exact nearest triangle.
-template <bool UVW, bool SLOT>
+//
+// Tail control: a packet whose walk grows past a warp's fair share of the
+// launch (the mean node + leaf visits of the packets finished so far, in
+// stats[0] / stats[1], times the packets per warp `ppw`; at least
+// kHeavyMinWork) would hold the launch's tail alone: points deep inside a
+// closed mesh or near its medial axis are about equally far from very many
+// triangles.  Such a packet stops and appends its queries to the heavy list,
+// which k_udf_heavy serves with a warp per query.  When the list is full the
+// packet finishes here instead.
+//
+// The check costs registers in the traversal loop, so it is compiled in
+// (TAIL) only for launches with few packets per warp (below 24): with ppw packets per
+// warp at most one packet in ppw can pass the fair share, and only such
+// launches end on a few long packets.
+template <bool UVW, bool SLOT, bool TAIL>
 __global__ void __launch_bounds__(kQBlock) k_udf(Work w, const uint32_t* __restrict__ order,
                                                  const float* __restrict__ pts, float* __restrict__ dist,
                                                  int64_t* __restrict__ face_id, float* __restrict__ uvw,
                                                  int32_t* __restrict__ slot_out, const CNode* __restrict__ nodes,
                                                  const CTri* __restrict__ tris,
-                                                 unsigned long long* __restrict__ ctr, int64_t grab) {
+                                                 unsigned long long* __restrict__ ctr, int64_t grab,
+                                                 uint2* __restrict__ heavy, unsigned long long* __restrict__ n_heavy,
+                                                 int64_t heavy_cap, unsigned long long* __restrict__ stats,
+                                                 float ppw) {
     const int lane = threadIdx.x & 31;
     __shared__ __align__(16) float s_box[kQBlock / 32][64];
     float* sb = s_box[threadIdx.x >> 5];
@@ -384,7 +405,29 @@ __global__ void __launch_bounds__(kQBlock) k_udf(Work w, const uint32_t* __restr
         WarpStack st;
         int cur = root;
         bool live = __any_sync(kFull, act);
+        int work = 0;
+        bool handed_off = false;
         while (live) {
+            // warp-uniform; checked every 64 visits from kHeavyMinWork on
+            if (TAIL && (++work & 63) == 0 && work >= kHeavyMinWork) {
+                unsigned long long su = 0, np = 0;
+                if (lane == 0) {
+                    su = *reinterpret_cast<volatile unsigned long long*>(stats);
+                    np = *reinterpret_cast<volatile unsigned long long*>(stats + 1);
+                }
+                su = __shfl_sync(kFull, su, 0);
+                np = __shfl_sync(kFull, np, 0);
+                if (np >= 32 && (float)work > (float)su / (float)np * ppw) {
+                    unsigned long long b = 0;
+                    if (lane == 0) b = atomicAdd(n_heavy, (unsigned long long)cnt);
+                    b = __shfl_sync(kFull, b, 0);
+                    const uint32_t mesh = w.table ? (uint32_t)w.table[pk].mesh : 0u;
+                    if (act && (int64_t)b + lane < heavy_cap) heavy[b + lane] = make_uint2((uint32_t)idx, mesh);
+                    if ((int64_t)b + cnt <= heavy_cap) { handed_off = true; break; }
+                    // list full: finish the packet here (later checks append again; the list
+                    // length used is min(count, capacity))
+                }
+            }
             if (cur >= 0) {
                 const NodeLinks nd = decode_node_warp(nodes, cur, sb);
                 uint32_t k[8];
@@ -432,7 +475,11 @@ __global__ void __launch_bounds__(kQBlock) k_udf(Work w, const uint32_t* __restr
                 live = st.next(cullmax, cur);
             }
         }
-        if (!act) continue;
+        if (TAIL && !handed_off && lane == 0) {
+            atomicAdd(stats, (unsigned long long)work);
+            atomicAdd(stats + 1, 1ull);
+        }
+        if (handed_off || !act) continue;
         flush(true);
         double d64;
         if (sx < 0) {  // nothing within MAX_DIST: distance 0 on face 0
@@ -451,6 +498,222 @@ __global__ void __launch_bounds__(kQBlock) k_udf(Work w, const uint32_t* __restr
             uvw[3 * idx] = __double2float_rn(bary[0]);
             uvw[3 * idx + 1] = __double2float_rn(bary[1]);
             uvw[3 * idx + 2] = __double2float_rn(bary[2]);
+        }
+    }
+}
+
+
+// ---------------------------------------------------------- heavy queries
+// One warp per query handed off by k_udf.  Each step pops up to four live
+// nodes from a stack in shared memory (lane = child j of popped node i,
+// 8 * i + j), pushes the internal children within the bound and tests the
+// triangles of the leaf children 32 at a time, one per lane.  U (an upper
+// bound of the squared distance) and the candidate list are the warp's, and
+// candidates are settled in double exactly as in k_udf, so the result is the
+// same exact nearest triangle (lowest face index on ties).
+constexpr int kHStack = 512;
+constexpr int kHCand = 64;
+// Each step pushes at most 32 children one level below the deepest node it
+// popped, so the stack holds at most one such batch per tree level.
+static_assert(kHStack >= 32 * (kMaxDepth + 1), "heavy-query stack too small for the tree depth");
+struct HeavyWarp {
+    int ref[kHStack];
+    uint32_t key[kHStack];
+    int pop[4];
+    int tslot[4 * 32];
+    int cs[kHCand];
+    float cl[kHCand];
+};
+
+// Exact minimum (ties -> lowest face index) over the candidates i < nc whose
+// lower bound is <= lim, merged into (bx, sx, ix); warp-parallel, the result
+// is the same in every lane.
+__device__ void heavy_settle(const HeavyWarp& S, int nc, float lim, const CTri* __restrict__ tris, float3 p,
+                             double& bx, int& sx, int& ix) {
+    const int lane = threadIdx.x & 31;
+    double e = CUDART_INF;
+    int s = -1, id = INT_MAX;
+    for (int i = lane; i < nc; i += 32) {
+        if (S.cl[i] > lim) continue;
+        const int sl = S.cs[i];
+        const TriV t = load_tri(tris, sl);
+        double bary[3]; d3 cp;
+        const double d = closest_on_tri_d(to_d3(p), to_d3(t.a), to_d3(t.b), to_d3(t.c), bary, &cp);
+        if (d < e || (d == e && t.id < id)) { e = d; s = sl; id = t.id; }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double e2 = __shfl_xor_sync(kFull, e, o);
+        const int s2 = __shfl_xor_sync(kFull, s, o), id2 = __shfl_xor_sync(kFull, id, o);
+        if (e2 < e || (e2 == e && id2 < id)) { e = e2; s = s2; id = id2; }
+    }
+    if (s >= 0 && (e < bx || (e == bx && (sx < 0 || id < ix)))) { bx = e; sx = s; ix = id; }
+}
+
+template <bool UVW, bool SLOT>
+__global__ void __launch_bounds__(kQBlock) k_udf_heavy(const uint2* __restrict__ heavy,
+                                                       const unsigned long long* __restrict__ n_heavy,
+                                                       int64_t heavy_cap, const MeshDesc* __restrict__ meshes,
+                                                       int slot_face0, const float* __restrict__ pts,
+                                                       float* __restrict__ dist, int64_t* __restrict__ face_id,
+                                                       float* __restrict__ uvw, int32_t* __restrict__ slot_out,
+                                                       const CNode* __restrict__ nodes, const CTri* __restrict__ tris,
+                                                       unsigned long long* __restrict__ ctr) {
+    __shared__ HeavyWarp shw[kQBlock / 32];
+    HeavyWarp& S = shw[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int64_t nh_all = (int64_t)*n_heavy;
+    const int64_t nh = nh_all < heavy_cap ? nh_all : heavy_cap;
+    while (true) {
+        unsigned long long qi = 0;
+        if (lane == 0) qi = atomicAdd(ctr, 1ull);
+        qi = __shfl_sync(kFull, qi, 0);
+        if ((int64_t)qi >= nh) break;
+        const uint2 hq = heavy[qi];
+        const int64_t idx = hq.x;
+        int root = 0, s0 = slot_face0;
+        if (meshes) {
+            const MeshDesc md = meshes[hq.y];
+            root = md.root;
+            s0 = md.slot0;
+        }
+        const float3 p = load3(pts, idx);
+        float U = 1e6f;  // MAX_DIST^2
+        double bx = 1e6;
+        int sx = -1, ix = 0;
+        int nc = 0, sp = 1;
+        __syncwarp();  // the previous query is done with S
+        if (lane == 0) { S.ref[0] = root; S.key[0] = 0u; }
+        __syncwarp();
+        while (sp > 0) {
+            const float cull = U * 1.000002f;
+            // pop: of the top 32 entries, the first four (from the top) whose
+            // key is within the bound; the culled ones above them go too
+            const int pos = sp - 1 - lane;
+            const bool alive = pos >= 0 && S.key[pos] <= __float_as_uint(cull);
+            const unsigned m = __ballot_sync(kFull, alive);
+            int nn = __popc(m), used = sp < 32 ? sp : 32;
+            if (nn >= 4) {  // up to and including the fourth live entry
+                unsigned m4 = m;
+                m4 &= m4 - 1u;
+                m4 &= m4 - 1u;
+                m4 &= m4 - 1u;
+                used = __ffs(m4);
+                nn = 4;
+            }
+            if (alive && __popc(m & lt) < 4) S.pop[__popc(m & lt)] = S.ref[pos];
+            sp -= used;
+            __syncwarp();
+            // children of the popped nodes
+            const int ni = lane >> 3, j = lane & 7;
+            bool take = false, leaf = false;
+            int cref = 0;
+            uint32_t key = 0u;
+            if (ni < nn) {
+                const NodeView nd = load_node(nodes, S.pop[ni]);
+                const uint32_t mm = meta_of(nd, j);
+                if (mm != kEmpty) {
+                    float3 lo, hi;
+                    child_box(nd, j, lo, hi);
+                    const float d2 = box_d2(p, lo, hi);
+                    if (d2 <= cull) {
+                        take = true;
+                        key = __float_as_uint(d2);
+                        cref = child_ref(nd, mm);
+                        leaf = cref < 0;
+                    }
+                }
+            }
+            const unsigned mi = __ballot_sync(kFull, take && !leaf);
+            if (take && !leaf) {
+                const int q = sp + __popc(mi & lt);
+                S.ref[q] = cref;
+                S.key[q] = key;
+            }
+            sp += __popc(mi);
+            // the leaf children's triangles, 32 per round
+            int c = 0, a = 0;
+            if (take && leaf) {
+                int b;
+                leaf_range(cref, a, b);
+                c = b - a;
+            }
+            int incl = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(kFull, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const int T = __shfl_sync(kFull, incl, 31);
+            for (int i = 0; i < c; ++i) S.tslot[incl - c + i] = a + i;
+            __syncwarp();
+            for (int base = 0; base < T; base += 32) {
+                const int t = base + lane;
+                float e32 = 0.f, err = 0.f;
+                int slot = -1;
+                if (t < T) {
+                    slot = S.tslot[t];
+                    e32 = tri_d2_f(p, load_tri(tris, slot), &err);
+                }
+                const float ub = t < T ? e32 + err : CUDART_INF_F;
+                U = fminf(U, __uint_as_float(__reduce_min_sync(kFull, __float_as_uint(ub))));
+                const float lb = e32 - err;
+                const bool cand = t < T && lb <= U;
+                const unsigned mc = __ballot_sync(kFull, cand);
+                if (nc + __popc(mc) > kHCand) {  // warp-uniform: drop dead candidates, else settle them
+                    int keep = 0;
+                    for (int i0 = 0; i0 < nc; i0 += 32) {
+                        const int i = i0 + lane;
+                        const bool kp = i < nc && S.cl[i] <= U;
+                        const int cs_i = kp ? S.cs[i] : 0;
+                        const float cl_i = kp ? S.cl[i] : 0.f;
+                        const unsigned mk = __ballot_sync(kFull, kp);
+                        __syncwarp();  // every lane has read its entry
+                        if (kp) {
+                            S.cs[keep + __popc(mk & lt)] = cs_i;
+                            S.cl[keep + __popc(mk & lt)] = cl_i;
+                        }
+                        keep += __popc(mk);
+                        __syncwarp();
+                    }
+                    nc = keep;
+                    if (nc + __popc(mc) > kHCand) {
+                        heavy_settle(S, nc, CUDART_INF_F, tris, p, bx, sx, ix);
+                        U = fminf(U, __double2float_ru(bx));
+                        nc = 0;
+                        __syncwarp();
+                    }
+                }
+                if (cand) {
+                    S.cs[nc + __popc(mc & lt)] = slot;
+                    S.cl[nc + __popc(mc & lt)] = lb;
+                }
+                nc += __popc(mc);
+                __syncwarp();
+            }
+        }
+        heavy_settle(S, nc, U, tris, p, bx, sx, ix);
+        if (lane == 0) {
+            double d64;
+            if (sx < 0) {  // nothing within MAX_DIST: distance 0 on face 0
+                sx = s0;
+                d64 = 0.0;
+                ix = load_tri(tris, sx).id;
+            } else {
+                d64 = __dsqrt_rn(bx);
+            }
+            dist[idx] = __double2float_rn(d64);
+            face_id[idx] = (int64_t)ix;
+            if (SLOT) slot_out[idx] = sx;
+            if (UVW) {
+                const TriV t = load_tri(tris, sx);
+                double bary[3]; d3 cp;
+                closest_on_tri_d(to_d3(p), to_d3(t.a), to_d3(t.b), to_d3(t.c), bary, &cp);
+                uvw[3 * idx] = __double2float_rn(bary[0]);
+                uvw[3 * idx + 1] = __double2float_rn(bary[1]);
+                uvw[3 * idx + 2] = __double2float_rn(bary[2]);
+            }
         }
     }
 }
@@ -844,6 +1107,22 @@ int cell_bits(int64_t n) {
 
 }  // namespace
 
+// Heavy-query list length for n queries: a 32nd of them (at least 32768, at
+// most n); a full list only means packets finish in place.
+int64_t heavy_cap_for(int64_t n) {
+    const int64_t c = n / 32 > 32768 ? n / 32 : 32768;
+    return c < n ? c : n;
+}
+
+namespace {
+// launches with fewer packets per warp run k_udf with tail control
+constexpr float kTailPpw = 24.f;
+// packets per warp of a launch
+float packets_per_warp(int64_t packets, unsigned grid) {
+    return (float)packets / (float)((int64_t)grid * (kQBlock / 32));
+}
+}  // namespace
+
 size_t query_workspace_bytes(int mode, int64_t n) {
     size_t b = 256;                                               // packet counters
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
@@ -855,6 +1134,7 @@ size_t query_workspace_bytes(int mode, int64_t n) {
         b += al(sizeof(uint32_t) * 8);                            // query box
     }
     if (mode > 0) b += al(sizeof(int32_t) * n);                   // winning slots
+    if (mode >= 0) b += al(sizeof(uint2) * heavy_cap_for(n));     // heavy-query list
     return b;
 }
 
@@ -903,10 +1183,24 @@ cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts
         k_cell_scatter<<<g, 256, 0, stream>>>(n, pts, box, bits, hist, order);
     }
     int32_t* slots = mode != 0 ? reinterpret_cast<int32_t*>(w) : nullptr;
+    if (mode != 0) w += al(sizeof(int32_t) * n);
+    uint2* heavy = reinterpret_cast<uint2*>(w);
+    const int64_t hcap = heavy_cap_for(n);
     const Work work{nullptr, nullptr, n, slot_face0};
-#define CUBVH_L(U, S) do { const unsigned g_ = persistent_grid(k_udf<U, S>, n); \
-        k_udf<U, S><<<g_, kQBlock, 0, stream>>>(work, order, pts, dist, fid, uvw, slots, nodes, tris, \
-                                                ctr, grab_for(n, g_)); } while (0)
+#define CUBVH_L(U, S) do { const unsigned g_ = persistent_grid(k_udf<U, S, false>, n); \
+        const float ppw_ = packets_per_warp((n + 31) / 32, g_); \
+        if (ppw_ >= kTailPpw) { \
+            k_udf<U, S, false><<<g_, kQBlock, 0, stream>>>(work, order, pts, dist, fid, uvw, slots, nodes, tris, \
+                                                           ctr, grab_for(n, g_), heavy, ctr + 6, hcap, ctr + 8, ppw_); \
+        } else { \
+            const unsigned gt_ = persistent_grid(k_udf<U, S, true>, n); \
+            k_udf<U, S, true><<<gt_, kQBlock, 0, stream>>>(work, order, pts, dist, fid, uvw, slots, nodes, tris, \
+                                                           ctr, grab_for(n, gt_), heavy, ctr + 6, hcap, ctr + 8, \
+                                                           packets_per_warp((n + 31) / 32, gt_)); \
+            const unsigned gh_ = persistent_grid(k_udf_heavy<U, S>, 32 * hcap); \
+            k_udf_heavy<U, S><<<gh_, kQBlock, 0, stream>>>(heavy, ctr + 6, hcap, nullptr, slot_face0, pts, dist, \
+                                                           fid, uvw, slots, nodes, tris, ctr + 7); \
+        } } while (0)
     if (mode == 0) { if (want_uvw) CUBVH_L(true, false); else CUBVH_L(false, false); }
     else { if (want_uvw) CUBVH_L(true, true); else CUBVH_L(false, true); }
 #undef CUBVH_L
@@ -979,9 +1273,23 @@ cudaError_t launch_arena_distance(const ArenaLaunch& a, const float* pts, float*
     k_arena_scatter<<<g, 256, 0, stream>>>(a.n_queries, pts, a.qoff, a.n_meshes, a.sort, a.hist, a.order);
     const bool signed_any = a.n_wt_packets > 0 || a.n_rs_packets > 0;
     const Work all{a.packets, a.meshes, a.n_packets, 0};
-#define CUBVH_L(U, S) do { const unsigned g_ = persistent_grid(k_udf<U, S>, a.n_queries); \
-        k_udf<U, S><<<g_, kQBlock, 0, stream>>>(all, a.order, pts, dist, fid, uvw, a.slots, a.nodes, a.tris, \
-                                                a.counters, grab_for(a.n_queries, g_)); } while (0)
+#define CUBVH_L(U, S) do { const unsigned g_ = persistent_grid(k_udf<U, S, false>, a.n_queries); \
+        const float ppw_ = packets_per_warp(a.n_packets, g_); \
+        if (ppw_ >= kTailPpw) { \
+            k_udf<U, S, false><<<g_, kQBlock, 0, stream>>>(all, a.order, pts, dist, fid, uvw, a.slots, a.nodes, \
+                                                           a.tris, a.counters, grab_for(a.n_queries, g_), a.heavy, \
+                                                           a.counters + 6, a.heavy_cap, a.counters + 8, ppw_); \
+        } else { \
+            const unsigned gt_ = persistent_grid(k_udf<U, S, true>, a.n_queries); \
+            k_udf<U, S, true><<<gt_, kQBlock, 0, stream>>>(all, a.order, pts, dist, fid, uvw, a.slots, a.nodes, \
+                                                           a.tris, a.counters, grab_for(a.n_queries, gt_), a.heavy, \
+                                                           a.counters + 6, a.heavy_cap, a.counters + 8, \
+                                                           packets_per_warp(a.n_packets, gt_)); \
+            const unsigned gh_ = persistent_grid(k_udf_heavy<U, S>, 32 * a.heavy_cap); \
+            k_udf_heavy<U, S><<<gh_, kQBlock, 0, stream>>>(a.heavy, a.counters + 6, a.heavy_cap, a.meshes, 0, pts, \
+                                                           dist, fid, uvw, a.slots, a.nodes, a.tris, \
+                                                           a.counters + 7); \
+        } } while (0)
     if (uvw) { if (signed_any) CUBVH_L(true, true); else CUBVH_L(true, false); }
     else { if (signed_any) CUBVH_L(false, true); else CUBVH_L(false, false); }
 #undef CUBVH_L
