@@ -40,7 +40,13 @@ sys.path.insert(0, ROOT)
 METRIC = "mesh queries/s (ray_trace + signed_distance watertight), 1 B200"
 # launches of this library's kernels per op call (floodfill: zero status,
 # pack, count, 3 scan passes, runs, union, root, root label, write)
-KERNELS_PER_OP = {"ray": 1, "sdf_watertight": 1, "udf": 1, "udf_uvw": 1, "floodfill": 11}
+
+
+def _launches() -> int:
+    """Kernels launched so far by libcubvh_b200 in this process (the library
+    counts its own launches; torch's kernels are not included)."""
+    from cubvh_b200._lib import kernel_launches
+    return kernel_launches()
 
 
 # ----------------------------------------------------------------- helpers
@@ -345,12 +351,14 @@ def run_ours(args):
            for _ in range(args.steps)]
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
+    n_launch0 = _launches()
     with ClockSampler(local) as clk:
         t0.record(stream)
         for s in range(args.steps):
             step(kev[s])
         t1.record(stream)
         barrier()
+    gpu_launches = _launches() - n_launch0
     ms = t0.elapsed_time(t1)
     per_op_ms = [sum(kev[s][i][0].elapsed_time(kev[s][i][1]) for s in range(args.steps)) / args.steps
                  for i in range(len(dev_ops))]
@@ -442,7 +450,7 @@ def run_ours(args):
                          "algorithmic_bytes_per_launch": alg},
             "cpu_baseline": {"value": cpu_q / cpu_t, "unit": "queries/s", "cores": cpu_thr, "kind": "port",
                              "sample": cpu_desc},
-            "gpu_launches": args.steps * sum(KERNELS_PER_OP[o] for o, _, _, _ in dev_ops),
+            "gpu_launches": gpu_launches,
             "clocks": clk.summary(),
             "ops": ops_detail,
         }
@@ -559,8 +567,10 @@ def run_ours_fwd_bwd(args):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
+    n_launch0 = _launches()
     with ClockSampler(local) as clk:
         ms_step = _timed(step, args.steps, stream)
+    gpu_launches = _launches() - n_launch0
     ms_step = max_over_ranks(ms_step, dev)
     value = world * nq / (ms_step / 1e3)
     if args.workload == "batch_256":
@@ -606,14 +616,13 @@ def run_ours_fwd_bwd(args):
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
                          "algorithmic_bytes_per_launch": nq * io,
                          "note": "query I/O bytes only (no traversal bytes) for the fwd+bwd workloads"},
-            "cpu_baseline": None, "gpu_launches": None, "clocks": clk.summary(), "ops": extra,
+            "cpu_baseline": None, "gpu_launches": gpu_launches, "clocks": clk.summary(), "ops": extra,
         }
         if args.workload == "grad_displaced":
             wl = build_workload("grad_displaced")
             cq, ct, cthr, cdesc = cpu_time_sample(wl, 4 << 20)
             line["cpu_baseline"] = {"value": cq / ct, "unit": "queries/s", "cores": cthr, "kind": "port",
                                     "sample": cdesc + " (forward only: the reference has no backward)"}
-            line["gpu_launches"] = args.steps * 9
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.barrier()

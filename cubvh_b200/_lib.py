@@ -48,6 +48,7 @@ _SIGS = {
     "cubvh_distance_backward": [c_vp, c_vp, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp],
 }
 _STR_FUNCS = ("cubvh_version", "cubvh_last_error")
+_U64_FUNCS = ("cubvh_kernel_launches",)
 
 
 def lib():
@@ -67,12 +68,16 @@ def lib():
             fn = getattr(L, name)
             fn.argtypes = []
             fn.restype = ctypes.c_char_p
+        for name in _U64_FUNCS:
+            fn = getattr(L, name)
+            fn.argtypes = []
+            fn.restype = ctypes.c_uint64
         _lib = L
     return _lib
 
 
 def exported_symbols():
-    return list(_SIGS) + list(_STR_FUNCS)
+    return list(_SIGS) + list(_STR_FUNCS) + list(_U64_FUNCS)
 
 
 def check(rc: int, what: str):
@@ -83,3 +88,8 @@ def check(rc: int, what: str):
 
 def version() -> str:
     return lib().cubvh_version().decode()
+
+
+def kernel_launches() -> int:
+    """Kernels launched by the library in this process so far."""
+    return int(lib().cubvh_kernel_launches())

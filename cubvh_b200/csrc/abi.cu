@@ -13,6 +13,7 @@
 
 #include "../../include/cubvh_b200.h"
 #include "build.h"
+#include "launches.h"
 #include "kernels.h"
 
 using namespace cubvh;
@@ -134,9 +135,15 @@ int set_error(int code, const std::string& msg) { return fail(code, msg); }
         return fail(CUBVH_ERR_INVALID, "unknown error");                         \
     }
 
+namespace cubvh {
+std::atomic<uint64_t> g_kernel_launches{0};
+}  // namespace cubvh
+
 extern "C" {
 
 const char* cubvh_version(void) { return "cubvh_b200 0.1.0 (sm_100a)"; }
+
+uint64_t cubvh_kernel_launches(void) { return cubvh::g_kernel_launches.load(std::memory_order_relaxed); }
 
 const char* cubvh_last_error(void) { return g_err.c_str(); }
 

@@ -25,6 +25,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "launches.h"
 #include "kernels.h"
 #include "scan.cuh"
 
@@ -287,22 +288,22 @@ cudaError_t launch_floodfill(const uint8_t* grid, int B, int H, int W, int D, in
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const unsigned sgrid = (unsigned)nsm * 8;
 
-    k_zero<<<1, 1, 0, stream>>>(status);
+    k_zero<<<1, 1, 0, stream>>>(status); count_launch();
     if (W % 32 == 0 && (reinterpret_cast<uintptr_t>(grid) & 15) == 0) {
         const int64_t n16 = p.ntot / 16;
-        k_pack16<<<sgrid, 256, 0, stream>>>(reinterpret_cast<const uint4*>(grid), bits, n16);
+        k_pack16<<<sgrid, 256, 0, stream>>>(reinterpret_cast<const uint4*>(grid), bits, n16); count_launch();
     } else {
-        k_pack<<<sgrid, 256, 0, stream>>>(grid, bits, p.rows, W, p.wpr);
+        k_pack<<<sgrid, 256, 0, stream>>>(grid, bits, p.rows, W, p.wpr); count_launch();
     }
     const unsigned rgrid = (unsigned)((p.rows + 255) / 256);
-    k_count<<<rgrid, 256, 0, stream>>>(bits, wpref, rowoff, p.rows, p.wpr);
+    k_count<<<rgrid, 256, 0, stream>>>(bits, wpref, rowoff, p.rows, p.wpr); count_launch();
     scan::exclusive(rowoff, bsum, p.rows, stream);
-    k_runs<<<rgrid, 256, 0, stream>>>(bits, rowoff, start, parent, p.rows, p.wpr, W);
+    k_runs<<<rgrid, 256, 0, stream>>>(bits, rowoff, start, parent, p.rows, p.wpr, W); count_launch();
     const unsigned ugrid = (unsigned)((2 * p.rows + 255) / 256);
-    k_union<<<ugrid, 256, 0, stream>>>(bits, rowoff, wpref, parent, status, p.rows, p.wpr, H, D);
-    k_root<<<sgrid, 256, 0, stream>>>(parent, rowoff, p.rows, status);
-    k_root_label<<<sgrid, 256, 0, stream>>>(parent, start, rowoff, p.rows);
-    k_write<<<sgrid, 256, 0, stream>>>(bits, rowoff, wpref, parent, labels, p.rows, p.wpr, W);
+    k_union<<<ugrid, 256, 0, stream>>>(bits, rowoff, wpref, parent, status, p.rows, p.wpr, H, D); count_launch();
+    k_root<<<sgrid, 256, 0, stream>>>(parent, rowoff, p.rows, status); count_launch();
+    k_root_label<<<sgrid, 256, 0, stream>>>(parent, start, rowoff, p.rows); count_launch();
+    k_write<<<sgrid, 256, 0, stream>>>(bits, rowoff, wpref, parent, labels, p.rows, p.wpr, W); count_launch();
     return cudaGetLastError();
 }
 

@@ -15,6 +15,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "launches.h"
 #include "geom.cuh"
 #include "kernels.h"
 #include "scan.cuh"
@@ -251,11 +252,11 @@ __global__ void k_arena_backward_points(int64_t n, const float* __restrict__ pts
 cudaError_t launch_refit(int64_t n_tris, CTri* tris, const int32_t* face_vidx, const float* V, CNode* nodes,
                          float* node_box, const int32_t* level_start, int n_levels, cudaStream_t stream) {
     if (n_tris <= 0) return cudaSuccess;
-    k_refit_soup<<<(unsigned)((n_tris + 255) / 256), 256, 0, stream>>>(n_tris, tris, face_vidx, V);
+    k_refit_soup<<<(unsigned)((n_tris + 255) / 256), 256, 0, stream>>>(n_tris, tris, face_vidx, V); count_launch();
     for (int l = n_levels - 1; l >= 0; --l) {
         const int l0 = level_start[l], l1 = level_start[l + 1];
         if (l1 <= l0) continue;
-        k_refit_level<<<(unsigned)((l1 - l0 + 63) / 64), 64, 0, stream>>>(l0, l1, nodes, tris, node_box);
+        k_refit_level<<<(unsigned)((l1 - l0 + 63) / 64), 64, 0, stream>>>(l0, l1, nodes, tris, node_box); count_launch();
     }
     return cudaGetLastError();
 }
@@ -265,7 +266,7 @@ cudaError_t launch_arena_backward(int64_t n, const float* pts, const int64_t* fi
                                   const int32_t* gslot, const CTri* tris, float* gpts, cudaStream_t stream) {
     if (n <= 0) return cudaSuccess;
     k_arena_backward_points<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(n, pts, fid, gout, dist, qoff, M, face_off,
-                                                                             gslot, tris, gpts);
+                                                                             gslot, tris, gpts); count_launch();
     return cudaGetLastError();
 }
 
@@ -289,11 +290,11 @@ cudaError_t launch_backward(int64_t n, const float* pts, const int64_t* fid, con
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const unsigned g = (unsigned)nsm * 8;
-    k_face_hist<<<g, 256, 0, stream>>>(n, fid, nf, hist);
+    k_face_hist<<<g, 256, 0, stream>>>(n, fid, nf, hist); count_launch();
     scan::exclusive(hist, bsum, nf + 1, stream);
-    k_face_scatter<<<g, 256, 0, stream>>>(n, fid, nf, hist, order);
+    k_face_scatter<<<g, 256, 0, stream>>>(n, fid, nf, hist, order); count_launch();
     k_backward<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(n, order, pts, fid, gout, dist, V, fv, fslot, tris, nf,
-                                                                gpts, gV);
+                                                                gpts, gV); count_launch();
     return cudaGetLastError();
 }
 

@@ -28,6 +28,7 @@
 #include <cuda_runtime.h>
 #include <math_constants.h>
 
+#include "launches.h"
 #include "geom.cuh"
 #include "kernels.h"
 #include "scan.cuh"
@@ -1176,11 +1177,11 @@ cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts
         uint32_t* box = reinterpret_cast<uint32_t*>(w); w += al(sizeof(uint32_t) * 8);
         if ((e = cudaMemsetAsync(hist, 0, sizeof(uint32_t) * (cells + 1), stream)) != cudaSuccess) return e;
         const unsigned g = (unsigned)sm_count() * 8;
-        k_box_init<<<1, 32, 0, stream>>>(box);
-        k_box<<<g, 256, 0, stream>>>(n, pts, box);
-        k_cell_hist<<<g, 256, 0, stream>>>(n, pts, box, bits, hist);
+        k_box_init<<<1, 32, 0, stream>>>(box); count_launch();
+        k_box<<<g, 256, 0, stream>>>(n, pts, box); count_launch();
+        k_cell_hist<<<g, 256, 0, stream>>>(n, pts, box, bits, hist); count_launch();
         scan::exclusive(hist, bsum, cells, stream);
-        k_cell_scatter<<<g, 256, 0, stream>>>(n, pts, box, bits, hist, order);
+        k_cell_scatter<<<g, 256, 0, stream>>>(n, pts, box, bits, hist, order); count_launch();
     }
     int32_t* slots = mode != 0 ? reinterpret_cast<int32_t*>(w) : nullptr;
     if (mode != 0) w += al(sizeof(int32_t) * n);
@@ -1191,25 +1192,25 @@ cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts
         const float ppw_ = packets_per_warp((n + 31) / 32, g_); \
         if (ppw_ >= kTailPpw) { \
             k_udf<U, S, false><<<g_, kQBlock, 0, stream>>>(work, order, pts, dist, fid, uvw, slots, nodes, tris, \
-                                                           ctr, grab_for(n, g_), heavy, ctr + 6, hcap, ctr + 8, ppw_); \
+                                                           ctr, grab_for(n, g_), heavy, ctr + 6, hcap, ctr + 8, ppw_); count_launch(); \
         } else { \
             const unsigned gt_ = persistent_grid(k_udf<U, S, true>, n); \
             k_udf<U, S, true><<<gt_, kQBlock, 0, stream>>>(work, order, pts, dist, fid, uvw, slots, nodes, tris, \
                                                            ctr, grab_for(n, gt_), heavy, ctr + 6, hcap, ctr + 8, \
-                                                           packets_per_warp((n + 31) / 32, gt_)); \
+                                                           packets_per_warp((n + 31) / 32, gt_)); count_launch(); \
             const unsigned gh_ = persistent_grid(k_udf_heavy<U, S>, 32 * hcap); \
             k_udf_heavy<U, S><<<gh_, kQBlock, 0, stream>>>(heavy, ctr + 6, hcap, nullptr, slot_face0, pts, dist, \
-                                                           fid, uvw, slots, nodes, tris, ctr + 7); \
+                                                           fid, uvw, slots, nodes, tris, ctr + 7); count_launch(); \
         } } while (0)
     if (mode == 0) { if (want_uvw) CUBVH_L(true, false); else CUBVH_L(false, false); }
     else { if (want_uvw) CUBVH_L(true, true); else CUBVH_L(false, true); }
 #undef CUBVH_L
     if (mode == 1) {
         const unsigned g = persistent_grid(k_sign_watertight, n);
-        k_sign_watertight<<<g, kQBlock, 0, stream>>>(work, order, pts, dist, slots, nodes, tris, ctr + 1, grab_for(n, g));
+        k_sign_watertight<<<g, kQBlock, 0, stream>>>(work, order, pts, dist, slots, nodes, tris, ctr + 1, grab_for(n, g)); count_launch();
     } else if (mode == 2) {
         const unsigned g = persistent_grid(k_sign_raystab, n);
-        k_sign_raystab<<<g, kQBlock, 0, stream>>>(work, order, pts, dist, nodes, tris, ctr + 1, chunk_for(n, g));
+        k_sign_raystab<<<g, kQBlock, 0, stream>>>(work, order, pts, dist, nodes, tris, ctr + 1, chunk_for(n, g)); count_launch();
     }
     return cudaGetLastError();
 }
@@ -1221,7 +1222,7 @@ cudaError_t launch_ray(int64_t n, const float* ro, const float* rd, float* pos, 
     cudaError_t e = cudaMemsetAsync(ctr, 0, 256, stream);
     if (e != cudaSuccess) return e;
     const unsigned g = persistent_grid(k_ray, n);
-    k_ray<<<g, kQBlock, 0, stream>>>(n, ro, rd, pos, fid, depth, nodes, tris, ctr, grab_for(n, g));
+    k_ray<<<g, kQBlock, 0, stream>>>(n, ro, rd, pos, fid, depth, nodes, tris, ctr, grab_for(n, g)); count_launch();
     return cudaGetLastError();
 }
 
@@ -1268,9 +1269,9 @@ cudaError_t launch_arena_distance(const ArenaLaunch& a, const float* pts, float*
     if (e != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(a.hist, 0, sizeof(uint32_t) * (a.n_cells + 1), stream)) != cudaSuccess) return e;
     const unsigned g = (unsigned)sm_count() * 8;
-    k_arena_hist<<<g, 256, 0, stream>>>(a.n_queries, pts, a.qoff, a.n_meshes, a.sort, a.hist);
+    k_arena_hist<<<g, 256, 0, stream>>>(a.n_queries, pts, a.qoff, a.n_meshes, a.sort, a.hist); count_launch();
     scan::exclusive(a.hist, a.bsum, a.n_cells, stream);
-    k_arena_scatter<<<g, 256, 0, stream>>>(a.n_queries, pts, a.qoff, a.n_meshes, a.sort, a.hist, a.order);
+    k_arena_scatter<<<g, 256, 0, stream>>>(a.n_queries, pts, a.qoff, a.n_meshes, a.sort, a.hist, a.order); count_launch();
     const bool signed_any = a.n_wt_packets > 0 || a.n_rs_packets > 0;
     const Work all{a.packets, a.meshes, a.n_packets, 0};
 #define CUBVH_L(U, S) do { const unsigned g_ = persistent_grid(k_udf<U, S, false>, a.n_queries); \
@@ -1278,17 +1279,17 @@ cudaError_t launch_arena_distance(const ArenaLaunch& a, const float* pts, float*
         if (ppw_ >= kTailPpw) { \
             k_udf<U, S, false><<<g_, kQBlock, 0, stream>>>(all, a.order, pts, dist, fid, uvw, a.slots, a.nodes, \
                                                            a.tris, a.counters, grab_for(a.n_queries, g_), a.heavy, \
-                                                           a.counters + 6, a.heavy_cap, a.counters + 8, ppw_); \
+                                                           a.counters + 6, a.heavy_cap, a.counters + 8, ppw_); count_launch(); \
         } else { \
             const unsigned gt_ = persistent_grid(k_udf<U, S, true>, a.n_queries); \
             k_udf<U, S, true><<<gt_, kQBlock, 0, stream>>>(all, a.order, pts, dist, fid, uvw, a.slots, a.nodes, \
                                                            a.tris, a.counters, grab_for(a.n_queries, gt_), a.heavy, \
                                                            a.counters + 6, a.heavy_cap, a.counters + 8, \
-                                                           packets_per_warp(a.n_packets, gt_)); \
+                                                           packets_per_warp(a.n_packets, gt_)); count_launch(); \
             const unsigned gh_ = persistent_grid(k_udf_heavy<U, S>, 32 * a.heavy_cap); \
             k_udf_heavy<U, S><<<gh_, kQBlock, 0, stream>>>(a.heavy, a.counters + 6, a.heavy_cap, a.meshes, 0, pts, \
                                                            dist, fid, uvw, a.slots, a.nodes, a.tris, \
-                                                           a.counters + 7); \
+                                                           a.counters + 7); count_launch(); \
         } } while (0)
     if (uvw) { if (signed_any) CUBVH_L(true, true); else CUBVH_L(true, false); }
     else { if (signed_any) CUBVH_L(false, true); else CUBVH_L(false, false); }
@@ -1297,13 +1298,13 @@ cudaError_t launch_arena_distance(const ArenaLaunch& a, const float* pts, float*
         const Work w{a.wt_packets, a.meshes, a.n_wt_packets, 0};
         const unsigned gw = persistent_grid(k_sign_watertight, 32 * a.n_wt_packets);
         k_sign_watertight<<<gw, kQBlock, 0, stream>>>(w, a.order, pts, dist, a.slots, a.nodes, a.tris,
-                                                      a.counters + 1, grab_for(32 * a.n_wt_packets, gw));
+                                                      a.counters + 1, grab_for(32 * a.n_wt_packets, gw)); count_launch();
     }
     if (a.n_rs_packets > 0) {
         const Work w{a.rs_packets, a.meshes, a.n_rs_packets, 0};
         const unsigned gr = persistent_grid(k_sign_raystab, 32 * a.n_rs_packets);
         k_sign_raystab<<<gr, kQBlock, 0, stream>>>(w, a.order, pts, dist, a.nodes, a.tris, a.counters + 2,
-                                                   chunk_for(32 * a.n_rs_packets, gr));
+                                                   chunk_for(32 * a.n_rs_packets, gr)); count_launch();
     }
     return cudaGetLastError();
 }

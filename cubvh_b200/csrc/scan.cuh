@@ -3,6 +3,7 @@
 // of the chunk sums, per-chunk scans.  Scratch: (ceil(n / kScanChunk) + 1)
 // uint32 for the chunk sums.
 #pragma once
+#include "launches.h"
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -72,9 +73,9 @@ __global__ void k_apply(uint32_t* __restrict__ cnt, const uint32_t* __restrict__
 // cnt: n + 1 entries; bsum: num_chunks(n) + 1 entries.  n >= 1.
 inline void exclusive(uint32_t* cnt, uint32_t* bsum, int64_t n, cudaStream_t s) {
     const int64_t nblk = num_chunks(n);
-    k_chunk_sums<<<(unsigned)nblk, 256, 0, s>>>(cnt, bsum, n);
-    k_top<<<1, 1024, 0, s>>>(bsum, nblk);
-    k_apply<<<(unsigned)nblk, 1024, 0, s>>>(cnt, bsum, n);
+    k_chunk_sums<<<(unsigned)nblk, 256, 0, s>>>(cnt, bsum, n); count_launch();
+    k_top<<<1, 1024, 0, s>>>(bsum, nblk); count_launch();
+    k_apply<<<(unsigned)nblk, 1024, 0, s>>>(cnt, bsum, n); count_launch();
 }
 
 }  // namespace

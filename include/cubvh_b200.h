@@ -39,6 +39,11 @@ const char* cubvh_version(void);
 /* Message of the last failed call on this thread ("" if none). */
 const char* cubvh_last_error(void);
 
+/* Number of CUDA kernels this library has launched in the process so far
+ * (counted on the host at each launch; replays of a CUDA graph that captured
+ * them are not counted).  For measurement; no counterpart in the reference. */
+uint64_t cubvh_kernel_launches(void);
+
 /* Build a BVH on the host from an indexed mesh; touches no GPU (the device
  * copy is made by the first query on each device).
  * vertices: float32 [n_vertices, 3] (host); faces: int64 [n_faces, 3] (host),
