@@ -1,7 +1,8 @@
 """Throughput benchmark of the cubvh query path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload rays_displaced|udf_icosphere|dense_tori]
+                    [--workload rays_displaced|udf_icosphere|dense_tori|raystab_displaced|
+                                grad_displaced|batch_256]
 
 Default workload (``rays_displaced``): displaced icosphere level 6 (81,920
 faces); one step = ray_trace of 33,554,432 camera rays (8 poses x 2048^2,
@@ -166,6 +167,16 @@ def build_workload(name: str, res: int = 2048, sdf_points: int = 8 << 20):
         return dict(name=name, vertices=w["vertices"], faces=w["faces"], ops=[("udf", (w["points"],))],
                     desc="displaced icosphere L6 (81,920 faces); 4,194,304 points (half U[-1,1]^3, half "
                          "+-0.05 of the surface); fwd + bwd w.r.t. points and vertices")
+    if name == "raystab_displaced":
+        v, f = W.displaced_icosphere(6, 1)
+        lo, hi = v.min(0), v.max(0)
+        c, h = (lo + hi) / 2, (hi - lo) / 2 * 1.1
+        p = (c + np.random.default_rng(5).uniform(-1, 1, (2 << 20, 3)) * h).astype(np.float32)
+        # ~3,000 box and ~1,300 triangle tests per query in the reference
+        # traversal: a 512k-query CPU sample keeps that leg near 10-20 s
+        return dict(name=name, vertices=v, faces=f, ops=[("sdf_raystab", (p,))], cpu_sample=1 << 19,
+                    desc="displaced icosphere L6 (81,920 faces); 2,097,152 raystab SDF points uniform in the "
+                         "bounding box dilated by 10% (the batched workload's query distribution)")
     if name == "batch_256":
         raise SystemExit("batch_256 has no single-mesh CPU view")
     raise SystemExit(f"unknown workload {name}")
@@ -178,7 +189,7 @@ def n_queries(op, args):
 
 
 def io_bytes_per_query(op):
-    return {"ray": 48, "sdf_watertight": 24, "udf": 24, "udf_uvw": 36}.get(op, 0)
+    return {"ray": 48, "sdf_watertight": 24, "sdf_raystab": 24, "udf": 24, "udf_uvw": 36}.get(op, 0)
 
 
 def traversal_counts(wl, sample_stride=64):
@@ -194,9 +205,9 @@ def traversal_counts(wl, sample_stride=64):
             ro, rd = args[0][::sample_stride], args[1][::sample_stride]
             *_, c = ref.ray_trace(ro, rd, count=True)
             n = len(ro)
-        elif op == "sdf_watertight":
+        elif op in ("sdf_watertight", "sdf_raystab"):
             p = args[0][::sample_stride]
-            *_, c = ref.signed_distance(p, mode=0, count=True)
+            *_, c = ref.signed_distance(p, mode=0 if op == "sdf_watertight" else 1, count=True)
             n = len(p)
         else:
             p = args[0][::sample_stride]
@@ -228,8 +239,8 @@ def cpu_time_sample(wl, max_queries, threads=None):
         else:
             p = np.ascontiguousarray(args[0][::stride])
             t0 = time.perf_counter()
-            if op == "sdf_watertight":
-                ref.signed_distance(p, mode=0)
+            if op in ("sdf_watertight", "sdf_raystab"):
+                ref.signed_distance(p, mode=0 if op == "sdf_watertight" else 1)
             else:
                 ref.unsigned_distance(p, return_uvw=(op == "udf_uvw"))
             dt = time.perf_counter() - t0
@@ -297,7 +308,7 @@ def run_ours(args):
             fn = (lambda ro=ro, rd=rd, n=n, o=outs: check(
                 L.cubvh_ray_trace(h, P(ro), P(rd), n, P(o[0]), P(o[1]), P(o[2]), sp), "ray_trace"))
             dev_ops.append((op, n, fn, "ray: k_ray"))
-        elif op in ("sdf_watertight", "udf", "udf_uvw"):
+        elif op in ("sdf_watertight", "sdf_raystab", "udf", "udf_uvw"):
             p = torch.from_numpy(a[0]).to(dev)
             n = p.shape[0]
             d = torch.empty(n, device=dev); fid = torch.empty(n, dtype=torch.int64, device=dev)
@@ -307,6 +318,10 @@ def run_ours(args):
                 fn = (lambda p=p, n=n, d=d, fid=fid: check(
                     L.cubvh_signed_distance(h, P(p), n, 0, P(d), P(fid), ctypes.c_void_p(0), sp), "sdf"))
                 kname = "sdf_watertight: Morton bucketing + k_udf<0,1> + k_sign_watertight"
+            elif op == "sdf_raystab":
+                fn = (lambda p=p, n=n, d=d, fid=fid: check(
+                    L.cubvh_signed_distance(h, P(p), n, 1, P(d), P(fid), ctypes.c_void_p(0), sp), "sdf"))
+                kname = "sdf_raystab: Morton bucketing + k_udf<0,1> + k_sign_raystab"
             else:
                 fn = (lambda p=p, n=n, d=d, fid=fid, u=uptr: check(
                     L.cubvh_unsigned_distance(h, P(p), n, P(d), P(fid), u, sp), "udf"))
@@ -383,6 +398,8 @@ def run_ours(args):
                 res = bvh.ray_trace(tensors[0], tensors[1])
             elif op == "sdf_watertight":
                 res = bvh.signed_distance(tensors[0], mode="watertight")
+            elif op == "sdf_raystab":
+                res = bvh.signed_distance(tensors[0], mode="raystab")
             else:
                 res = bvh.unsigned_distance(tensors[0], return_uvw=(op == "udf_uvw"))
             for j, r in enumerate(res):
@@ -424,7 +441,7 @@ def run_ours(args):
             nb_, nt_ = counts[op]
             alg = n * (io_bytes_per_query(op) + 24.0 * nb_ + 36.0 * nt_)
         achieved = alg / (per_op_ms[dom] / 1e3) / 1e9
-        cpu_q, cpu_t, cpu_thr, cpu_desc = cpu_time_sample(wl, 16 << 20)
+        cpu_q, cpu_t, cpu_thr, cpu_desc = cpu_time_sample(wl, wl.get("cpu_sample", 16 << 20))
         ops_detail = {}
         for i, (o, nq, _, kn) in enumerate(dev_ops):
             d = {"kernel": kn, "ms_per_launch": per_op_ms[i]}
@@ -636,7 +653,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="rays_displaced",
-                    choices=["rays_displaced", "udf_icosphere", "dense_tori", "grad_displaced", "batch_256"])
+                    choices=["rays_displaced", "udf_icosphere", "dense_tori", "raystab_displaced",
+                             "grad_displaced", "batch_256"])
     ap.add_argument("--adam-steps", type=int, default=200, help="grad_displaced: sphere-fitting steps")
     ap.add_argument("--meshes", type=int, default=256, help="batch_256: number of meshes")
     ap.add_argument("--res", type=int, default=2048, help="camera resolution (rays_displaced)")

@@ -227,6 +227,45 @@ __device__ __forceinline__ void push_ray_children(const NodeView& nd, float3 o, 
 
 // Entry distance (as ordered bits) of the ray into each child of nd, kFull
 // where the ray does not need the child.
+// The same step for a ray without zero direction components, with the
+// node's affine decode folded into the ray: along axis a the plane of byte q
+// is met at t = (origin_a + q * s_a - o_a) * inv_a, computed as
+// fma(q, A_a, B_a) with A_a = s_a * inv_a and B_a = (origin_a - o_a) * inv_a.
+// Against the decoded plane (itself origin + q * s rounded once) this is off
+// by less than 6 * 2^-24 * S_a, S_a = |origin_a * inv_a| + 255 |A_a| + |B_a|
+// (inv from the hardware reciprocal, within 1 ulp), so entries are computed
+// with B_a - E_a and exits with B_a + E_a, E_a = 1e-6 * S_a (about 16 * 2^-24
+// * S_a).  The ray's direction signs fix which of a child's two planes is
+// the near one on each axis, so no per-child min / max is needed.
+__device__ __forceinline__ void push_ray_children_affine(const NodeView& nd, float3 o, float3 inv, float cull,
+                                                         int* st, int& sp) {
+    const float ax = nd.sx * inv.x, ay = nd.sy * inv.y, az = nd.sz * inv.z;
+    const float bx = (nd.ox - o.x) * inv.x, by = (nd.oy - o.y) * inv.y, bz = (nd.oz - o.z) * inv.z;
+    const float ex = 1e-6f * (fabsf(nd.ox * inv.x) + 255.f * fabsf(ax) + fabsf(bx));
+    const float ey = 1e-6f * (fabsf(nd.oy * inv.y) + 255.f * fabsf(ay) + fabsf(by));
+    const float ez = 1e-6f * (fabsf(nd.oz * inv.z) + 255.f * fabsf(az) + fabsf(bz));
+    const float nbx = bx - ex, fbx = bx + ex, nby = by - ey, fby = by + ey, nbz = bz - ez, fbz = bz + ez;
+    const bool px = inv.x >= 0.f, py = inv.y >= 0.f, pz = inv.z >= 0.f;
+    // near / far quantised words per axis (children 0-3, 4-7)
+    const uint32_t nx0 = px ? nd.lx0 : nd.hx0, nx1 = px ? nd.lx1 : nd.hx1;
+    const uint32_t fx0 = px ? nd.hx0 : nd.lx0, fx1 = px ? nd.hx1 : nd.lx1;
+    const uint32_t ny0 = py ? nd.ly0 : nd.hy0, ny1 = py ? nd.ly1 : nd.hy1;
+    const uint32_t fy0 = py ? nd.hy0 : nd.ly0, fy1 = py ? nd.hy1 : nd.ly1;
+    const uint32_t nz0 = pz ? nd.lz0 : nd.hz0, nz1 = pz ? nd.lz1 : nd.hz1;
+    const uint32_t fz0 = pz ? nd.hz0 : nd.lz0, fz1 = pz ? nd.hz1 : nd.lz1;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const uint32_t m = meta_of(nd, j);
+        const int b = j & 3;
+        const bool h = j >= 4;
+        const float tn = fmaxf(fmaxf(fmaf(qbyte(h ? nx1 : nx0, b), ax, nbx), fmaf(qbyte(h ? ny1 : ny0, b), ay, nby)),
+                               fmaf(qbyte(h ? nz1 : nz0, b), az, nbz));
+        const float tf = fminf(fminf(fmaf(qbyte(h ? fx1 : fx0, b), ax, fbx), fmaf(qbyte(h ? fy1 : fy0, b), ay, fby)),
+                               fmaf(qbyte(h ? fz1 : fz0, b), az, fbz));
+        if (m != kEmpty && tn <= tf && tf >= 0.f && tn <= cull) st[sp++] = child_ref(nd, m);
+    }
+}
+
 template <bool SAFE>
 __device__ __forceinline__ void ray_child_keys(const NodeLinks& nd, const float* sb, float3 o, float3 inv, float cull,
                                                uint32_t k[8]) {
@@ -874,7 +913,7 @@ __global__ void __launch_bounds__(kQBlock) k_sign_raystab(Work w, const uint32_t
             if (ref >= 0) {
                 const NodeView nd = load_node(nodes, ref);
                 if (degen) push_ray_children<true>(nd, p, inv, cull, st, sp);
-                else push_ray_children<false>(nd, p, inv, cull, st, sp);
+                else push_ray_children_affine(nd, p, inv, cull, st, sp);
             } else {
                 int a, b;
                 leaf_range(ref, a, b);
