@@ -39,8 +39,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "mesh queries/s (ray_trace + signed_distance watertight), 1 B200"
-# launches of this library's kernels per op call (floodfill: zero status,
-# pack, count, 3 scan passes, runs, union, root, root label, write)
+# ops over a voxel grid (no query count, no traversal)
+GRID_OPS = ("floodfill", "udf_to_sdf")
 
 
 def _launches() -> int:
@@ -160,8 +160,9 @@ def build_workload(name: str, res: int = 2048, sdf_points: int = 8 << 20):
     if name == "dense_tori":
         w = W.dense_tori()
         g = W.dense_grid(w["grid_res"])
-        return dict(name=name, vertices=w["vertices"], faces=w["faces"], ops=[("udf", (g,)), ("floodfill", (512,))],
-                    desc="12 tori (174,778 faces, 10% removed); UDF on the 512^3 grid + floodfill of udf < 2/512")
+        return dict(name=name, vertices=w["vertices"], faces=w["faces"], ops=[("udf", (g,)), ("floodfill", (512,)), ("udf_to_sdf", (512,))],
+                    desc="12 tori (174,778 faces, 10% removed); UDF on the 512^3 grid + floodfill of udf < 2/512 "
+                         "+ the fused udf -> sdf step (occupancy, floodfill, signs)")
     if name == "grad_displaced":
         w = W.grad_displaced()
         return dict(name=name, vertices=w["vertices"], faces=w["faces"], ops=[("udf", (w["points"],))],
@@ -183,7 +184,7 @@ def build_workload(name: str, res: int = 2048, sdf_points: int = 8 << 20):
 
 
 def n_queries(op, args):
-    if op == "floodfill":
+    if op in GRID_OPS:
         return 0
     return len(args[0])
 
@@ -199,7 +200,7 @@ def traversal_counts(wl, sample_stride=64):
     ref = O.RefBVH(wl["vertices"], wl["faces"])
     out = {}
     for op, args in wl["ops"]:
-        if op == "floodfill":
+        if op in GRID_OPS:
             continue
         if op == "ray":
             ro, rd = args[0][::sample_stride], args[1][::sample_stride]
@@ -226,11 +227,11 @@ def cpu_time_sample(wl, max_queries, threads=None):
     if threads:
         O.set_threads(threads)
     ref = O.RefBVH(wl["vertices"], wl["faces"])
-    total = sum(len(a[0]) for op, a in wl["ops"] if op != "floodfill")
+    total = sum(len(a[0]) for op, a in wl["ops"] if op not in GRID_OPS)
     stride = max(1, -(-total // int(max_queries)))
     q, t, parts = 0, 0.0, []
     for op, args in wl["ops"]:
-        if op == "floodfill":
+        if op in GRID_OPS:
             continue
         if op == "ray":
             ro, rd = np.ascontiguousarray(args[0][::stride]), np.ascontiguousarray(args[1][::stride])
@@ -329,6 +330,17 @@ def run_ours(args):
             dev_ops.append((op, n, fn, kname))
             if args.workload == "dense_tori":
                 occ_src = d
+        elif op == "udf_to_sdf":
+            res = a[0]
+            sdf_out = torch.empty(res, res, res, device=dev)
+            nb = ctypes.c_size_t()
+            check(L.cubvh_floodfill_workspace_size(1, res, res, res, ctypes.byref(nb)), "ws")
+            ws2 = torch.empty(nb.value, dtype=torch.uint8, device=dev)
+
+            def fn(res=res, out=sdf_out, ws=ws2, nb=nb.value):
+                check(L.cubvh_udf_to_sdf(P(occ_src), 1, res, res, res, ctypes.c_float(2.0 / res), P(out), P(ws), nb,
+                                         sp), "udf_to_sdf")
+            dev_ops.append((op, 0, fn, "udf_to_sdf: pack of udf < eps, floodfill passes, signed write"))
         elif op == "floodfill":
             res = a[0]
             grid = torch.empty(res, res, res, dtype=torch.bool, device=dev)
@@ -383,7 +395,7 @@ def run_ours(args):
     # ---- e2e through the public API from pinned host buffers
     host_in = []
     for op, a in wl["ops"]:
-        if op == "floodfill":
+        if op in GRID_OPS:
             continue
         host_in.append((op, [torch.from_numpy(x).pin_memory() for x in a]))
     e2e_steps = max(2, min(args.steps, 5))
@@ -435,8 +447,8 @@ def run_ours(args):
         peak, peak_kind = _peaks()
         dom = max(range(len(dev_ops)), key=lambda i: per_op_ms[i])
         op, n, _, kname = dev_ops[dom]
-        if op == "floodfill":
-            alg = 5.0 * 512 ** 3
+        if op in GRID_OPS:  # floodfill: 1 B in + 4 B out per voxel; udf_to_sdf: 4 B in + 4 B out
+            alg = (5.0 if op == "floodfill" else 8.0) * 512 ** 3
         else:
             nb_, nt_ = counts[op]
             alg = n * (io_bytes_per_query(op) + 24.0 * nb_ + 36.0 * nt_)

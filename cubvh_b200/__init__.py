@@ -6,10 +6,11 @@
     sdf, face_id, _ = bvh.signed_distance(points, mode="watertight")
     pos, face_id, depth = bvh.ray_trace(rays_o, rays_d)
     labels = cubvh.floodfill(occupancy)
+    sdf = cubvh.udf_to_sdf(udf_grid)     # occupancy -> floodfill -> signed grid, fused
 """
 
 from ._lib import version
-from .api import cuBVH, floodfill
+from .api import cuBVH, floodfill, udf_to_sdf
 from .arena import BVHArena
 
-__all__ = ["cuBVH", "floodfill", "BVHArena", "version"]
+__all__ = ["cuBVH", "floodfill", "udf_to_sdf", "BVHArena", "version"]

@@ -38,6 +38,7 @@ _SIGS = {
     "cubvh_floodfill_workspace_size": [c_int, c_int, c_int, c_int, ctypes.POINTER(c_sz)],
     "cubvh_floodfill": [c_vp, c_int, c_int, c_int, c_int, c_vp, c_vp, c_sz, c_vp],
     "cubvh_floodfill_check": [c_vp, c_int, c_int, c_int, c_int, c_vp],
+    "cubvh_udf_to_sdf": [c_vp, c_int, c_int, c_int, c_int, ctypes.c_float, c_vp, c_vp, c_sz, c_vp],
     "cubvh_bvh_refit": [c_vp, c_vp, c_i64, c_vp],
     "cubvh_arena_create": [ctypes.c_int32, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(c_vp)],
     "cubvh_arena_destroy": [c_vp],

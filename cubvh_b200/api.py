@@ -266,3 +266,41 @@ def floodfill(grid, check_bounds: bool = False):
         if check_bounds:
             check(lib().cubvh_floodfill_check(_ptr(ws), B, H, W, D, stream), "floodfill")
     return mask.squeeze(0) if squeeze else mask
+
+
+def udf_to_sdf(udf, eps: float = None, check_bounds: bool = False):
+    """Signed distance grid from an unsigned distance grid, in one fused
+    floodfill pass: the occupancy -> SDF step of the reference's watertight
+    recipe (test/benchmark_watertight.py:89-143, readme.md:95-102), which the
+    reference runs as torch ops around ``floodfill``:
+
+        occ = udf < eps; labels = floodfill(occ)
+        outside = labels == labels[0, 0, 0]            # per volume
+        sdf = udf - eps; sdf[~outside & (sdf > 0)] *= -1
+
+    udf: float32 [B, H, W, D] or [H, W, D] (a UDF sampled on a grid).
+    eps: occupancy threshold; default 2 / resolution, resolution = the last
+    dimension (the reference's 2-voxel tolerance for a res^3 grid).
+    Returns float32 of the same shape.  Results equal the composition above
+    bit for bit (voxel labels as ``floodfill``)."""
+    udf = udf.float().contiguous()
+    if not udf.is_cuda: udf = udf.cuda()
+    squeeze = udf.dim() == 3
+    if squeeze:
+        udf = udf.unsqueeze(0)
+    if udf.dim() != 4:
+        raise RuntimeError(f"udf_to_sdf expects [B, H, W, D] or [H, W, D], got {tuple(udf.shape)}")
+    B, H, W, D = (int(s) for s in udf.shape)
+    if eps is None:
+        eps = 2.0 / D
+    sdf = torch.empty_like(udf)
+    with torch.cuda.device(udf.device):
+        nbytes = ctypes.c_size_t()
+        check(lib().cubvh_floodfill_workspace_size(B, H, W, D, ctypes.byref(nbytes)), "udf_to_sdf")
+        ws = torch.empty(max(int(nbytes.value), 1), dtype=torch.uint8, device=udf.device)
+        stream = _stream_ptr(udf.device)
+        check(lib().cubvh_udf_to_sdf(_ptr(udf), B, H, W, D, ctypes.c_float(eps), _ptr(sdf), _ptr(ws),
+                                     int(nbytes.value), stream), "udf_to_sdf")
+        if check_bounds:
+            check(lib().cubvh_floodfill_check(_ptr(ws), B, H, W, D, stream), "udf_to_sdf")
+    return sdf.squeeze(0) if squeeze else sdf

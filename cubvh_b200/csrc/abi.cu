@@ -363,6 +363,34 @@ int cubvh_floodfill(const uint8_t* grid, int B, int H, int W, int D, int32_t* la
     CUBVH_GUARD_END
 }
 
+int cubvh_udf_to_sdf(const float* udf, int B, int H, int W, int D, float eps, float* sdf, void* workspace,
+                     size_t workspace_bytes, void* stream) {
+    CUBVH_GUARD_BEGIN
+    int rc = check_grid_dims(B, H, W, D);
+    if (rc != CUBVH_OK) return rc;
+    if ((int64_t)B * H * W * D == 0) return CUBVH_OK;
+    if (!udf || !sdf) return fail(CUBVH_ERR_INVALID, "udf/sdf is null");
+    if (!(eps == eps)) return fail(CUBVH_ERR_INVALID, "eps is NaN");
+    const size_t need = floodfill_workspace_bytes(B, H, W, D);
+    cudaStream_t s = (cudaStream_t)stream;
+    void* ws = workspace;
+    cudaError_t e;
+    if (ws) {
+        if (workspace_bytes < need) return fail(CUBVH_ERR_INVALID, "workspace smaller than cubvh_floodfill_workspace_size()");
+        if (reinterpret_cast<uintptr_t>(ws) & 255) return fail(CUBVH_ERR_INVALID, "workspace must be 256-byte aligned");
+    } else if ((e = cudaMallocAsync(&ws, need, s)) != cudaSuccess) {
+        return cuda_fail(e, "cudaMallocAsync(udf_to_sdf workspace)");
+    }
+    e = launch_udf_to_sdf(udf, B, H, W, D, eps, sdf, ws, s);
+    if (!workspace) {
+        const cudaError_t e2 = cudaFreeAsync(ws, s);
+        if (e == cudaSuccess) e = e2;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "udf_to_sdf launch");
+    return CUBVH_OK;
+    CUBVH_GUARD_END
+}
+
 int cubvh_floodfill_check(const void* workspace, int B, int H, int W, int D, void* stream) {
     CUBVH_GUARD_BEGIN
     if (!workspace) return fail(CUBVH_ERR_INVALID, "workspace is null");

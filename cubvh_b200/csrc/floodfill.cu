@@ -97,6 +97,24 @@ __global__ void k_pack16(const uint4* __restrict__ grid, uint32_t* __restrict__ 
     }
 }
 
+// 1'. free mask of an unsigned-distance grid thresholded at eps: a voxel is
+// occupied iff udf < eps (a NaN distance is free, as !(NaN < eps))
+__global__ void k_pack_udf(const float* __restrict__ udf, uint32_t* __restrict__ bits, int64_t rows, int W,
+                           int64_t wpr, float eps) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t words = rows * wpr;
+    for (int64_t w = warp; w < words; w += nwarps) {
+        const int64_t r = w / wpr;
+        const int x = (int)(w - r * wpr) * 32 + lane;
+        bool fr = false;
+        if (x < W) fr = !(__ldg(udf + r * W + x) < eps);
+        const uint32_t m = __ballot_sync(0xFFFFFFFFu, fr);
+        if (lane == 0) bits[w] = m;
+    }
+}
+
 __device__ __forceinline__ uint32_t starts_of(uint32_t f, uint32_t prev_word) {
     return f & ~((f << 1) | (prev_word >> 31));
 }
@@ -264,7 +282,65 @@ __global__ void k_write(const uint32_t* __restrict__ bits, const uint32_t* __res
     }
 }
 
+// 5'. signed distances instead of labels: s = udf - eps, negated where the
+// voxel's label (-1 when occupied) differs from the label of its volume's
+// first voxel (b, 0, 0, 0) and s > 0.  Same traversal of the run tables as
+// k_write; the first voxel's label is its row's first run when it is free.
+__global__ void k_write_sdf(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ rowoff,
+                            const uint32_t* __restrict__ wpref, const int32_t* __restrict__ runlab,
+                            const float* __restrict__ udf, float* __restrict__ sdf, int64_t rows, int64_t wpr,
+                            int W, int64_t rows_per_volume, float eps) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t words = rows * wpr;
+    const uint32_t below = (lane == 31) ? 0xFFFFFFFFu : ((2u << lane) - 1u);
+    for (int64_t w0 = warp * 32; w0 < words; w0 += nwarps * 32) {
+        const int64_t wk = w0 + lane;
+        uint32_t f = 0, s = 0, base = 0;
+        int32_t empty = -1;
+        if (wk < words) {
+            const int64_t r = wk / wpr, wi = wk - r * wpr;
+            f = bits[wk];
+            const uint32_t prev = wi > 0 ? bits[wk - 1] : 0u;
+            s = starts_of(f, prev);
+            base = rowoff[r] + wpref[wk];
+            const int64_t r0 = (r / rows_per_volume) * rows_per_volume;
+            if (bits[r0 * wpr] & 1u) empty = __ldg(runlab + rowoff[r0]);
+        }
+        const int nw = (int)min((int64_t)32, words - w0);
+        for (int k = 0; k < nw; ++k) {
+            const uint32_t fk = __shfl_sync(0xFFFFFFFFu, f, k);
+            const uint32_t sk = __shfl_sync(0xFFFFFFFFu, s, k);
+            const uint32_t bk = __shfl_sync(0xFFFFFFFFu, base, k);
+            const int32_t ek = __shfl_sync(0xFFFFFFFFu, empty, k);
+            const int64_t wg = w0 + k;
+            const int64_t r = wg / wpr;
+            const int x = (int)(wg - r * wpr) * 32 + lane;
+            if (x < W) {
+                int32_t lab = -1;
+                if ((fk >> lane) & 1u) lab = __ldg(runlab + (bk + __popc(sk & below) - 1));
+                const float d = __fsub_rn(__ldcs(udf + r * W + x), eps);
+                __stcs(sdf + r * W + x, (lab != ek && d > 0.f) ? -d : d);
+            }
+        }
+    }
+}
+
 __global__ void k_zero(int* p) { *p = 0; }
+
+// 2-5a. runs, union-find over adjacent rows, run labels (parent[] := label)
+void label_runs(const FFPlan& p, int H, int D, uint32_t* bits, uint32_t* wpref, uint32_t* rowoff, uint32_t* bsum,
+                int32_t* start, int32_t* parent, int* status, unsigned sgrid, cudaStream_t stream) {
+    const unsigned rgrid = (unsigned)((p.rows + 255) / 256);
+    k_count<<<rgrid, 256, 0, stream>>>(bits, wpref, rowoff, p.rows, p.wpr); count_launch();
+    scan::exclusive(rowoff, bsum, p.rows, stream);
+    k_runs<<<rgrid, 256, 0, stream>>>(bits, rowoff, start, parent, p.rows, p.wpr, (int)(p.ntot / p.rows)); count_launch();
+    const unsigned ugrid = (unsigned)((2 * p.rows + 255) / 256);
+    k_union<<<ugrid, 256, 0, stream>>>(bits, rowoff, wpref, parent, status, p.rows, p.wpr, H, D); count_launch();
+    k_root<<<sgrid, 256, 0, stream>>>(parent, rowoff, p.rows, status); count_launch();
+    k_root_label<<<sgrid, 256, 0, stream>>>(parent, start, rowoff, p.rows); count_launch();
+}
 
 }  // namespace
 
@@ -295,15 +371,33 @@ cudaError_t launch_floodfill(const uint8_t* grid, int B, int H, int W, int D, in
     } else {
         k_pack<<<sgrid, 256, 0, stream>>>(grid, bits, p.rows, W, p.wpr); count_launch();
     }
-    const unsigned rgrid = (unsigned)((p.rows + 255) / 256);
-    k_count<<<rgrid, 256, 0, stream>>>(bits, wpref, rowoff, p.rows, p.wpr); count_launch();
-    scan::exclusive(rowoff, bsum, p.rows, stream);
-    k_runs<<<rgrid, 256, 0, stream>>>(bits, rowoff, start, parent, p.rows, p.wpr, W); count_launch();
-    const unsigned ugrid = (unsigned)((2 * p.rows + 255) / 256);
-    k_union<<<ugrid, 256, 0, stream>>>(bits, rowoff, wpref, parent, status, p.rows, p.wpr, H, D); count_launch();
-    k_root<<<sgrid, 256, 0, stream>>>(parent, rowoff, p.rows, status); count_launch();
-    k_root_label<<<sgrid, 256, 0, stream>>>(parent, start, rowoff, p.rows); count_launch();
+    label_runs(p, H, D, bits, wpref, rowoff, bsum, start, parent, status, sgrid, stream);
     k_write<<<sgrid, 256, 0, stream>>>(bits, rowoff, wpref, parent, labels, p.rows, p.wpr, W); count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_udf_to_sdf(const float* udf, int B, int H, int W, int D, float eps, float* sdf, void* ws,
+                              cudaStream_t stream) {
+    const FFPlan p = make_plan(B, H, W, D);
+    if (p.ntot <= 0) return cudaSuccess;
+    char* base = static_cast<char*>(ws);
+    uint32_t* bits = reinterpret_cast<uint32_t*>(base + p.off_bits);
+    uint32_t* wpref = reinterpret_cast<uint32_t*>(base + p.off_wpref);
+    uint32_t* rowoff = reinterpret_cast<uint32_t*>(base + p.off_rowoff);
+    uint32_t* bsum = reinterpret_cast<uint32_t*>(base + p.off_blocksum);
+    int32_t* start = reinterpret_cast<int32_t*>(base + p.off_start);
+    int32_t* parent = reinterpret_cast<int32_t*>(base + p.off_parent);
+    int* status = reinterpret_cast<int*>(base + p.off_status);
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const unsigned sgrid = (unsigned)nsm * 8;
+
+    k_zero<<<1, 1, 0, stream>>>(status); count_launch();
+    k_pack_udf<<<sgrid, 256, 0, stream>>>(udf, bits, p.rows, W, p.wpr, eps); count_launch();
+    label_runs(p, H, D, bits, wpref, rowoff, bsum, start, parent, status, sgrid, stream);
+    k_write_sdf<<<sgrid, 256, 0, stream>>>(bits, rowoff, wpref, parent, udf, sdf, p.rows, p.wpr, W,
+                                           (int64_t)D * H, eps); count_launch();
     return cudaGetLastError();
 }
 

@@ -70,6 +70,10 @@ cudaError_t launch_backward(int64_t n, const float* pts, const int64_t* fid, con
 size_t floodfill_workspace_bytes(int B, int H, int W, int D);
 cudaError_t launch_floodfill(const uint8_t* grid, int B, int H, int W, int D, int32_t* labels,
                              void* workspace, cudaStream_t stream);
+// Floodfill of the occupancy udf < eps with a signed-distance epilogue
+// (same workspace as launch_floodfill).
+cudaError_t launch_udf_to_sdf(const float* udf, int B, int H, int W, int D, float eps, float* sdf,
+                              void* workspace, cudaStream_t stream);
 // Offset of the int32 status word inside the floodfill workspace.
 size_t floodfill_status_offset(int B, int H, int W, int D);
 // Floodfill with the library's fixed scratch array (floodfill_noalloc.cu).

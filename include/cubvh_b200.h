@@ -179,6 +179,19 @@ int cubvh_floodfill(const uint8_t* grid, int B, int H, int W, int D, int32_t* la
  * that last used `workspace` (same B, H, W, D) hit a device-side bound. */
 int cubvh_floodfill_check(const void* workspace, int B, int H, int W, int D, void* stream);
 
+/* Signed distance grid from an unsigned one, fused into the floodfill (the
+ * occupancy -> SDF step of the reference's watertight recipe,
+ * test/benchmark_watertight.py:89-143 and readme.md:95-102, which the
+ * reference does in torch around floodfill).  udf float32 [B, H, W, D]
+ * (device); sdf float32 of the same shape (may not alias udf).  For each
+ * volume b: occupied = udf < eps; labels = floodfill(occupied);
+ * s = udf - eps (float32); sdf = -s where the voxel's label (-1 when
+ * occupied) differs from the label of voxel (b, 0, 0, 0) and s > 0, else s.
+ * Workspace, asynchrony and cubvh_floodfill_check as cubvh_floodfill (same
+ * size: cubvh_floodfill_workspace_size). */
+int cubvh_udf_to_sdf(const float* udf, int B, int H, int W, int D, float eps, float* sdf, void* workspace,
+                     size_t workspace_bytes, void* stream);
+
 /* Floodfill for callers that must not allocate GPU memory during the call
  * (code running inside another framework's memory pool or arena that forbids
  * cudaMalloc / cudaFree, or loops that must never touch the allocator).  No

@@ -155,6 +155,25 @@ def floodfill(grid):
     return out[0] if squeeze else out
 
 
+def udf_to_sdf(udf, eps):
+    """The reference's occupancy -> SDF recipe (test/benchmark_watertight.py:
+    98-143, readme.md:95-102) on float32 numpy grids [B,H,W,D] or [H,W,D]:
+    occ = udf < eps, labels = floodfill(occ), the component of voxel (0,0,0)
+    of each volume is outside, sdf = udf - eps negated on the other voxels
+    where it is > 0."""
+    u = np.asarray(udf, np.float32)
+    squeeze = u.ndim == 3
+    if squeeze:
+        u = u[None]
+    lab = floodfill(u < np.float32(eps))
+    s = u - np.float32(eps)
+    out = s.copy()
+    for b in range(u.shape[0]):
+        inner = (lab[b] != lab[b, 0, 0, 0]) & (s[b] > 0)
+        out[b][inner] = -s[b][inner]
+    return out[0] if squeeze else out
+
+
 # ------------------------------------------------- FP32 mirror of the reference
 class RefBVH:
     """FP32 restatement of the reference's BVH4 build + traversals (CPU)."""

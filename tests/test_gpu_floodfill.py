@@ -57,3 +57,41 @@ def test_floodfill_occupancy_pipeline(oracle, dev):
 def test_floodfill_rejects_non_bool(dev):
     with pytest.raises(RuntimeError):
         cubvh.floodfill(torch.zeros(4, 4, 4, dtype=torch.int32, device=dev))
+
+
+@pytest.mark.parametrize("shape", [(32, 32, 32), (2, 24, 17, 40), (1, 9, 64, 7), (3, 16, 16, 16)])
+def test_udf_to_sdf_random(oracle, dev, shape):
+    """Fused occupancy -> floodfill -> signed grid against the reference recipe
+    (oracle floodfill + the same float32 arithmetic), bit for bit; includes
+    volumes whose first voxel is occupied and NaN distances."""
+    rng = np.random.default_rng(sum(shape))
+    u = rng.random(shape).astype(np.float32)
+    u[rng.random(shape) < 0.35] = 0.0           # occupied walls
+    if len(shape) == 4:
+        u[-1, 0, 0, 0] = 0.0                    # last volume: first voxel occupied
+    u.reshape(-1)[rng.choice(u.size, 5, replace=False)] = np.nan
+    eps = 0.05
+    got = cubvh.udf_to_sdf(torch.from_numpy(u).to(dev), eps=eps, check_bounds=True).cpu().numpy()
+    want = oracle.udf_to_sdf(u, eps)
+    assert got.dtype == np.float32 and got.shape == u.shape
+    assert np.array_equal(got, want, equal_nan=True)
+
+
+def test_udf_to_sdf_sphere_grid(oracle, dev):
+    """The reference pipeline on a mesh: dense UDF of a sphere on a 64^3
+    grid, then the signed grid; the same as torch ops around floodfill, and
+    negative inside the sphere."""
+    v, f = W.icosphere(3, 0.6)
+    res = 64
+    g = torch.linspace(-1, 1, res, device=dev)
+    pts = torch.stack(torch.meshgrid(g, g, g, indexing="ij"), -1).view(-1, 3)
+    udf = cubvh.cuBVH(v, f).unsigned_distance(pts)[0].view(res, res, res)
+    eps = 2.0 / res
+    sdf = cubvh.udf_to_sdf(udf)
+    lab = cubvh.floodfill(udf < eps)
+    ref = udf - eps
+    inner = (lab != lab[0, 0, 0]) & (ref > 0)
+    ref[inner] *= -1
+    assert torch.equal(sdf, ref)
+    r = pts.norm(dim=1).view(res, res, res)
+    assert (sdf[r < 0.4] < 0).all() and (sdf[r > 0.8] > 0).all()

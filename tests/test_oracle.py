@@ -194,3 +194,22 @@ def test_ref32_mirror_tracks_fp64(oracle):
     assert (df - d64).max() < 2e-7
     nodes, tris = ref.state_dict_arrays()
     assert nodes.shape == (1365, 9) and tris.shape == (5120, 12)
+
+
+def test_udf_to_sdf_known_answer():
+    """Hollow box: a 6^3 shell of occupied voxels (udf 0) around a 4^3
+    cavity (udf 1) inside an 10^3 grid whose outside voxels have udf 1: the
+    cavity is cut off from voxel (0,0,0), so it is inside and negative."""
+    from oracle import oracle as O
+    u = np.ones((10, 10, 10), np.float32)
+    u[2:8, 2:8, 2:8] = 0.0
+    u[3:7, 3:7, 3:7] = 1.0
+    eps = np.float32(0.25)
+    s = O.udf_to_sdf(u, eps)
+    assert s[0, 0, 0] == np.float32(0.75) and s[9, 9, 9] == np.float32(0.75)
+    assert (s[3:7, 3:7, 3:7] == np.float32(-0.75)).all()
+    assert (s[2, 2:8, 2:8] == np.float32(-0.25)).all()      # shell: udf - eps < 0 stays as is
+    # voxel (0,0,0) occupied: its label is -1, so every occupied voxel is "outside"
+    u2 = u.copy(); u2[0, 0, 0] = 0.0
+    s2 = O.udf_to_sdf(u2, eps)
+    assert (s2[3:7, 3:7, 3:7] == np.float32(-0.75)).all() and s2[9, 9, 9] == np.float32(-0.75)
