@@ -183,6 +183,30 @@ def build_workload(name: str, res: int = 2048, sdf_points: int = 8 << 20):
     raise SystemExit(f"unknown workload {name}")
 
 
+def build_time_device(cubvh, wl, dev, reps=3):
+    """Seconds to build the workload's BVH on the GPU (best of reps, after
+    one warm-up build; outside every timed region)."""
+    import torch
+    cubvh.cuBVH(wl["vertices"], wl["faces"], device_build=True)
+    best = float("inf")
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        cubvh.cuBVH(wl["vertices"], wl["faces"], device_build=True)
+        torch.cuda.synchronize()
+        best = min(best, time.perf_counter() - t0)
+    return best
+
+
+def build_time_reference(wl):
+    """Seconds for the reference's own host build (its BVH4 median-split
+    build, restated in the oracle's FP32 mirror)."""
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    O.RefBVH(wl["vertices"], wl["faces"])
+    return time.perf_counter() - t0
+
+
 def n_queries(op, args):
     if op in GRID_OPS:
         return 0
@@ -291,7 +315,10 @@ def run_ours(args):
     from cubvh_b200._lib import lib, check
 
     wl = build_workload(args.workload, args.res, args.sdf_points)
+    t0 = time.perf_counter()
     bvh = cubvh.cuBVH(wl["vertices"], wl["faces"])
+    build_host_s = time.perf_counter() - t0
+    build_dev_s = build_time_device(cubvh, wl, dev)
     L = lib()
     h = bvh.impl.raw
     stream = torch.cuda.current_stream(dev)
@@ -454,7 +481,8 @@ def run_ours(args):
             alg = n * (io_bytes_per_query(op) + 24.0 * nb_ + 36.0 * nt_)
         achieved = alg / (per_op_ms[dom] / 1e3) / 1e9
         cpu_q, cpu_t, cpu_thr, cpu_desc = cpu_time_sample(wl, wl.get("cpu_sample", 16 << 20))
-        ops_detail = {}
+        ops_detail = {"bvh_build": {"faces": int(len(wl["faces"])), "host_sah_s": build_host_s,
+                                    "device_lbvh_s": build_dev_s, "reference_cpu_s": build_time_reference(wl)}}
         for i, (o, nq, _, kn) in enumerate(dev_ops):
             d = {"kernel": kn, "ms_per_launch": per_op_ms[i]}
             if nq:

@@ -99,13 +99,23 @@ class _DistanceFn(torch.autograd.Function):
 
 
 class cuBVH:
-    def __init__(self, vertices, triangles):
+    def __init__(self, vertices, triangles, device_build: bool = False):
         # vertices: np.ndarray / torch.Tensor [N, 3]; triangles: [M, 3]
+        # device_build: build the BVH on the current GPU (a linear BVH; the
+        # default builds on the host like the reference).  Results of every
+        # query are the same either way.
         V, F = _mesh_arrays(vertices, triangles)
         assert F.shape[0] > 8, "BVH needs at least 8 triangles."
         raw = ctypes.c_void_p()
-        check(lib().cubvh_bvh_create(V.ctypes.data, V.shape[0], F.ctypes.data, F.shape[0],
-                                     ctypes.byref(raw)), "cuBVH")
+        if device_build:
+            dev = torch.device("cuda", torch.cuda.current_device())
+            Vd = torch.from_numpy(V).to(dev)
+            Fd = torch.from_numpy(F).to(dev)
+            check(lib().cubvh_bvh_create_device(_ptr(Vd), V.shape[0], _ptr(Fd), F.shape[0], 0, _stream_ptr(dev),
+                                                ctypes.byref(raw)), "cuBVH")
+        else:
+            check(lib().cubvh_bvh_create(V.ctypes.data, V.shape[0], F.ctypes.data, F.shape[0],
+                                         ctypes.byref(raw)), "cuBVH")
         self.impl = _Handle(raw)
 
     # ---------------------------------------------------------------- info

@@ -13,6 +13,7 @@
 
 #include "../../include/cubvh_b200.h"
 #include "build.h"
+#include "gpubuild.h"
 #include "launches.h"
 #include "kernels.h"
 
@@ -174,6 +175,61 @@ int cubvh_bvh_create(const float* vertices, int64_t n_vertices, const int64_t* f
     }
     const int rc = finish_build(h);
     if (rc != CUBVH_OK) { delete h; return rc; }
+    *out = h;
+    return CUBVH_OK;
+    CUBVH_GUARD_END
+}
+
+int cubvh_bvh_create_device(const float* vertices, int64_t n_vertices, const int64_t* faces, int64_t n_faces,
+                            int32_t max_leaf, void* stream, cubvh_bvh** out) {
+    CUBVH_GUARD_BEGIN
+    if (!out) return fail(CUBVH_ERR_INVALID, "out is null");
+    *out = nullptr;
+    if (!vertices || !faces) return fail(CUBVH_ERR_INVALID, "vertices/faces is null");
+    if (n_vertices <= 0 || n_faces <= 0) return fail(CUBVH_ERR_INVALID, "empty mesh");
+    if (n_vertices > INT32_MAX) return fail(CUBVH_ERR_INVALID, "more than 2^31-1 vertices");
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    if ((e = ensure_constants(device)) != cudaSuccess) return cuda_fail(e, "constant upload");
+    cudaStream_t s = (cudaStream_t)stream;
+    DeviceBuild db;
+    std::string err;
+    const int rc = build_bvh_device(vertices, n_vertices, faces, n_faces, max_leaf ? max_leaf : kMaxLeafTris, s, db, err);
+    if (rc != 0) return fail(rc == 1 ? CUBVH_ERR_INVALID : CUBVH_ERR_CUDA, err);
+    auto* h = new cubvh_bvh();
+    HostBvh& hb = h->host;
+    hb.nodes.resize((size_t)db.n_nodes);
+    hb.tris.resize((size_t)n_faces);
+    std::vector<int64_t> f64((size_t)n_faces * 3);
+    if ((e = cudaMemcpyAsync(hb.nodes.data(), db.nodes, sizeof(CNode) * db.n_nodes, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(hb.tris.data(), db.tris, sizeof(CTri) * n_faces, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(f64.data(), faces, sizeof(int64_t) * 3 * n_faces, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess) {
+        cudaFree(db.nodes); cudaFree(db.tris); delete h;
+        return cuda_fail(e, "GPU build download");
+    }
+    hb.depth = db.depth;
+    hb.level_start = db.level_start;
+    hb.slot_of_face0 = db.slot_of_face0;
+    for (int k = 0; k < 3; ++k) { hb.lo[k] = db.lo[k]; hb.hi[k] = db.hi[k]; }
+    hb.n_vertices = n_vertices;
+    hb.faces.resize((size_t)n_faces * 3);
+    for (size_t i = 0; i < f64.size(); ++i) hb.faces[i] = (int32_t)f64[i];
+    // face-order coordinates and ids (state_dict export, other devices)
+    h->xyz.resize((size_t)n_faces * 9);
+    h->ids.resize((size_t)n_faces);
+    for (const CTri& t : hb.tris) {
+        float* p = &h->xyz[(size_t)t.id * 9];
+        p[0] = t.ax; p[1] = t.ay; p[2] = t.az; p[3] = t.bx; p[4] = t.by; p[5] = t.bz;
+        p[6] = t.cx; p[7] = t.cy; p[8] = t.cz;
+        h->ids[(size_t)t.id] = t.id;
+    }
+    DevCopy d;
+    d.device = device;
+    d.nodes = db.nodes;
+    d.tris = db.tris;
+    h->dev.push_back(d);
     *out = h;
     return CUBVH_OK;
     CUBVH_GUARD_END

@@ -54,6 +54,19 @@ uint64_t cubvh_kernel_launches(void);
 int cubvh_bvh_create(const float* vertices, int64_t n_vertices, const int64_t* faces, int64_t n_faces,
                      cubvh_bvh** out);
 
+/* Build the BVH on the current GPU (no counterpart in the reference, which
+ * builds on the host only: TriangleBvh4::build, src/bvh.cu:515-620).
+ * vertices: device float32 [n_vertices, 3]; faces: device int64
+ * [n_faces, 3]; max_leaf in [1, 4] (0 = 4).  A linear BVH (sorted Morton
+ * codes, binary radix tree, collapsed to the 8-wide layout of
+ * cubvh_bvh_create); query results are identical to those of a host-built
+ * BVH.  Synchronous on `stream`; the device copy for the current device is
+ * the built one, and a host copy is kept as for cubvh_bvh_create.  Fails
+ * with CUBVH_ERR_INVALID on a bad vertex index, a non-finite coordinate or a
+ * tree deeper than 13 levels. */
+int cubvh_bvh_create_device(const float* vertices, int64_t n_vertices, const int64_t* faces, int64_t n_faces,
+                            int32_t max_leaf, void* stream, cubvh_bvh** out);
+
 /* Build a BVH from triangle records in the reference's state_dict format:
  * int32 [n_faces, 12] per record = float a[3], b[3], c[3], 4 pad bytes,
  * int64 face id (host).  The reference's node records are not needed (the
