@@ -42,6 +42,7 @@ _SIGS = {
     "cubvh_udf_to_sdf": [c_vp, c_int, c_int, c_int, c_int, ctypes.c_float, c_vp, c_vp, c_sz, c_vp],
     "cubvh_bvh_refit": [c_vp, c_vp, c_i64, c_vp],
     "cubvh_arena_create": [ctypes.c_int32, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(c_vp)],
+    "cubvh_arena_create_device": [ctypes.c_int32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(c_vp)],
     "cubvh_arena_destroy": [c_vp],
     "cubvh_arena_info": [c_vp, ctypes.POINTER(c_i32), ctypes.POINTER(c_i64), ctypes.POINTER(c_i64)],
     "cubvh_arena_set_queries": [c_vp, c_vp, c_vp],

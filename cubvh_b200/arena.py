@@ -57,7 +57,9 @@ class BVHArena:
     """meshes: list of (vertices [V, 3], faces [F, 3]) (numpy or torch);
     leaf_sizes: optional per-mesh leaf size in [1, 4] (see autotune)."""
 
-    def __init__(self, meshes, leaf_sizes=None):
+    def __init__(self, meshes, leaf_sizes=None, device_build=False):
+        # device_build: build all meshes on the current GPU in one pass
+        # (linear BVHs; the same query results as the default host build)
         self._keep = []
         vs, fs, nv, nf = [], [], [], []
         for v, f in meshes:
@@ -74,10 +76,15 @@ class BVHArena:
         NF = (ctypes.c_int64 * M)(*nf)
         LS = (ctypes.c_int32 * M)(*leaf_sizes) if leaf_sizes is not None else None
         h = ctypes.c_void_p()
-        check(lib().cubvh_arena_create(M, ctypes.cast(VP, ctypes.c_void_p), ctypes.cast(NV, ctypes.c_void_p),
-                                       ctypes.cast(FP, ctypes.c_void_p), ctypes.cast(NF, ctypes.c_void_p),
-                                       ctypes.cast(LS, ctypes.c_void_p) if LS is not None else None,
-                                       ctypes.byref(h)), "arena")
+        args = (M, ctypes.cast(VP, ctypes.c_void_p), ctypes.cast(NV, ctypes.c_void_p),
+                ctypes.cast(FP, ctypes.c_void_p), ctypes.cast(NF, ctypes.c_void_p),
+                ctypes.cast(LS, ctypes.c_void_p) if LS is not None else None)
+        if device_build:
+            dev = torch.device("cuda", torch.cuda.current_device())
+            stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+            check(lib().cubvh_arena_create_device(*args, stream, ctypes.byref(h)), "arena")
+        else:
+            check(lib().cubvh_arena_create(*args, ctypes.byref(h)), "arena")
         self._h = h
         self._keep = None
         self.n_meshes = M

@@ -23,6 +23,7 @@
 
 #include "../../include/cubvh_b200.h"
 #include "build.h"
+#include "gpubuild.h"
 #include "kernels.h"
 #include "scan.cuh"
 
@@ -39,6 +40,7 @@ struct cubvh_arena {
     std::vector<int64_t> face_off;   // [M + 1]
     std::vector<int32_t> gslot;      // [total faces] soup slot of (mesh, face)
     std::vector<float> box;          // [M][6]
+    int64_t n_nodes = 0, n_tris = 0;
     std::mutex mu;
     int device = -1;
     CNode* d_nodes = nullptr;
@@ -159,6 +161,72 @@ int cubvh_arena_create(int32_t n_meshes, const float* const* vertices, const int
             a->gslot[(size_t)a->face_off[m] + (size_t)hb[m].tris[s].id] = to + (int32_t)s;
         for (int k = 0; k < 3; ++k) { a->box[6 * m + k] = hb[m].lo[k]; a->box[6 * m + 3 + k] = hb[m].hi[k]; }
     }
+    a->n_nodes = (int64_t)a->nodes.size();
+    a->n_tris = (int64_t)a->tris.size();
+    *out = a;
+    return CUBVH_OK;
+    ARENA_GUARD_END
+}
+
+int cubvh_arena_create_device(int32_t n_meshes, const float* const* vertices, const int64_t* n_vertices,
+                              const int64_t* const* faces, const int64_t* n_faces, const int32_t* max_leaf,
+                              void* stream, cubvh_arena** out) {
+    ARENA_GUARD_BEGIN
+    if (!out) return set_error(CUBVH_ERR_INVALID, "out is null");
+    *out = nullptr;
+    if (n_meshes <= 0 || !vertices || !n_vertices || !faces || !n_faces)
+        return set_error(CUBVH_ERR_INVALID, "arena needs at least one mesh and non-null arrays");
+    const int M = n_meshes;
+    std::vector<int64_t> voff(M + 1, 0), foff(M + 1, 0);
+    std::vector<int32_t> leaf(M);
+    for (int m = 0; m < M; ++m) {
+        if (!vertices[m] || !faces[m] || n_vertices[m] <= 0 || n_faces[m] <= 0)
+            return set_error(CUBVH_ERR_INVALID, "mesh " + std::to_string(m) + " is empty or null");
+        leaf[m] = max_leaf ? max_leaf[m] : kMaxLeafTris;
+        voff[m + 1] = voff[m] + n_vertices[m];
+        foff[m + 1] = foff[m] + n_faces[m];
+    }
+    if (foff[M] >= (int64_t)(1 << 28)) return set_error(CUBVH_ERR_INVALID, "arena too large (2^28 triangles)");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_err(e, "cudaGetDevice");
+    cudaStream_t s = (cudaStream_t)stream;
+    // one upload of all vertices and faces
+    float* dv = nullptr;
+    int64_t* df = nullptr;
+    if ((e = cudaMalloc(&dv, sizeof(float) * 3 * voff[M])) != cudaSuccess) return cuda_err(e, "cudaMalloc(vertices)");
+    if ((e = cudaMalloc(&df, sizeof(int64_t) * 3 * foff[M])) != cudaSuccess) { cudaFree(dv); return cuda_err(e, "cudaMalloc(faces)"); }
+    for (int m = 0; m < M && e == cudaSuccess; ++m) {
+        e = cudaMemcpyAsync(dv + 3 * voff[m], vertices[m], sizeof(float) * 3 * n_vertices[m], cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(df + 3 * foff[m], faces[m], sizeof(int64_t) * 3 * n_faces[m], cudaMemcpyHostToDevice, s);
+    }
+    if (e != cudaSuccess) { cudaFree(dv); cudaFree(df); return cuda_err(e, "arena mesh upload"); }
+    DeviceBuild db;
+    std::string err;
+    const int rc = build_meshes_device(dv, df, voff, foff, leaf, s, db, err, true);
+    cudaFree(dv);
+    cudaFree(df);
+    if (rc != 0) return set_error(rc == 1 ? CUBVH_ERR_INVALID : CUBVH_ERR_CUDA, err);
+    auto* a = new cubvh_arena();
+    a->M = M;
+    a->root.resize(M);
+    for (int m = 0; m < M; ++m) a->root[m] = m;  // level 0 of the build holds the roots
+    a->slot0 = db.slot0;
+    a->face_off = foff;
+    a->box = db.mesh_box;
+    a->n_nodes = db.n_nodes;
+    a->n_tris = foff[M];
+    a->d_nodes = db.nodes;
+    a->d_tris = db.tris;
+    a->d_gslot = db.gslot;
+    if ((e = cudaMalloc(&a->d_face_off, sizeof(int64_t) * (M + 1))) != cudaSuccess ||
+        (e = cudaMemcpy(a->d_face_off, foff.data(), sizeof(int64_t) * (M + 1), cudaMemcpyHostToDevice)) != cudaSuccess) {
+        a->device = dev;
+        cubvh_arena_destroy(a);
+        return cuda_err(e, "arena face offsets");
+    }
+    a->device = dev;
     *out = a;
     return CUBVH_OK;
     ARENA_GUARD_END
@@ -182,8 +250,8 @@ int cubvh_arena_destroy(cubvh_arena* a) {
 int cubvh_arena_info(const cubvh_arena* a, int32_t* n_meshes, int64_t* n_faces, int64_t* n_nodes) {
     if (!a) return set_error(CUBVH_ERR_INVALID, "arena is null");
     if (n_meshes) *n_meshes = a->M;
-    if (n_faces) *n_faces = (int64_t)a->tris.size();
-    if (n_nodes) *n_nodes = (int64_t)a->nodes.size();
+    if (n_faces) *n_faces = a->n_tris;
+    if (n_nodes) *n_nodes = a->n_nodes;
     return CUBVH_OK;
 }
 

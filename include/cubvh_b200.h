@@ -166,6 +166,13 @@ typedef struct cubvh_arena cubvh_arena;
 int cubvh_arena_create(int32_t n_meshes, const float* const* vertices, const int64_t* n_vertices,
                        const int64_t* const* faces, const int64_t* n_faces, const int32_t* max_leaf,
                        cubvh_arena** out);
+/* cubvh_arena_create_device: the same arena built on the current GPU in one
+ * pass for all meshes (linear BVHs in the same layout; query results are
+ * identical).  Same host arguments as cubvh_arena_create; synchronous on
+ * `stream`; the arena lives on the current device. */
+int cubvh_arena_create_device(int32_t n_meshes, const float* const* vertices, const int64_t* n_vertices,
+                              const int64_t* const* faces, const int64_t* n_faces, const int32_t* max_leaf,
+                              void* stream, cubvh_arena** out);
 int cubvh_arena_destroy(cubvh_arena* arena);
 int cubvh_arena_info(const cubvh_arena* arena, int32_t* n_meshes, int64_t* n_faces, int64_t* n_nodes);
 int cubvh_arena_set_queries(cubvh_arena* arena, const int64_t* query_offsets, const uint32_t* modes);

@@ -135,3 +135,35 @@ def test_device_build_errors(dev):
     vn[3, 0] = np.nan
     with pytest.raises(RuntimeError, match="finite"):
         cubvh.cuBVH(vn, f, device_build=True)
+
+
+def test_device_built_arena(dev):
+    """All meshes built on the GPU in one pass: every query of every mesh
+    equals the host-built arena's result, including raystab and per-mesh
+    leaf sizes, one-face and four-face meshes, and the backward."""
+    meshes = [W.displaced_icosphere(2, 1), W.icosphere(3, 0.6), W.torus(0.5, 0.2, 24, 8),
+              W.displaced_icosphere(4, 2), W.dodecahedron(), W.random_tori(5, n_tori=2, n_major=32, n_minor=8)]
+    meshes = [(np.asarray(v, np.float32), np.asarray(f, np.int64)) for v, f in meshes]
+    v0, f0 = meshes[1]
+    meshes.append((v0, f0[:1]))          # a one-face mesh
+    meshes.append((v0, f0[:4]))          # a single-leaf mesh
+    counts = [1000, 300, 33, 5000, 31, 4097, 50, 70]
+    modes = ["unsigned", "raystab", "watertight", "raystab", "watertight", "unsigned", "unsigned", "unsigned"]
+    leaves = [4, 2, 3, 4, 1, 3, 4, 2]
+    rng = np.random.default_rng(7)
+    qs = []
+    for (v, f), c in zip(meshes, counts):
+        lo, hi = v.min(0), v.max(0)
+        qs.append(((lo + hi) / 2 + rng.uniform(-1, 1, (c, 3)) * (hi - lo) / 2 * 1.1).astype(np.float32))
+    pts = torch.from_numpy(np.concatenate(qs)).to(dev)
+    res = []
+    for device_build in (False, True):
+        ar = cubvh.BVHArena(meshes, leaf_sizes=leaves, device_build=device_build)
+        ar.set_queries(counts, modes)
+        p = pts.clone().requires_grad_()
+        d, fid, uvw = ar.distance(p, return_uvw=True)
+        d.sum().backward()
+        res.append((d.detach(), fid, uvw, p.grad, ar.info()))
+    (d0, f0_, u0, g0, i0), (d1, f1, u1, g1, i1) = res
+    assert torch.equal(d0, d1) and torch.equal(f0_, f1) and torch.equal(u0, u1) and torch.equal(g0, g1)
+    assert i0["faces"] == i1["faces"] and i1["meshes"] == len(meshes)
