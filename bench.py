@@ -592,7 +592,15 @@ def run_ours_fwd_bwd(args):
         qs = [m["points"] for m in ms]
         modes = ["unsigned" if i % 2 == 0 else "raystab" for i in range(len(ms))]
         leaves, report = autotune_leaf_sizes(meshes, qs, modes, sample=32768, repeats=2, device=dev)
+        t0 = time.perf_counter()
         arena = cubvh.BVHArena(meshes, leaf_sizes=leaves)
+        arena_host_s = time.perf_counter() - t0
+        cubvh.BVHArena(meshes[:2], leaf_sizes=leaves[:2], device_build=True)  # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        arena_dev = cubvh.BVHArena(meshes, leaf_sizes=leaves, device_build=True)
+        torch.cuda.synchronize()
+        arena_dev_s = time.perf_counter() - t0
         counts = [len(q) for q in qs]
         arena.set_queries(counts, modes, device=dev)
         pts = torch.from_numpy(np.concatenate(qs)).to(dev)
@@ -621,6 +629,19 @@ def run_ours_fwd_bwd(args):
         kname = "batched fwd_bwd: arena bucketing + k_udf + k_sign_raystab + k_arena_backward_points"
         extra["per_call"] = {"ms_per_step": pc_ms, "queries_per_s": nq / (pc_ms / 1e3)}
         extra["autotune"] = {str(k): v for k, v in report.items()}
+        # the same step on the arena built on the GPU (linear BVHs)
+        arena_dev.set_queries(counts, modes, device=dev)
+
+        def step_dev():
+            p = pts.detach().requires_grad_()
+            d, _, _ = arena_dev.distance(p)
+            d.sum().backward()
+
+        step_dev()
+        extra["arena_build"] = {"faces": int(sum(len(f) for _, f in meshes)), "host_s": arena_host_s,
+                                "device_one_pass_s": arena_dev_s,
+                                "step_ms_on_device_built_arena": _timed(step_dev, 2, stream)}
+        del arena_dev
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
