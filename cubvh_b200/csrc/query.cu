@@ -761,8 +761,9 @@ __global__ void __launch_bounds__(kQBlock) k_udf_heavy(const uint2* __restrict__
 // ------------------------------------------------------------ watertight
 // Sum of unit normals of every triangle whose squared distance to cp is
 // below 1e-6 (src/bvh.cu:356-396; the division by the count does not change
-// the sign and is omitted).
-__device__ d3 normal_sum(const CNode* __restrict__ nodes, const CTri* __restrict__ tris, d3 cp, int root) {
+// the sign and is omitted).  cp lies on the triangle in soup slot `own` (the
+// query's nearest), so that one needs no distance test.
+__device__ d3 normal_sum(const CNode* __restrict__ nodes, const CTri* __restrict__ tris, d3 cp, int root, int own) {
     const float3 cf = make_float3(__double2float_rn(cp.x), __double2float_rn(cp.y), __double2float_rn(cp.z));
     const float cinf = f3inf(cf);
     const float r = 1e-3f + 4e-7f * (1.f + cinf);
@@ -793,7 +794,7 @@ __device__ d3 normal_sum(const CNode* __restrict__ nodes, const CTri* __restrict
                 if (d2 - err - slack > 1.000001e-6f) continue;
                 double bary[3]; d3 q;
                 const d3 a = to_d3(t.a), b = to_d3(t.b), c = to_d3(t.c);
-                if (closest_on_tri_d(cp, a, b, c, bary, &q) < 1e-6) {
+                if (s == own || closest_on_tri_d(cp, a, b, c, bary, &q) < 1e-6) {
                     const d3 nr = dcross(dsub(b, a), dsub(c, a));
                     const double len = __dsqrt_rn(ddot(nr, nr));
                     if (len > 0.0) sum = dadd(sum, d3{dD(nr.x, len), dD(nr.y, len), dD(nr.z, len)});
@@ -820,10 +821,11 @@ __global__ void __launch_bounds__(kQBlock) k_sign_watertight(Work w, const uint3
         const int64_t q = start + (threadIdx.x & 31);
         const int64_t idx = order ? (int64_t)order[q] : q;
         const d3 pd = to_d3(load3(pts, idx));
-        const TriV t = load_tri(tris, slots[idx]);
+        const int own = slots[idx];
+        const TriV t = load_tri(tris, own);
         double bary[3]; d3 cp;
         closest_on_tri_d(pd, to_d3(t.a), to_d3(t.b), to_d3(t.c), bary, &cp);
-        const d3 ns = normal_sum(nodes, tris, cp, root);
+        const d3 ns = normal_sum(nodes, tris, cp, root, own);
         // copysign(distance, avg_normal . (p - cp))
         const double s = ddot(ns, dsub(pd, cp));
         const float d = dist[idx];
