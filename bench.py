@@ -275,11 +275,47 @@ def cpu_time_sample(wl, max_queries, threads=None):
     return q, t, O.threads(), "every %d-th query (%s)" % (stride, "; ".join(parts))
 
 
+def reference_cuda_floodfill(wl, steps, warmup):
+    """The reference's own CUDA floodfill (oracle/_ref, compiled from its
+    include/gpu/floodfill.cuh) on the workload's occupancy grid: wall time of
+    its host entry point `_floodfill_batch` (cudaMalloc, host->device copy of
+    the grid, its hook/compress passes, device->host copy of the labels,
+    cudaFree) with pageable host buffers.  The grid is udf < 2/res, the udf
+    taken from the oracle's FP32 mirror of the reference traversal on the host
+    cores, so no kernel of this package runs in the reference arm."""
+    from oracle import oracle as O
+    import torch
+    if not O.ref_floodfill_available():
+        return {"unavailable": "oracle/_ref/libref_floodfill.so not built (needs the reference tree)"}
+    if not torch.cuda.is_available():
+        return {"unavailable": "no CUDA device"}
+    res = next(a[0] for op, a in wl["ops"] if op == "floodfill")
+    pts = next(a[0] for op, a in wl["ops"] if op == "udf")
+    t0 = time.perf_counter()
+    udf = O.RefBVH(wl["vertices"], wl["faces"]).unsigned_distance(pts)[0]
+    t_udf = time.perf_counter() - t0
+    grid = np.ascontiguousarray(udf.reshape(res, res, res) < np.float32(2.0 / res))
+    for _ in range(max(1, warmup)):
+        O.ref_floodfill(grid)
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        O.ref_floodfill(grid)
+        times.append(time.perf_counter() - t0)
+    return {"e2e_ms": 1e3 * statistics.median(times), "steps": steps,
+            "grid": f"{res}^3 occupancy udf < 2/{res}, blocked fraction {grid.mean():.4f}",
+            "host_buffers": "pageable numpy arrays",
+            "occupancy_udf": f"oracle FP32 mirror of the reference traversal, {t_udf:.1f} s on the host cores"}
+
+
 def run_reference(args):
     rank, world, _ = _rank_info()
     if rank != 0:
         return
     wl = build_workload(args.workload, args.res, args.sdf_points)
+    ref_cuda = {}
+    if any(op == "floodfill" for op, _ in wl["ops"]):
+        ref_cuda["floodfill"] = reference_cuda_floodfill(wl, args.steps, args.warmup)
     per_step = 4 << 20        # bounded sample of the workload per step
     for _ in range(args.warmup):
         cpu_time_sample(wl, per_step)
@@ -297,6 +333,8 @@ def run_reference(args):
         "cpu_baseline": {"value": val, "unit": "queries/s", "cores": thr, "kind": "port", "sample": desc},
         "e2e": {"value": val, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if ref_cuda:
+        line["reference_cuda"] = ref_cuda
     print(json.dumps(line), flush=True)
 
 
@@ -466,6 +504,22 @@ def run_ours(args):
     e2e_ms = max_over_ranks(e2e_ms, dev)
     e2e_val = world * q_per_step * e2e_steps / (e2e_ms / 1e3)
 
+    # floodfill from a pageable host grid to host labels through the public
+    # API, the same footing as the reference arm's CUDA floodfill timing
+    ff_host_ms = None
+    if any(op == "floodfill" for op, _ in wl["ops"]):
+        res = next(a[0] for op, a in wl["ops"] if op == "floodfill")
+        g_host = (occ_src.view(res, res, res) < 2.0 / res).cpu()
+        for _ in range(2):
+            cubvh.floodfill(g_host).cpu()
+        torch.cuda.synchronize()
+        tt = []
+        for _ in range(max(3, min(args.steps, 5))):
+            w0 = time.perf_counter()
+            cubvh.floodfill(g_host).cpu()
+            tt.append(time.perf_counter() - w0)
+        ff_host_ms = 1e3 * statistics.median(tt)
+
     line = None
     if rank == 0:
         # roofline of the dominant kernel: algorithmic bytes per launch (query
@@ -491,6 +545,8 @@ def run_ours(args):
                 if o in counts:
                     d["ref_traversal_boxes_per_query"] = counts[o][0]
                     d["ref_traversal_tris_per_query"] = counts[o][1]
+            if o == "floodfill" and ff_host_ms is not None:
+                d["e2e_host_pageable_ms"] = ff_host_ms
             ops_detail[o] = d
         line = {
             "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,

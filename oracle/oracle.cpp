@@ -20,13 +20,17 @@
 //      sign behaviour, the traversal work counters used for the roofline's
 //      algorithmic bytes, and it is the CPU baseline timed by bench.py.
 //
-// Parity pinning: the reference cannot be compiled in this image (its Eigen
-// submodule is empty and Eigen is not installed), so no reference outputs can
-// be generated here, and the reference's tests hold no golden vectors for this
-// path (they compare with trimesh at runtime).  The FP64 oracle is pinned by
-// analytic known answers (tests/test_oracle.py) and the pcg32 restatement by the
-// published PCG32 known-answer sequence.  Parity against the reference's own
-// outputs is therefore UNPINNED.
+// Parity pinning: the reference's BVH code cannot be compiled in this image
+// (every BVH header includes Eigen; its Eigen submodule is empty and Eigen is
+// not installed), and the reference's tests hold no golden vectors for this
+// path (they compare with trimesh at runtime).  The FP64 distance / ray / sign
+// oracle is pinned by analytic known answers (tests/test_oracle.py) and the
+// pcg32 restatement by the published PCG32 known-answer sequence; its parity
+// with the reference's own outputs is UNPINNED.  The floodfill IS pinned to
+// the reference's own outputs: its CUDA floodfill (include/gpu/floodfill.cuh,
+// CUDA runtime only) is compiled from the reference tree into oracle/_ref, and
+// orc_floodfill reproduces its labels bit for bit on the 13 grids of
+// tests/golden/ref_floodfill.npz (tests/test_ref_floodfill.py).
 //
 // Reference files followed (paths relative to the cubvh project root):
 //   include/gpu/triangle.cuh:27-68, 114-158     triangle tests, closest point, uvw

@@ -1,10 +1,12 @@
 """ctypes front end of the CPU oracle (oracle.cpp).
 
-TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
-CPU-baseline leg of bench.py, never by the cubvh_b200 package.  See the header
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke(), the
+CPU-baseline leg and the reference arm of bench.py, never by the cubvh_b200
+package.  See the header
 of oracle.cpp for what is restated from which reference file, and for the
-pinning status (parity against the reference's own outputs is unpinned: the
-reference cannot be built in this image).
+pinning status (floodfill: pinned to the reference's own CUDA floodfill,
+compiled into oracle/_ref; distance, ray and sign queries: unpinned against
+the reference's outputs, whose BVH code cannot be built in this image).
 """
 
 from __future__ import annotations
@@ -152,6 +154,40 @@ def floodfill(grid):
                              ctypes.c_int(D), _p(out))
     if rc != 0:
         raise ValueError("grid too large for int32 labels")
+    return out[0] if squeeze else out
+
+
+_REF_FF_PATH = os.path.join(_HERE, "_ref", "libref_floodfill.so")
+_ref_ff = None
+
+
+def ref_floodfill_available() -> bool:
+    """True when the reference's own CUDA floodfill has been compiled into
+    oracle/_ref (oracle/Makefile target `ref`; needs the reference tree)."""
+    return os.path.exists(_REF_FF_PATH)
+
+
+def ref_floodfill(grid):
+    """The reference's own CUDA floodfill (include/gpu/floodfill.cuh
+    `_floodfill_batch`) on a host grid: bool/uint8 [B,H,W,D] or [H,W,D] ->
+    int32 labels.  Needs a GPU; its iteration count is the reference's
+    (at most min(ceil(|(H,W,D)|) + 50, 10 max(H,W,D)) hook passes)."""
+    global _ref_ff
+    if _ref_ff is None:
+        if not ref_floodfill_available():
+            raise FileNotFoundError(_REF_FF_PATH + " not built (make -C oracle ref)")
+        _ref_ff = ctypes.CDLL(_REF_FF_PATH)
+        _ref_ff.ref_floodfill.restype = ctypes.c_int
+    g = np.ascontiguousarray(np.asarray(grid) != 0, dtype=np.uint8)
+    squeeze = g.ndim == 3
+    if squeeze:
+        g = g[None]
+    B, H, W, D = g.shape
+    out = np.empty(g.shape, np.int32)
+    rc = _ref_ff.ref_floodfill(_p(g), ctypes.c_int(B), ctypes.c_int(H), ctypes.c_int(W),
+                               ctypes.c_int(D), _p(out))
+    if rc != 0:
+        raise RuntimeError("reference floodfill failed (code %d)" % rc)
     return out[0] if squeeze else out
 
 
