@@ -144,7 +144,7 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------- workloads
-def build_workload(name: str, res: int = 2048, sdf_points: int = 8 << 20):
+def build_workload(name: str, res: int = 2048, sdf_points: int = 8 << 20, grid: int = 512):
     from cubvh_b200 import workloads as W
     if name == "rays_displaced":
         w = W.rays_displaced(res=res, n_sdf=sdf_points)
@@ -158,10 +158,11 @@ def build_workload(name: str, res: int = 2048, sdf_points: int = 8 << 20):
                     ops=[("udf_uvw", (w["points"],))],
                     desc="icosphere L4 r 0.8 (5,120 faces); 1,048,576 points U[-1,1]^3, uvw on")
     if name == "dense_tori":
-        w = W.dense_tori()
+        w = W.dense_tori(grid)
         g = W.dense_grid(w["grid_res"])
-        return dict(name=name, vertices=w["vertices"], faces=w["faces"], ops=[("udf", (g,)), ("floodfill", (512,)), ("udf_to_sdf", (512,))],
-                    desc="12 tori (174,778 faces, 10% removed); UDF on the 512^3 grid + floodfill of udf < 2/512 "
+        return dict(name=name, vertices=w["vertices"], faces=w["faces"],
+                    ops=[("udf", (g,)), ("floodfill", (grid,)), ("udf_to_sdf", (grid,))],
+                    desc=f"12 tori (174,778 faces, 10% removed); UDF on the {grid}^3 grid + floodfill of udf < 2/{grid} "
                          "+ the fused udf -> sdf step (occupancy, floodfill, signs)")
     if name == "grad_displaced":
         w = W.grad_displaced()
@@ -312,7 +313,7 @@ def run_reference(args):
     rank, world, _ = _rank_info()
     if rank != 0:
         return
-    wl = build_workload(args.workload, args.res, args.sdf_points)
+    wl = build_workload(args.workload, args.res, args.sdf_points, args.grid)
     ref_cuda = {}
     if any(op == "floodfill" for op, _ in wl["ops"]):
         ref_cuda["floodfill"] = reference_cuda_floodfill(wl, args.steps, args.warmup)
@@ -352,7 +353,7 @@ def run_ours(args):
     import cubvh_b200 as cubvh
     from cubvh_b200._lib import lib, check
 
-    wl = build_workload(args.workload, args.res, args.sdf_points)
+    wl = build_workload(args.workload, args.res, args.sdf_points, args.grid)
     t0 = time.perf_counter()
     bvh = cubvh.cuBVH(wl["vertices"], wl["faces"])
     build_host_s = time.perf_counter() - t0
@@ -529,7 +530,7 @@ def run_ours(args):
         dom = max(range(len(dev_ops)), key=lambda i: per_op_ms[i])
         op, n, _, kname = dev_ops[dom]
         if op in GRID_OPS:  # floodfill: 1 B in + 4 B out per voxel; udf_to_sdf: 4 B in + 4 B out
-            alg = (5.0 if op == "floodfill" else 8.0) * 512 ** 3
+            alg = (5.0 if op == "floodfill" else 8.0) * args.grid ** 3
         else:
             nb_, nt_ = counts[op]
             alg = n * (io_bytes_per_query(op) + 24.0 * nb_ + 36.0 * nt_)
@@ -776,6 +777,7 @@ def main():
     ap.add_argument("--meshes", type=int, default=256, help="batch_256: number of meshes")
     ap.add_argument("--res", type=int, default=2048, help="camera resolution (rays_displaced)")
     ap.add_argument("--sdf-points", type=int, default=8 << 20, help="SDF queries (rays_displaced)")
+    ap.add_argument("--grid", type=int, default=512, help="grid resolution (dense_tori)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -245,7 +245,10 @@ __global__ void k_root_label(int32_t* __restrict__ parent, const int32_t* __rest
         parent[i] = start[parent[i]];
 }
 
-// 5b. labels: one warp writes 32 consecutive voxels per store (128 B).
+// 5b. labels: one warp writes 32 consecutive voxels per store (128 B).  Lane
+// k of the warp decodes word w0 + k once (its row, its first voxel and how
+// many of its 32 bits lie inside the row); the loop over the 32 words then
+// only shuffles those values.
 __global__ void k_write(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ rowoff,
                         const uint32_t* __restrict__ wpref, const int32_t* __restrict__ runlab,
                         int32_t* __restrict__ labels, int64_t rows, int64_t wpr, int W) {
@@ -255,30 +258,66 @@ __global__ void k_write(const uint32_t* __restrict__ bits, const uint32_t* __res
     const int64_t words = rows * wpr;
     const uint32_t below = (lane == 31) ? 0xFFFFFFFFu : ((2u << lane) - 1u);
     for (int64_t w0 = warp * 32; w0 < words; w0 += nwarps * 32) {
-        // lane k loads word w0 + k, its previous word and its run base
         const int64_t wk = w0 + lane;
-        uint32_t f = 0, s = 0, base = 0;
+        uint32_t f = 0, s = 0, base = 0, vb = 0;
+        int nval = 0;
         if (wk < words) {
             const int64_t r = wk / wpr, wi = wk - r * wpr;
             f = bits[wk];
             const uint32_t prev = wi > 0 ? bits[wk - 1] : 0u;
             s = starts_of(f, prev);
             base = rowoff[r] + wpref[wk];
+            vb = (uint32_t)(r * W + wi * 32);   // < 2^31 voxels (checked on the host)
+            nval = min(32, W - (int)wi * 32);
         }
         const int nw = (int)min((int64_t)32, words - w0);
         for (int k = 0; k < nw; ++k) {
             const uint32_t fk = __shfl_sync(0xFFFFFFFFu, f, k);
             const uint32_t sk = __shfl_sync(0xFFFFFFFFu, s, k);
             const uint32_t bk = __shfl_sync(0xFFFFFFFFu, base, k);
-            const int64_t wg = w0 + k;
-            const int64_t r = wg / wpr;
-            const int x = (int)(wg - r * wpr) * 32 + lane;
-            if (x < W) {
+            const uint32_t vk = __shfl_sync(0xFFFFFFFFu, vb, k);
+            const int nk = __shfl_sync(0xFFFFFFFFu, nval, k);
+            if (lane < nk) {
                 int32_t lab = -1;
                 if ((fk >> lane) & 1u) lab = __ldg(runlab + (bk + __popc(sk & below) - 1));
-                __stcs(labels + r * W + x, lab);
+                __stcs(labels + vk + lane, lab);
             }
         }
+    }
+}
+
+// 5b (W % 32 == 0, 16-byte aligned output).  Rows hold whole words, so voxel
+// 32 w + b is bit b of word w.  A warp covers 4 words (128 voxels) per step:
+// lane l takes word l / 8 and its 4 bits from 4 (l % 8), and writes their
+// labels with one 16-byte streaming store (512 contiguous bytes per warp).
+__device__ __forceinline__ void run_labels4(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ rowoff,
+                                            const uint32_t* __restrict__ wpref,
+                                            const int32_t* __restrict__ runlab, uint32_t w, uint32_t wpr,
+                                            uint32_t q, int32_t o[4]) {
+    const uint32_t r = w / wpr, wi = w - r * wpr;
+    const uint32_t f = bits[w];
+    const uint32_t s = starts_of(f, wi ? bits[w - 1] : 0u);
+    const uint32_t base = rowoff[r] + wpref[w];
+    uint32_t cnt = __popc(s & ((1u << q) - 1u));   // run starts below bit q
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        cnt += (s >> (q + j)) & 1u;
+        o[j] = ((f >> (q + j)) & 1u) ? __ldg(runlab + (base + cnt - 1)) : -1;
+    }
+}
+__global__ void k_write4(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ rowoff,
+                         const uint32_t* __restrict__ wpref, const int32_t* __restrict__ runlab,
+                         int4* __restrict__ labels, uint32_t words, uint32_t wpr) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t sub = (uint32_t)lane >> 3, q = (uint32_t)(lane & 7) * 4;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t c = warp; c * 4 < (int64_t)words; c += nwarps) {
+        const uint32_t w = (uint32_t)(c * 4) + sub;
+        if (w >= words) continue;
+        int32_t o[4];
+        run_labels4(bits, rowoff, wpref, runlab, w, wpr, q, o);
+        __stcs(labels + (size_t)w * 8 + (lane & 7), make_int4(o[0], o[1], o[2], o[3]));
     }
 }
 
@@ -297,7 +336,8 @@ __global__ void k_write_sdf(const uint32_t* __restrict__ bits, const uint32_t* _
     const uint32_t below = (lane == 31) ? 0xFFFFFFFFu : ((2u << lane) - 1u);
     for (int64_t w0 = warp * 32; w0 < words; w0 += nwarps * 32) {
         const int64_t wk = w0 + lane;
-        uint32_t f = 0, s = 0, base = 0;
+        uint32_t f = 0, s = 0, base = 0, vb = 0;
+        int nval = 0;
         int32_t empty = -1;
         if (wk < words) {
             const int64_t r = wk / wpr, wi = wk - r * wpr;
@@ -305,6 +345,8 @@ __global__ void k_write_sdf(const uint32_t* __restrict__ bits, const uint32_t* _
             const uint32_t prev = wi > 0 ? bits[wk - 1] : 0u;
             s = starts_of(f, prev);
             base = rowoff[r] + wpref[wk];
+            vb = (uint32_t)(r * W + wi * 32);
+            nval = min(32, W - (int)wi * 32);
             const int64_t r0 = (r / rows_per_volume) * rows_per_volume;
             if (bits[r0 * wpr] & 1u) empty = __ldg(runlab + rowoff[r0]);
         }
@@ -313,17 +355,42 @@ __global__ void k_write_sdf(const uint32_t* __restrict__ bits, const uint32_t* _
             const uint32_t fk = __shfl_sync(0xFFFFFFFFu, f, k);
             const uint32_t sk = __shfl_sync(0xFFFFFFFFu, s, k);
             const uint32_t bk = __shfl_sync(0xFFFFFFFFu, base, k);
+            const uint32_t vk = __shfl_sync(0xFFFFFFFFu, vb, k);
+            const int nk = __shfl_sync(0xFFFFFFFFu, nval, k);
             const int32_t ek = __shfl_sync(0xFFFFFFFFu, empty, k);
-            const int64_t wg = w0 + k;
-            const int64_t r = wg / wpr;
-            const int x = (int)(wg - r * wpr) * 32 + lane;
-            if (x < W) {
+            if (lane < nk) {
                 int32_t lab = -1;
                 if ((fk >> lane) & 1u) lab = __ldg(runlab + (bk + __popc(sk & below) - 1));
-                const float d = __fsub_rn(__ldcs(udf + r * W + x), eps);
-                __stcs(sdf + r * W + x, (lab != ek && d > 0.f) ? -d : d);
+                const float d = __fsub_rn(__ldcs(udf + vk + lane), eps);
+                __stcs(sdf + vk + lane, (lab != ek && d > 0.f) ? -d : d);
             }
         }
+    }
+}
+// 5' (W % 32 == 0, 16-byte aligned udf and sdf): the k_write4 layout, one
+// 16-byte load of udf and one 16-byte store of sdf per lane.
+__global__ void k_write_sdf4(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ rowoff,
+                             const uint32_t* __restrict__ wpref, const int32_t* __restrict__ runlab,
+                             const float4* __restrict__ udf, float4* __restrict__ sdf, uint32_t words,
+                             uint32_t wpr, uint32_t rows_per_volume, float eps) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t sub = (uint32_t)lane >> 3, q = (uint32_t)(lane & 7) * 4;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t c = warp; c * 4 < (int64_t)words; c += nwarps) {
+        const uint32_t w = (uint32_t)(c * 4) + sub;
+        if (w >= words) continue;
+        int32_t o[4];
+        run_labels4(bits, rowoff, wpref, runlab, w, wpr, q, o);
+        const uint32_t r0 = (w / wpr / rows_per_volume) * rows_per_volume;
+        const int32_t empty = (bits[(size_t)r0 * wpr] & 1u) ? __ldg(runlab + rowoff[r0]) : -1;
+        const size_t i4 = (size_t)w * 8 + (lane & 7);
+        const float4 u = __ldcs(udf + i4);
+        float d[4] = {__fsub_rn(u.x, eps), __fsub_rn(u.y, eps), __fsub_rn(u.z, eps), __fsub_rn(u.w, eps)};
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (o[j] != empty && d[j] > 0.f) d[j] = -d[j];
+        __stcs(sdf + i4, make_float4(d[0], d[1], d[2], d[3]));
     }
 }
 
@@ -372,7 +439,12 @@ cudaError_t launch_floodfill(const uint8_t* grid, int B, int H, int W, int D, in
         k_pack<<<sgrid, 256, 0, stream>>>(grid, bits, p.rows, W, p.wpr); count_launch();
     }
     label_runs(p, H, D, bits, wpref, rowoff, bsum, start, parent, status, sgrid, stream);
-    k_write<<<sgrid, 256, 0, stream>>>(bits, rowoff, wpref, parent, labels, p.rows, p.wpr, W); count_launch();
+    if (W % 32 == 0 && (reinterpret_cast<uintptr_t>(labels) & 15) == 0) {
+        k_write4<<<sgrid, 256, 0, stream>>>(bits, rowoff, wpref, parent, reinterpret_cast<int4*>(labels),
+                                            (uint32_t)p.words, (uint32_t)p.wpr); count_launch();
+    } else {
+        k_write<<<sgrid, 256, 0, stream>>>(bits, rowoff, wpref, parent, labels, p.rows, p.wpr, W); count_launch();
+    }
     return cudaGetLastError();
 }
 
@@ -396,8 +468,14 @@ cudaError_t launch_udf_to_sdf(const float* udf, int B, int H, int W, int D, floa
     k_zero<<<1, 1, 0, stream>>>(status); count_launch();
     k_pack_udf<<<sgrid, 256, 0, stream>>>(udf, bits, p.rows, W, p.wpr, eps); count_launch();
     label_runs(p, H, D, bits, wpref, rowoff, bsum, start, parent, status, sgrid, stream);
-    k_write_sdf<<<sgrid, 256, 0, stream>>>(bits, rowoff, wpref, parent, udf, sdf, p.rows, p.wpr, W,
-                                           (int64_t)D * H, eps); count_launch();
+    if (W % 32 == 0 && ((reinterpret_cast<uintptr_t>(udf) | reinterpret_cast<uintptr_t>(sdf)) & 15) == 0) {
+        k_write_sdf4<<<sgrid, 256, 0, stream>>>(bits, rowoff, wpref, parent, reinterpret_cast<const float4*>(udf),
+                                                reinterpret_cast<float4*>(sdf), (uint32_t)p.words, (uint32_t)p.wpr,
+                                                (uint32_t)((int64_t)D * H), eps); count_launch();
+    } else {
+        k_write_sdf<<<sgrid, 256, 0, stream>>>(bits, rowoff, wpref, parent, udf, sdf, p.rows, p.wpr, W,
+                                               (int64_t)D * H, eps); count_launch();
+    }
     return cudaGetLastError();
 }
 

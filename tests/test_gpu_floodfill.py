@@ -95,3 +95,51 @@ def test_udf_to_sdf_sphere_grid(oracle, dev):
     assert torch.equal(sdf, ref)
     r = pts.norm(dim=1).view(res, res, res)
     assert (sdf[r < 0.4] < 0).all() and (sdf[r > 0.8] > 0).all()
+
+
+@pytest.mark.parametrize("shape", [(1, 40, 64, 24), (2, 12, 96, 20)])
+def test_c_abi_unaligned_buffers(oracle, dev, shape):
+    """W % 32 == 0 grids (W = shape[2], the reference's row length) through the C ABI with the grid, labels, udf and sdf
+    pointers moved off 16-byte alignment (the byte-wise pack and the
+    word-per-store label/sdf writers) and aligned (the 16-byte paths): the
+    same labels and signed grids either way."""
+    import ctypes
+    from cubvh_b200._lib import lib, check
+    L = lib()
+    B, H, Wd, D = shape
+    n = B * H * Wd * D
+    rng = np.random.default_rng(n)
+    g = rng.random(shape) < 0.45
+    u = rng.random(shape).astype(np.float32)
+    u[rng.random(shape) < 0.35] = 0.0
+    want_lab, want_sdf = oracle.floodfill(g), oracle.udf_to_sdf(u, 0.05)
+    nb = ctypes.c_size_t()
+    check(L.cubvh_floodfill_workspace_size(B, H, Wd, D, ctypes.byref(nb)), "ws")
+    ws = torch.empty(nb.value, dtype=torch.uint8, device=dev)
+    sp = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    for off in (0, 1):
+        gbuf = torch.zeros(n + 16, dtype=torch.uint8, device=dev)
+        gbuf[off:off + n] = torch.from_numpy(g.reshape(-1).astype(np.uint8)).to(dev)
+        lbuf = torch.full((n + 4,), -7, dtype=torch.int32, device=dev)
+        check(L.cubvh_floodfill(ctypes.c_void_p(gbuf.data_ptr() + off), B, H, Wd, D,
+                                ctypes.c_void_p(lbuf.data_ptr() + 4 * off), ctypes.c_void_p(ws.data_ptr()),
+                                nb.value, sp), "floodfill")
+        got = lbuf[off:off + n].cpu().numpy().reshape(shape)
+        assert np.array_equal(got, want_lab)
+        assert (lbuf[:off] == -7).all() and (lbuf[off + n:] == -7).all()
+        ubuf = torch.zeros(n + 4, dtype=torch.float32, device=dev)
+        ubuf[off:off + n] = torch.from_numpy(u.reshape(-1)).to(dev)
+        sbuf = torch.full((n + 4,), 7.0, dtype=torch.float32, device=dev)
+        check(L.cubvh_udf_to_sdf(ctypes.c_void_p(ubuf.data_ptr() + 4 * off), B, H, Wd, D, ctypes.c_float(0.05),
+                                 ctypes.c_void_p(sbuf.data_ptr() + 4 * off), ctypes.c_void_p(ws.data_ptr()),
+                                 nb.value, sp), "udf_to_sdf")
+        assert np.array_equal(sbuf[off:off + n].cpu().numpy().reshape(shape), want_sdf)
+        assert (sbuf[:off] == 7.0).all() and (sbuf[off + n:] == 7.0).all()
+
+
+@pytest.mark.parametrize("shape,p", [((1, 96, 96, 96), 0.3), ((2, 64, 64, 64), 0.6), ((1, 8, 32, 8), 0.5)])
+def test_floodfill_aligned_rows(oracle, dev, shape, p):
+    """Rows of whole 32-voxel words (the 16-byte label store path)."""
+    g = np.random.default_rng(int(p * 10) + shape[-1]).random(shape) < p
+    got = cubvh.floodfill(torch.from_numpy(g).to(dev), check_bounds=True).cpu().numpy()
+    assert np.array_equal(got, oracle.floodfill(g))
