@@ -26,6 +26,10 @@ struct DevCopy {
     int32_t* face_vidx = nullptr;  // [F, 3] (meshes only), uploaded on first use
     int32_t* face_slot = nullptr;  // [F] soup slot of each face id, -1 if none
     float* node_box = nullptr;     // [n_nodes, 6] refit scratch
+    int32_t* near_cnt = nullptr;   // watertight candidate lists (launch_near_lists)
+    int32_t* near_lst = nullptr;
+    bool near_valid = false;       // false until built, and again after a refit
+    bool near_off = false;         // lists not kept (too large or allocation failed)
 };
 
 struct cubvh_bvh {
@@ -104,6 +108,46 @@ int grad_buffers(cubvh_bvh* h, DevCopy* d, bool need_vidx) {
         if ((e = cudaMemcpy(d->face_vidx, h->host.faces.data(), nf * 3 * sizeof(int32_t), cudaMemcpyHostToDevice)) != cudaSuccess)
             return cuda_fail(e, "upload(face_vidx)");
     }
+    return CUBVH_OK;
+}
+
+// Watertight candidate lists of this device copy: built on first use on the
+// caller's stream and waited for, so that calls on any stream see finished
+// lists; rebuilt after a refit.  Not built while the stream is being captured
+// into a graph, nor for BVHs whose lists would exceed 1 GiB: the sign pass
+// then walks the tree, with the same results.
+int near_lists(cubvh_bvh* h, DevCopy* d, cudaStream_t s, const int32_t** cnt, const int32_t** lst) {
+    *cnt = nullptr; *lst = nullptr;
+    std::lock_guard<std::mutex> lk(h->mu);
+    if (d->near_off) return CUBVH_OK;
+    const int64_t nt = (int64_t)h->host.tris.size();
+    if (!d->near_valid) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cudaError_t e = cudaStreamIsCapturing(s, &cs);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamIsCapturing");
+        if (cs != cudaStreamCaptureStatusNone) return CUBVH_OK;
+        if (!d->near_cnt) {
+            const size_t lb = (size_t)nt * kNear * sizeof(int32_t);
+            if (lb > ((size_t)1 << 30) || cudaMalloc(&d->near_cnt, (size_t)nt * sizeof(int32_t)) != cudaSuccess) {
+                cudaGetLastError();
+                d->near_cnt = nullptr;
+                d->near_off = true;
+                return CUBVH_OK;
+            }
+            if (cudaMalloc(&d->near_lst, lb) != cudaSuccess) {
+                cudaGetLastError();
+                cudaFree(d->near_cnt);
+                d->near_cnt = nullptr;
+                d->near_off = true;
+                return CUBVH_OK;
+            }
+        }
+        if ((e = launch_near_lists(nt, d->nodes, d->tris, d->near_cnt, d->near_lst, s)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(s)) != cudaSuccess)
+            return cuda_fail(e, "watertight candidate lists");
+        d->near_valid = true;
+    }
+    *cnt = d->near_cnt; *lst = d->near_lst;
     return CUBVH_OK;
 }
 
@@ -266,6 +310,8 @@ int cubvh_bvh_destroy(cubvh_bvh* h) {
             if (d.face_vidx) cudaFree(d.face_vidx);
             if (d.face_slot) cudaFree(d.face_slot);
             if (d.node_box) cudaFree(d.node_box);
+            if (d.near_cnt) cudaFree(d.near_cnt);
+            if (d.near_lst) cudaFree(d.near_lst);
         }
     }
     if (have && !h->dev.empty()) cudaSetDevice(cur);
@@ -339,12 +385,17 @@ int cubvh_signed_distance(cubvh_bvh* h, const float* points, int64_t n, uint32_t
     if (rc != CUBVH_OK) return rc;
     const int kmode = mode == 0xFFFFFFFFu ? 0 : (int)mode + 1;
     cudaStream_t s = (cudaStream_t)stream;
+    const int32_t *near_cnt = nullptr, *near_lst = nullptr;
+    if (kmode == 1) {
+        const int rc2 = near_lists(h, d, s, &near_cnt, &near_lst);
+        if (rc2 != CUBVH_OK) return rc2;
+    }
     const size_t wsb = query_workspace_bytes(kmode, n);
     void* ws = nullptr;
     cudaError_t e;
     if ((e = cudaMallocAsync(&ws, wsb, s)) != cudaSuccess) return cuda_fail(e, "cudaMallocAsync(query workspace)");
     e = launch_distance(kmode, uvw != nullptr, n, points, distances, face_id, uvw, d->nodes, d->tris,
-                        (int)h->host.slot_of_face0, ws, s);
+                        (int)h->host.slot_of_face0, near_cnt, near_lst, ws, s);
     if (ws) {
         const cudaError_t e2 = cudaFreeAsync(ws, s);
         if (e == cudaSuccess) e = e2;
@@ -477,6 +528,7 @@ int cubvh_bvh_refit(cubvh_bvh* h, const float* vertices, int64_t n_vertices, voi
         std::lock_guard<std::mutex> lk(h->mu);
         if (!d->node_box && (e = cudaMalloc(&d->node_box, h->host.nodes.size() * 6 * sizeof(float))) != cudaSuccess)
             return cuda_fail(e, "cudaMalloc(refit scratch)");
+        d->near_valid = false;  // the triangles move: rebuild the watertight lists on next use
     }
     e = launch_refit((int64_t)h->host.tris.size(), d->tris, d->face_vidx, vertices, d->nodes, d->node_box,
                      h->host.level_start.data(), (int)h->host.level_start.size() - 1, (cudaStream_t)stream);

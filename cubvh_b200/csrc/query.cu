@@ -805,12 +805,94 @@ __device__ d3 normal_sum(const CNode* __restrict__ nodes, const CTri* __restrict
     return sum;
 }
 
+// normal_sum over a precomputed candidate list of cp's triangle (k_near_lists):
+// the same tests in the same order, without the walk from the root.
+__device__ d3 normal_sum_list(const CTri* __restrict__ tris, d3 cp, int own, const int32_t* __restrict__ lst,
+                              int count) {
+    const float3 cf = make_float3(__double2float_rn(cp.x), __double2float_rn(cp.y), __double2float_rn(cp.z));
+    const float slack = 1e-9f * (1.f + f3inf(cf));
+    d3 sum{0.0, 0.0, 0.0};
+    for (int k = 0; k < count; ++k) {
+        const int s = __ldg(lst + k);
+        const TriV t = load_tri(tris, s);
+        float err;
+        const float d2 = tri_d2_f(cf, t, &err);
+        if (d2 - err - slack > 1.000001e-6f) continue;
+        double bary[3]; d3 q;
+        const d3 a = to_d3(t.a), b = to_d3(t.b), c = to_d3(t.c);
+        if (s == own || closest_on_tri_d(cp, a, b, c, bary, &q) < 1e-6) {
+            const d3 nr = dcross(dsub(b, a), dsub(c, a));
+            const double len = __dsqrt_rn(ddot(nr, nr));
+            if (len > 0.0) sum = dadd(sum, d3{dD(nr.x, len), dD(nr.y, len), dD(nr.z, len)});
+        }
+    }
+    return sum;
+}
+
+// Candidate lists of the watertight normal sum.  For soup slot t: every slot
+// whose triangle's bounding box meets t's box grown by 1.001e-3 + 1e-6 (1 +
+// max |coordinate|), in the order normal_sum's walk reaches them (depth-first,
+// children in the same push order, slots ascending in a leaf).  A point cp on
+// triangle t has every triangle within normal_sum's radius of it on t's list
+// (the radius is at most 1e-3 + 4e-7 (1 + |cp|_inf) and |cp| <= max |vertex|),
+// so the list replaces the walk and keeps the summation order.  cnt[t] = -1
+// when more than kNear slots qualify: that query walks the tree.
+__global__ void __launch_bounds__(kQBlock) k_near_lists(int64_t nt, const CNode* __restrict__ nodes,
+                                                        const CTri* __restrict__ tris, int root,
+                                                        int32_t* __restrict__ cnt, int32_t* __restrict__ lst) {
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += (int64_t)gridDim.x * blockDim.x) {
+        const TriV a = load_tri(tris, (int)t);
+        float3 lo = make_float3(fminf(a.a.x, fminf(a.b.x, a.c.x)), fminf(a.a.y, fminf(a.b.y, a.c.y)),
+                                fminf(a.a.z, fminf(a.b.z, a.c.z)));
+        float3 hi = make_float3(fmaxf(a.a.x, fmaxf(a.b.x, a.c.x)), fmaxf(a.a.y, fmaxf(a.b.y, a.c.y)),
+                                fmaxf(a.a.z, fmaxf(a.b.z, a.c.z)));
+        const float r = 1.001e-3f + 1e-6f * (1.f + fmaxf(f3inf(lo), f3inf(hi)));
+        lo = make_float3(lo.x - r, lo.y - r, lo.z - r);
+        hi = make_float3(hi.x + r, hi.y + r, hi.z + r);
+        int32_t* out = lst + t * kNear;
+        int c = 0;
+        int st[kStack];
+        int sp = 0;
+        st[sp++] = root;
+        while (sp > 0) {
+            const int ref = st[--sp];
+            if (ref >= 0) {
+                const NodeView nd = load_node(nodes, ref);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const uint32_t m = meta_of(nd, j);
+                    float3 clo, chi;
+                    child_box(nd, j, clo, chi);
+                    if (m != kEmpty && clo.x <= hi.x && clo.y <= hi.y && clo.z <= hi.z && chi.x >= lo.x &&
+                        chi.y >= lo.y && chi.z >= lo.z)
+                        st[sp++] = child_ref(nd, m);
+                }
+            } else {
+                int s0, s1;
+                leaf_range(ref, s0, s1);
+                for (int s = s0; s < s1; ++s) {
+                    const TriV b = load_tri(tris, s);
+                    if (fminf(b.a.x, fminf(b.b.x, b.c.x)) <= hi.x && fminf(b.a.y, fminf(b.b.y, b.c.y)) <= hi.y &&
+                        fminf(b.a.z, fminf(b.b.z, b.c.z)) <= hi.z && fmaxf(b.a.x, fmaxf(b.b.x, b.c.x)) >= lo.x &&
+                        fmaxf(b.a.y, fmaxf(b.b.y, b.c.y)) >= lo.y && fmaxf(b.a.z, fmaxf(b.b.z, b.c.z)) >= lo.z) {
+                        if (c < kNear) out[c] = s;
+                        ++c;
+                    }
+                }
+            }
+        }
+        cnt[t] = c <= kNear ? c : -1;
+    }
+}
+
 __global__ void __launch_bounds__(kQBlock) k_sign_watertight(Work w, const uint32_t* __restrict__ order,
                                                              const float* __restrict__ pts,
                                                              float* __restrict__ dist,
                                                              const int32_t* __restrict__ slots,
                                                              const CNode* __restrict__ nodes,
                                                              const CTri* __restrict__ tris,
+                                                             const int32_t* __restrict__ near_cnt,
+                                                             const int32_t* __restrict__ near_lst,
                                                              unsigned long long* __restrict__ ctr, int64_t grab) {
     PacketQueue pq(ctr, w.packets(), grab);
     for (int64_t pk = pq.take(); pk >= 0; pk = pq.take()) {
@@ -825,7 +907,9 @@ __global__ void __launch_bounds__(kQBlock) k_sign_watertight(Work w, const uint3
         const TriV t = load_tri(tris, own);
         double bary[3]; d3 cp;
         closest_on_tri_d(pd, to_d3(t.a), to_d3(t.b), to_d3(t.c), bary, &cp);
-        const d3 ns = normal_sum(nodes, tris, cp, root, own);
+        const int nc = near_cnt ? __ldg(near_cnt + own) : -1;
+        const d3 ns = nc >= 0 ? normal_sum_list(tris, cp, own, near_lst + (int64_t)own * kNear, nc)
+                              : normal_sum(nodes, tris, cp, root, own);
         // copysign(distance, avg_normal . (p - cp))
         const double s = ddot(ns, dsub(pd, cp));
         const float d = dist[idx];
@@ -1200,8 +1284,8 @@ int64_t chunk_for(int64_t n, unsigned grid) {
 }  // namespace
 
 cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts, float* dist, int64_t* fid,
-                            float* uvw, const CNode* nodes, const CTri* tris, int slot_face0, void* ws,
-                            cudaStream_t stream) {
+                            float* uvw, const CNode* nodes, const CTri* tris, int slot_face0,
+                            const int32_t* near_cnt, const int32_t* near_lst, void* ws, cudaStream_t stream) {
     if (n <= 0) return cudaSuccess;
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     char* w = static_cast<char*>(ws);
@@ -1248,11 +1332,20 @@ cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts
 #undef CUBVH_L
     if (mode == 1) {
         const unsigned g = persistent_grid(k_sign_watertight, n);
-        k_sign_watertight<<<g, kQBlock, 0, stream>>>(work, order, pts, dist, slots, nodes, tris, ctr + 1, grab_for(n, g)); count_launch();
+        k_sign_watertight<<<g, kQBlock, 0, stream>>>(work, order, pts, dist, slots, nodes, tris, near_cnt, near_lst,
+                                                     ctr + 1, grab_for(n, g)); count_launch();
     } else if (mode == 2) {
         const unsigned g = persistent_grid(k_sign_raystab, n);
         k_sign_raystab<<<g, kQBlock, 0, stream>>>(work, order, pts, dist, nodes, tris, ctr + 1, chunk_for(n, g)); count_launch();
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_near_lists(int64_t n_tris, const CNode* nodes, const CTri* tris, int32_t* cnt, int32_t* lst,
+                              cudaStream_t stream) {
+    if (n_tris <= 0) return cudaSuccess;
+    const unsigned g = persistent_grid(k_near_lists, n_tris);
+    k_near_lists<<<g, kQBlock, 0, stream>>>(n_tris, nodes, tris, 0, cnt, lst); count_launch();
     return cudaGetLastError();
 }
 
@@ -1338,8 +1431,8 @@ cudaError_t launch_arena_distance(const ArenaLaunch& a, const float* pts, float*
     if (a.n_wt_packets > 0) {
         const Work w{a.wt_packets, a.meshes, a.n_wt_packets, 0};
         const unsigned gw = persistent_grid(k_sign_watertight, 32 * a.n_wt_packets);
-        k_sign_watertight<<<gw, kQBlock, 0, stream>>>(w, a.order, pts, dist, a.slots, a.nodes, a.tris,
-                                                      a.counters + 1, grab_for(32 * a.n_wt_packets, gw)); count_launch();
+        k_sign_watertight<<<gw, kQBlock, 0, stream>>>(w, a.order, pts, dist, a.slots, a.nodes, a.tris, nullptr,
+                                                      nullptr, a.counters + 1, grab_for(32 * a.n_wt_packets, gw)); count_launch();
     }
     if (a.n_rs_packets > 0) {
         const Work w{a.rs_packets, a.meshes, a.n_rs_packets, 0};
