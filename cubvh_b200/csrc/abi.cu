@@ -28,6 +28,9 @@ struct DevCopy {
     float* node_box = nullptr;     // [n_nodes, 6] refit scratch
     int32_t* near_cnt = nullptr;   // watertight candidate lists (launch_near_lists)
     int32_t* near_lst = nullptr;
+    double* near_nrm = nullptr;
+    int* near_flag = nullptr;      // device int: some list overflowed
+    bool near_ovf = false;
     bool near_valid = false;       // false until built, and again after a refit
     bool near_off = false;         // lists not kept (too large or allocation failed)
 };
@@ -116,8 +119,8 @@ int grad_buffers(cubvh_bvh* h, DevCopy* d, bool need_vidx) {
 // lists; rebuilt after a refit.  Not built while the stream is being captured
 // into a graph, nor for BVHs whose lists would exceed 1 GiB: the sign pass
 // then walks the tree, with the same results.
-int near_lists(cubvh_bvh* h, DevCopy* d, cudaStream_t s, const int32_t** cnt, const int32_t** lst) {
-    *cnt = nullptr; *lst = nullptr;
+int near_lists(cubvh_bvh* h, DevCopy* d, cudaStream_t s, NearLists* out) {
+    *out = NearLists{};
     std::lock_guard<std::mutex> lk(h->mu);
     if (d->near_off) return CUBVH_OK;
     const int64_t nt = (int64_t)h->host.tris.size();
@@ -134,20 +137,30 @@ int near_lists(cubvh_bvh* h, DevCopy* d, cudaStream_t s, const int32_t** cnt, co
                 d->near_off = true;
                 return CUBVH_OK;
             }
-            if (cudaMalloc(&d->near_lst, lb) != cudaSuccess) {
+            if (cudaMalloc(&d->near_lst, lb) != cudaSuccess ||
+                cudaMalloc(&d->near_nrm, (size_t)nt * 3 * sizeof(double)) != cudaSuccess ||
+                cudaMalloc(&d->near_flag, sizeof(int)) != cudaSuccess) {
                 cudaGetLastError();
                 cudaFree(d->near_cnt);
+                if (d->near_lst) cudaFree(d->near_lst);
+                if (d->near_nrm) cudaFree(d->near_nrm);
                 d->near_cnt = nullptr;
+                d->near_lst = nullptr;
+                d->near_nrm = nullptr;
                 d->near_off = true;
                 return CUBVH_OK;
             }
         }
-        if ((e = launch_near_lists(nt, d->nodes, d->tris, d->near_cnt, d->near_lst, s)) != cudaSuccess ||
+        int flag = 0;
+        if ((e = launch_near_lists(nt, d->nodes, d->tris, d->near_cnt, d->near_lst, d->near_nrm, d->near_flag, s)) !=
+                cudaSuccess ||
+            (e = cudaMemcpyAsync(&flag, d->near_flag, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
             (e = cudaStreamSynchronize(s)) != cudaSuccess)
             return cuda_fail(e, "watertight candidate lists");
+        d->near_ovf = flag != 0;
         d->near_valid = true;
     }
-    *cnt = d->near_cnt; *lst = d->near_lst;
+    out->cnt = d->near_cnt; out->lst = d->near_lst; out->nrm = d->near_nrm; out->ovf = d->near_ovf;
     return CUBVH_OK;
 }
 
@@ -312,6 +325,8 @@ int cubvh_bvh_destroy(cubvh_bvh* h) {
             if (d.node_box) cudaFree(d.node_box);
             if (d.near_cnt) cudaFree(d.near_cnt);
             if (d.near_lst) cudaFree(d.near_lst);
+            if (d.near_nrm) cudaFree(d.near_nrm);
+            if (d.near_flag) cudaFree(d.near_flag);
         }
     }
     if (have && !h->dev.empty()) cudaSetDevice(cur);
@@ -385,9 +400,9 @@ int cubvh_signed_distance(cubvh_bvh* h, const float* points, int64_t n, uint32_t
     if (rc != CUBVH_OK) return rc;
     const int kmode = mode == 0xFFFFFFFFu ? 0 : (int)mode + 1;
     cudaStream_t s = (cudaStream_t)stream;
-    const int32_t *near_cnt = nullptr, *near_lst = nullptr;
+    NearLists near;
     if (kmode == 1) {
-        const int rc2 = near_lists(h, d, s, &near_cnt, &near_lst);
+        const int rc2 = near_lists(h, d, s, &near);
         if (rc2 != CUBVH_OK) return rc2;
     }
     const size_t wsb = query_workspace_bytes(kmode, n);
@@ -395,7 +410,7 @@ int cubvh_signed_distance(cubvh_bvh* h, const float* points, int64_t n, uint32_t
     cudaError_t e;
     if ((e = cudaMallocAsync(&ws, wsb, s)) != cudaSuccess) return cuda_fail(e, "cudaMallocAsync(query workspace)");
     e = launch_distance(kmode, uvw != nullptr, n, points, distances, face_id, uvw, d->nodes, d->tris,
-                        (int)h->host.slot_of_face0, near_cnt, near_lst, ws, s);
+                        (int)h->host.slot_of_face0, near, ws, s);
     if (ws) {
         const cudaError_t e2 = cudaFreeAsync(ws, s);
         if (e == cudaSuccess) e = e2;

@@ -49,16 +49,22 @@ constexpr int64_t kSortMinQueries = 2048;
 size_t query_workspace_bytes(int mode, int64_t n);
 // mode 0 unsigned, 1 watertight sign, 2 raystab sign.  ws:
 // query_workspace_bytes(mode, n) bytes, 256-byte aligned.
-// near_cnt / near_lst: watertight candidate lists (launch_near_lists) or
-// nullptr (the sign pass walks the tree).
-cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts, float* dist, int64_t* fid,
-                            float* uvw, const CNode* nodes, const CTri* tris, int slot_face0,
-                            const int32_t* near_cnt, const int32_t* near_lst, void* ws, cudaStream_t stream);
-// Watertight candidate lists of a single BVH (root node 0): for each soup slot
-// t, cnt[t] slots at lst[t * kNear ...] (cnt[t] = -1: more than kNear).
+// Watertight candidate lists of a single BVH (root node 0, launch_near_lists):
+// for each soup slot t, cnt[t] slots at lst[t * kNear ...] (cnt[t] = -1: more
+// than kNear), and nrm[3t .. 3t + 2] the FP64 unit normal of slot t (zero for
+// a degenerate triangle); ovf: some slot's list overflowed (those queries take
+// a second pass that walks the tree).  cnt nullptr: every query walks.
 constexpr int kNear = 32;
+struct NearLists {
+    const int32_t* cnt = nullptr; const int32_t* lst = nullptr; const double* nrm = nullptr;
+    bool ovf = false;
+};
+cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts, float* dist, int64_t* fid,
+                            float* uvw, const CNode* nodes, const CTri* tris, int slot_face0, NearLists near,
+                            void* ws, cudaStream_t stream);
+// any_ovf: one device int, set to 1 when some list overflowed.
 cudaError_t launch_near_lists(int64_t n_tris, const CNode* nodes, const CTri* tris, int32_t* cnt, int32_t* lst,
-                              cudaStream_t stream);
+                              double* nrm, int* any_ovf, cudaStream_t stream);
 cudaError_t launch_ray(int64_t n, const float* ro, const float* rd, float* pos, int64_t* fid, float* depth,
                        const CNode* nodes, const CTri* tris, void* ws, cudaStream_t stream);
 

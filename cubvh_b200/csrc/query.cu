@@ -806,9 +806,11 @@ __device__ d3 normal_sum(const CNode* __restrict__ nodes, const CTri* __restrict
 }
 
 // normal_sum over a precomputed candidate list of cp's triangle (k_near_lists):
-// the same tests in the same order, without the walk from the root.
+// the same tests in the same order, without the walk from the root, and the
+// unit normals read from the table k_near_lists computed them into (the same
+// operations as normal_sum's).
 __device__ d3 normal_sum_list(const CTri* __restrict__ tris, d3 cp, int own, const int32_t* __restrict__ lst,
-                              int count) {
+                              int count, const double* __restrict__ nrm) {
     const float3 cf = make_float3(__double2float_rn(cp.x), __double2float_rn(cp.y), __double2float_rn(cp.z));
     const float slack = 1e-9f * (1.f + f3inf(cf));
     d3 sum{0.0, 0.0, 0.0};
@@ -819,19 +821,47 @@ __device__ d3 normal_sum_list(const CTri* __restrict__ tris, d3 cp, int own, con
         const float d2 = tri_d2_f(cf, t, &err);
         if (d2 - err - slack > 1.000001e-6f) continue;
         double bary[3]; d3 q;
-        const d3 a = to_d3(t.a), b = to_d3(t.b), c = to_d3(t.c);
-        if (s == own || closest_on_tri_d(cp, a, b, c, bary, &q) < 1e-6) {
-            const d3 nr = dcross(dsub(b, a), dsub(c, a));
-            const double len = __dsqrt_rn(ddot(nr, nr));
-            if (len > 0.0) sum = dadd(sum, d3{dD(nr.x, len), dD(nr.y, len), dD(nr.z, len)});
-        }
+        if (s == own || closest_on_tri_d(cp, to_d3(t.a), to_d3(t.b), to_d3(t.c), bary, &q) < 1e-6)
+            // a zero normal (degenerate triangle) leaves the sum unchanged: its
+            // components are never -0, so adding +0 is exact
+            sum = dadd(sum, d3{__ldg(nrm + 3 * s), __ldg(nrm + 3 * s + 1), __ldg(nrm + 3 * s + 2)});
     }
     return sum;
 }
 
+// True when an axis among the two triangles' normals and the nine cross
+// products of their edges separates a and b by more than r: then no point of
+// b lies within r of a point of a.  Any axis u is a valid separating axis, so
+// rounding in u itself is harmless; each projection onto u is off by at most
+// a few ulps of |u| max|v|, covered by the margin 2e-6 (1 + scale) |u| added to
+// r (scale: the larger max |coordinate| of the two triangles).  Degenerate
+// axes (|u| = 0) separate nothing.
+__device__ bool tri_gap_exceeds(const TriV& a, const TriV& b, float r, float scale) {
+    const float3 ea[3] = {f3sub(a.b, a.a), f3sub(a.c, a.b), f3sub(a.a, a.c)};
+    const float3 eb[3] = {f3sub(b.b, b.a), f3sub(b.c, b.b), f3sub(b.a, b.c)};
+    const float rr = r + 2e-6f * (1.f + scale);
+    auto sep = [&](float3 u) {
+        const float l2 = f3dot(u, u);
+        if (!(l2 > 0.f)) return false;
+        const float a0 = f3dot(u, a.a), a1 = f3dot(u, a.b), a2 = f3dot(u, a.c);
+        const float b0 = f3dot(u, b.a), b1 = f3dot(u, b.b), b2 = f3dot(u, b.c);
+        const float amin = fminf(a0, fminf(a1, a2)), amax = fmaxf(a0, fmaxf(a1, a2));
+        const float bmin = fminf(b0, fminf(b1, b2)), bmax = fmaxf(b0, fmaxf(b1, b2));
+        return fmaxf(bmin - amax, amin - bmax) > rr * 1.0001f * sqrtf(l2);
+    };
+    if (sep(f3cross(ea[0], ea[1])) || sep(f3cross(eb[0], eb[1]))) return true;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            if (sep(f3cross(ea[i], eb[j]))) return true;
+    return false;
+}
+
 // Candidate lists of the watertight normal sum.  For soup slot t: every slot
-// whose triangle's bounding box meets t's box grown by 1.001e-3 + 1e-6 (1 +
-// max |coordinate|), in the order normal_sum's walk reaches them (depth-first,
+// whose triangle's bounding box meets t's box grown by r = 1.001e-3 + 1e-6 (1 +
+// max |coordinate|) and that no separating axis (tri_gap_exceeds) puts more
+// than r from t, in the order normal_sum's walk reaches them (depth-first,
 // children in the same push order, slots ascending in a leaf).  A point cp on
 // triangle t has every triangle within normal_sum's radius of it on t's list
 // (the radius is at most 1e-3 + 4e-7 (1 + |cp|_inf) and |cp| <= max |vertex|),
@@ -839,14 +869,25 @@ __device__ d3 normal_sum_list(const CTri* __restrict__ tris, d3 cp, int own, con
 // when more than kNear slots qualify: that query walks the tree.
 __global__ void __launch_bounds__(kQBlock) k_near_lists(int64_t nt, const CNode* __restrict__ nodes,
                                                         const CTri* __restrict__ tris, int root,
-                                                        int32_t* __restrict__ cnt, int32_t* __restrict__ lst) {
+                                                        int32_t* __restrict__ cnt, int32_t* __restrict__ lst,
+                                                        double* __restrict__ nrm, int* __restrict__ any_ovf) {
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += (int64_t)gridDim.x * blockDim.x) {
         const TriV a = load_tri(tris, (int)t);
+        {
+            const d3 da = to_d3(a.a), db = to_d3(a.b), dc = to_d3(a.c);
+            const d3 nr = dcross(dsub(db, da), dsub(dc, da));
+            const double len = __dsqrt_rn(ddot(nr, nr));
+            const bool ok = len > 0.0;
+            nrm[3 * t] = ok ? dD(nr.x, len) : 0.0;
+            nrm[3 * t + 1] = ok ? dD(nr.y, len) : 0.0;
+            nrm[3 * t + 2] = ok ? dD(nr.z, len) : 0.0;
+        }
         float3 lo = make_float3(fminf(a.a.x, fminf(a.b.x, a.c.x)), fminf(a.a.y, fminf(a.b.y, a.c.y)),
                                 fminf(a.a.z, fminf(a.b.z, a.c.z)));
         float3 hi = make_float3(fmaxf(a.a.x, fmaxf(a.b.x, a.c.x)), fmaxf(a.a.y, fmaxf(a.b.y, a.c.y)),
                                 fmaxf(a.a.z, fmaxf(a.b.z, a.c.z)));
-        const float r = 1.001e-3f + 1e-6f * (1.f + fmaxf(f3inf(lo), f3inf(hi)));
+        const float vinf = fmaxf(f3inf(lo), f3inf(hi));
+        const float r = 1.001e-3f + 1e-6f * (1.f + vinf);
         lo = make_float3(lo.x - r, lo.y - r, lo.z - r);
         hi = make_float3(hi.x + r, hi.y + r, hi.z + r);
         int32_t* out = lst + t * kNear;
@@ -874,7 +915,9 @@ __global__ void __launch_bounds__(kQBlock) k_near_lists(int64_t nt, const CNode*
                     const TriV b = load_tri(tris, s);
                     if (fminf(b.a.x, fminf(b.b.x, b.c.x)) <= hi.x && fminf(b.a.y, fminf(b.b.y, b.c.y)) <= hi.y &&
                         fminf(b.a.z, fminf(b.b.z, b.c.z)) <= hi.z && fmaxf(b.a.x, fmaxf(b.b.x, b.c.x)) >= lo.x &&
-                        fmaxf(b.a.y, fmaxf(b.b.y, b.c.y)) >= lo.y && fmaxf(b.a.z, fmaxf(b.b.z, b.c.z)) >= lo.z) {
+                        fmaxf(b.a.y, fmaxf(b.b.y, b.c.y)) >= lo.y && fmaxf(b.a.z, fmaxf(b.b.z, b.c.z)) >= lo.z &&
+                        (s == (int)t ||
+                         !tri_gap_exceeds(a, b, r, fmaxf(vinf, fmaxf(f3inf(b.a), fmaxf(f3inf(b.b), f3inf(b.c))))))) {
                         if (c < kNear) out[c] = s;
                         ++c;
                     }
@@ -882,18 +925,20 @@ __global__ void __launch_bounds__(kQBlock) k_near_lists(int64_t nt, const CNode*
             }
         }
         cnt[t] = c <= kNear ? c : -1;
+        if (c > kNear) atomicOr(any_ovf, 1);
     }
 }
 
-__global__ void __launch_bounds__(kQBlock) k_sign_watertight(Work w, const uint32_t* __restrict__ order,
-                                                             const float* __restrict__ pts,
-                                                             float* __restrict__ dist,
-                                                             const int32_t* __restrict__ slots,
-                                                             const CNode* __restrict__ nodes,
-                                                             const CTri* __restrict__ tris,
-                                                             const int32_t* __restrict__ near_cnt,
-                                                             const int32_t* __restrict__ near_lst,
-                                                             unsigned long long* __restrict__ ctr, int64_t grab) {
+// Watertight sign: copysign(distance, normal_sum . (p - cp)), cp the closest
+// point of the query's nearest triangle (soup slot `own`).  LIST: the normal
+// sum over own's candidate list; a query whose list overflowed is queued in
+// ovf for k_sign_watertight_ovf (single BVH).  !LIST: the walk (arenas).
+template <bool LIST>
+__global__ void __launch_bounds__(kQBlock)
+k_sign_watertight(Work w, const uint32_t* __restrict__ order, const float* __restrict__ pts, float* __restrict__ dist,
+                  const int32_t* __restrict__ slots, const CNode* __restrict__ nodes, const CTri* __restrict__ tris,
+                  const NearLists near, uint32_t* __restrict__ ovf, unsigned long long* __restrict__ ovf_n,
+                  unsigned long long* __restrict__ ctr, int64_t grab) {
     PacketQueue pq(ctr, w.packets(), grab);
     for (int64_t pk = pq.take(); pk >= 0; pk = pq.take()) {
         int64_t start, qoff;
@@ -902,15 +947,42 @@ __global__ void __launch_bounds__(kQBlock) k_sign_watertight(Work w, const uint3
         if ((int)(threadIdx.x & 31) >= cnt) continue;
         const int64_t q = start + (threadIdx.x & 31);
         const int64_t idx = order ? (int64_t)order[q] : q;
-        const d3 pd = to_d3(load3(pts, idx));
         const int own = slots[idx];
+        const int nc = LIST ? __ldg(near.cnt + own) : -1;  // in flight during the closest point
+        const d3 pd = to_d3(load3(pts, idx));
         const TriV t = load_tri(tris, own);
         double bary[3]; d3 cp;
         closest_on_tri_d(pd, to_d3(t.a), to_d3(t.b), to_d3(t.c), bary, &cp);
-        const int nc = near_cnt ? __ldg(near_cnt + own) : -1;
-        const d3 ns = nc >= 0 ? normal_sum_list(tris, cp, own, near_lst + (int64_t)own * kNear, nc)
-                              : normal_sum(nodes, tris, cp, root, own);
+        if (LIST && nc < 0) {
+            ovf[atomicAdd(ovf_n, 1ull)] = (uint32_t)idx;
+            continue;
+        }
+        const d3 ns = LIST ? normal_sum_list(tris, cp, own, near.lst + (int64_t)own * kNear, nc, near.nrm)
+                           : normal_sum(nodes, tris, cp, root, own);
         // copysign(distance, avg_normal . (p - cp))
+        const double s = ddot(ns, dsub(pd, cp));
+        const float d = dist[idx];
+        dist[idx] = signbit(s) ? -d : d;
+    }
+}
+// The queries k_sign_watertight<true> queued (their lists overflowed): the
+// walk from root 0.
+__global__ void __launch_bounds__(kQBlock) k_sign_watertight_ovf(const uint32_t* __restrict__ ovf,
+                                                                 const unsigned long long* __restrict__ ovf_n,
+                                                                 const float* __restrict__ pts,
+                                                                 float* __restrict__ dist,
+                                                                 const int32_t* __restrict__ slots,
+                                                                 const CNode* __restrict__ nodes,
+                                                                 const CTri* __restrict__ tris) {
+    const int64_t n = (int64_t)*ovf_n;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t idx = ovf[i];
+        const int own = slots[idx];
+        const d3 pd = to_d3(load3(pts, idx));
+        const TriV t = load_tri(tris, own);
+        double bary[3]; d3 cp;
+        closest_on_tri_d(pd, to_d3(t.a), to_d3(t.b), to_d3(t.c), bary, &cp);
+        const d3 ns = normal_sum(nodes, tris, cp, 0, own);
         const double s = ddot(ns, dsub(pd, cp));
         const float d = dist[idx];
         dist[idx] = signbit(s) ? -d : d;
@@ -1260,6 +1332,7 @@ size_t query_workspace_bytes(int mode, int64_t n) {
         b += al(sizeof(uint32_t) * 8);                            // query box
     }
     if (mode > 0) b += al(sizeof(int32_t) * n);                   // winning slots
+    if (mode == 1) b += al(sizeof(uint32_t) * n);                 // watertight overflow queue
     if (mode >= 0) b += al(sizeof(uint2) * heavy_cap_for(n));     // heavy-query list
     return b;
 }
@@ -1284,8 +1357,8 @@ int64_t chunk_for(int64_t n, unsigned grid) {
 }  // namespace
 
 cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts, float* dist, int64_t* fid,
-                            float* uvw, const CNode* nodes, const CTri* tris, int slot_face0,
-                            const int32_t* near_cnt, const int32_t* near_lst, void* ws, cudaStream_t stream) {
+                            float* uvw, const CNode* nodes, const CTri* tris, int slot_face0, NearLists near,
+                            void* ws, cudaStream_t stream) {
     if (n <= 0) return cudaSuccess;
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     char* w = static_cast<char*>(ws);
@@ -1310,6 +1383,8 @@ cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts
     }
     int32_t* slots = mode != 0 ? reinterpret_cast<int32_t*>(w) : nullptr;
     if (mode != 0) w += al(sizeof(int32_t) * n);
+    uint32_t* ovf = mode == 1 ? reinterpret_cast<uint32_t*>(w) : nullptr;
+    if (mode == 1) w += al(sizeof(uint32_t) * n);
     uint2* heavy = reinterpret_cast<uint2*>(w);
     const int64_t hcap = heavy_cap_for(n);
     const Work work{nullptr, nullptr, n, slot_face0};
@@ -1331,9 +1406,19 @@ cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts
     else { if (want_uvw) CUBVH_L(true, true); else CUBVH_L(false, true); }
 #undef CUBVH_L
     if (mode == 1) {
-        const unsigned g = persistent_grid(k_sign_watertight, n);
-        k_sign_watertight<<<g, kQBlock, 0, stream>>>(work, order, pts, dist, slots, nodes, tris, near_cnt, near_lst,
-                                                     ctr + 1, grab_for(n, g)); count_launch();
+        if (near.cnt) {
+            const unsigned g = persistent_grid(k_sign_watertight<true>, n);
+            k_sign_watertight<true><<<g, kQBlock, 0, stream>>>(work, order, pts, dist, slots, nodes, tris, near, ovf,
+                                                               ctr + 9, ctr + 1, grab_for(n, g)); count_launch();
+            if (near.ovf) {
+                const unsigned go = persistent_grid(k_sign_watertight_ovf, n);
+                k_sign_watertight_ovf<<<go, kQBlock, 0, stream>>>(ovf, ctr + 9, pts, dist, slots, nodes, tris); count_launch();
+            }
+        } else {
+            const unsigned g = persistent_grid(k_sign_watertight<false>, n);
+            k_sign_watertight<false><<<g, kQBlock, 0, stream>>>(work, order, pts, dist, slots, nodes, tris, near,
+                                                                nullptr, nullptr, ctr + 1, grab_for(n, g)); count_launch();
+        }
     } else if (mode == 2) {
         const unsigned g = persistent_grid(k_sign_raystab, n);
         k_sign_raystab<<<g, kQBlock, 0, stream>>>(work, order, pts, dist, nodes, tris, ctr + 1, chunk_for(n, g)); count_launch();
@@ -1342,10 +1427,12 @@ cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts
 }
 
 cudaError_t launch_near_lists(int64_t n_tris, const CNode* nodes, const CTri* tris, int32_t* cnt, int32_t* lst,
-                              cudaStream_t stream) {
+                              double* nrm, int* any_ovf, cudaStream_t stream) {
     if (n_tris <= 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(any_ovf, 0, sizeof(int), stream);
+    if (e != cudaSuccess) return e;
     const unsigned g = persistent_grid(k_near_lists, n_tris);
-    k_near_lists<<<g, kQBlock, 0, stream>>>(n_tris, nodes, tris, 0, cnt, lst); count_launch();
+    k_near_lists<<<g, kQBlock, 0, stream>>>(n_tris, nodes, tris, 0, cnt, lst, nrm, any_ovf); count_launch();
     return cudaGetLastError();
 }
 
@@ -1430,9 +1517,10 @@ cudaError_t launch_arena_distance(const ArenaLaunch& a, const float* pts, float*
 #undef CUBVH_L
     if (a.n_wt_packets > 0) {
         const Work w{a.wt_packets, a.meshes, a.n_wt_packets, 0};
-        const unsigned gw = persistent_grid(k_sign_watertight, 32 * a.n_wt_packets);
-        k_sign_watertight<<<gw, kQBlock, 0, stream>>>(w, a.order, pts, dist, a.slots, a.nodes, a.tris, nullptr,
-                                                      nullptr, a.counters + 1, grab_for(32 * a.n_wt_packets, gw)); count_launch();
+        const unsigned gw = persistent_grid(k_sign_watertight<false>, 32 * a.n_wt_packets);
+        k_sign_watertight<false><<<gw, kQBlock, 0, stream>>>(w, a.order, pts, dist, a.slots, a.nodes, a.tris,
+                                                             NearLists{}, nullptr, nullptr, a.counters + 1,
+                                                             grab_for(32 * a.n_wt_packets, gw)); count_launch();
     }
     if (a.n_rs_packets > 0) {
         const Work w{a.rs_packets, a.meshes, a.n_rs_packets, 0};
