@@ -79,25 +79,39 @@ def _peaks():
         return 6650.0, "fallback"
 
 
-def _profile_traffic(op: str, workload: str):
-    """DRAM bytes (read + write) of one full-size call of `op`, from the
-    committed ncu summary profiles/traffic_<workload>.json."""
+def _profile_traffic(op: str, workload: str, n_queries: int = 0):
+    """DRAM bytes (read + write) of one call of `op` over n_queries, from the
+    committed ncu summary profiles/traffic_<workload>.json: its captured bytes
+    per query times n_queries (the BVH stays in L2, so traffic grows with the
+    queries), or its full-size figure when no query count is given."""
     path = os.path.join(ROOT, "profiles", f"traffic_{workload}.json")
     try:
         with open(path) as fh:
-            return float(json.load(fh)[op]["dram_bytes_per_full_launch"])
+            e = json.load(fh)[op]
+        if n_queries and "captured_queries" in e:
+            return float(e["captured_dram_bytes"]) * n_queries / float(e["captured_queries"])
+        return float(e["dram_bytes_per_full_launch"])
     except Exception:
         return None
 
 
 class ClockSampler:
-    """nvidia-smi sampling of SM clock and throttle reasons during a region."""
+    """nvidia-smi sampling (every 100 ms) of SM clock and throttle reasons
+    during a region.  The sampler is running before the region starts; a
+    region shorter than the sampling period that catches no sample reports the
+    first sample taken after it (``window`` says which)."""
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
+        self.lines = []
+
+    def _reader(self):
+        for line in self.proc.stdout:
+            self.lines.append((time.perf_counter(), line))
 
     def __enter__(self):
+        import threading
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu),
@@ -108,25 +122,40 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
+            return self
+        self.thread = threading.Thread(target=self._reader, daemon=True)
+        self.thread.start()
+        deadline = time.perf_counter() + 10.0
+        while not self.lines and time.perf_counter() < deadline and self.proc.poll() is None:
+            time.sleep(0.01)
+        self.t0 = time.perf_counter()
         return self
 
     def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                out, _ = self.proc.communicate(timeout=5)
-            except Exception:
-                self.proc.kill()
-                out = ""
-            self.out = out
+        if self.proc is None:
+            return False
+        self.t1 = time.perf_counter()
+        deadline = self.t1 + 1.0
+        while not any(t > self.t1 for t, _ in self.lines) and time.perf_counter() < deadline:
+            time.sleep(0.01)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
         return False
 
     def summary(self):
         if self.proc is None:
             return None
+        inside = [ln for t, ln in self.lines if self.t0 <= t <= self.t1]
+        window = "timed region"
+        if not inside:
+            after = [ln for t, ln in self.lines if t > self.t1][:1]
+            inside, window = after, "first sample after a region shorter than the 100 ms sampling period"
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in getattr(self, "out", "").splitlines():
+        for line in inside:
             f = [x.strip() for x in line.split(",")]
             if len(f) < 7:
                 continue
@@ -140,7 +169,7 @@ class ClockSampler:
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "window": window}
 
 
 # --------------------------------------------------------------- workloads
@@ -560,7 +589,7 @@ def run_ours(args):
                     "steps": e2e_steps},
             "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": _profile_traffic(op, wl["name"]),
+                         "traffic": _profile_traffic(op, wl["name"], n),
                          "algorithmic_bytes_per_launch": alg},
             "cpu_baseline": {"value": cpu_q / cpu_t, "unit": "queries/s", "cores": cpu_thr, "kind": "port",
                              "sample": cpu_desc},
