@@ -162,6 +162,41 @@ def test_ray_trace_in_face_planes(oracle, dev):
     assert (_np(out[1]) >= 0).mean() > 0.3
 
 
+def test_ray_trace_order_independent(oracle, dev):
+    """Results do not depend on how the rays are split into calls (one call of
+    6000 rays against six of 1000: packets and work distribution differ) and
+    equal the oracle's, also for 2160 rays along cube face planes."""
+    v, f = W.random_tori(2, n_tori=3, n_major=48, n_minor=12)
+    bvh = cubvh.cuBVH(v, f)
+    rng = np.random.default_rng(21)
+    ro = rng.uniform(-1, 1, (6000, 3)).astype(np.float32)
+    rd = rng.standard_normal((6000, 3)).astype(np.float32)
+    rd[:300, 2] = 0.0
+    rd /= np.linalg.norm(rd, axis=1, keepdims=True)
+    ro_t, rd_t = torch.from_numpy(ro).to(dev), torch.from_numpy(rd).to(dev)
+    whole = bvh.ray_trace(ro_t, rd_t)
+    parts = [bvh.ray_trace(ro_t[i:i + 1000], rd_t[i:i + 1000]) for i in range(0, 6000, 1000)]
+    for k in range(3):
+        assert torch.equal(whole[k], torch.cat([p[k] for p in parts]))
+    check_rays(oracle, v, f, ro, rd, whole)
+    cv = np.array([[x, y, z] for x in (-1, 1) for y in (-1, 1) for z in (-1, 1)], np.float32)
+    quads = [(0, 1, 3, 2), (4, 6, 7, 5), (0, 4, 5, 1), (2, 3, 7, 6), (0, 2, 6, 4), (1, 5, 7, 3)]
+    cf = np.array([t for a, b, c, d in quads for t in ((a, b, c), (a, c, d))], np.int64)
+    o2, d2 = [], []
+    for ax in range(3):
+        u, w = (ax + 1) % 3, (ax + 2) % 3
+        for side in (-1.0, 1.0):
+            for x in np.linspace(-1.5, 1.5, 90):
+                for dirn in ((0.0, 1.0), (0.6, 0.8), (-0.28, 0.96), (0.28, -0.96)):
+                    o = np.zeros(3); o[ax] = side; o[u] = x; o[w] = -3.0 * np.sign(dirn[1])
+                    d = np.zeros(3); d[u], d[w] = dirn
+                    o2.append(o); d2.append(d)
+    o2, d2 = np.array(o2, np.float32), np.array(d2, np.float32)
+    assert len(o2) >= 2048
+    out = cubvh.cuBVH(cv, cf).ray_trace(torch.from_numpy(o2).to(dev), torch.from_numpy(d2).to(dev))
+    check_rays(oracle, cv, cf, o2, d2, out)
+
+
 def check_sdf(got, sd_o, fid_o, what):
     d, fid, _ = (_np(x) if x is not None else None for x in got)
     assert np.array_equal(fid, fid_o), f"{what}: face ids differ at {(fid != fid_o).sum()} points"
