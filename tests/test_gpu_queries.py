@@ -4,7 +4,7 @@ The kernels decide every distance, closest point, uvw, hit and sign in double
 with the oracle's operation order, so on the same float inputs the float32
 outputs must equal the oracle's double results rounded to float32 (bit for
 bit), and face_id must equal the oracle's lowest-index minimiser.  The
-tolerance the north star allows (1e-6 relative / 1e-7 absolute) is checked
+required tolerance (1e-6 relative / 1e-7 absolute) is checked
 as well and the maximum error reported.
 """
 
