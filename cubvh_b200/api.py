@@ -18,6 +18,7 @@ carry gradients to both through a hand-written backward kernel.
 from __future__ import annotations
 
 import ctypes
+import math
 
 import numpy as np
 import torch
@@ -39,6 +40,13 @@ def _stream_ptr(device: torch.device) -> ctypes.c_void_p:
 
 def _ptr(t) -> ctypes.c_void_p:
     return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
+
+
+def _check_out(t, shape, dtype, name):
+    """An out= tensor: host, contiguous, of the query count's shape."""
+    if t.is_cuda or t.dtype != dtype or not t.is_contiguous() or t.numel() != math.prod(shape):
+        raise ValueError(f"out {name}: expected a contiguous host {dtype} tensor of {math.prod(shape)} elements, "
+                         f"got {t.dtype} {tuple(t.shape)} on {t.device}")
 
 
 class _Handle:
@@ -178,8 +186,14 @@ class cuBVH:
         self._refit_key, self._refit_tensor = key, v
 
     # -------------------------------------------------------------- queries
-    def ray_trace(self, rays_o, rays_d):
+    def ray_trace(self, rays_o, rays_d, out=None):
         # rays_o, rays_d: torch.Tensor, float, [N, 3]
+        # out: optional (positions, face_id, depth) host tensors (float32 [..., 3],
+        # int64 [...], float32 [...]; page-locked for overlapped copies) for
+        # host rays: the rays stream through the GPU in chunks whose copies
+        # overlap the tracing, and the results are written there
+        if out is not None:
+            return self._ray_trace_host(rays_o, rays_d, out)
         rays_o = rays_o.float().contiguous()
         rays_d = rays_d.float().contiguous()
         if not rays_o.is_cuda: rays_o = rays_o.cuda()
@@ -199,6 +213,48 @@ class cuBVH:
                                         _ptr(face_id), _ptr(depth), _stream_ptr(rays_o.device)), "ray_trace")
 
         return positions.view(*prefix, 3), face_id.view(*prefix), depth.view(*prefix)
+
+    def _ray_trace_host(self, rays_o, rays_d, out):
+        if rays_o.is_cuda or rays_d.is_cuda or any(t.is_cuda for t in out):
+            raise ValueError("out= takes host (CPU) rays and host output tensors")
+        prefix = rays_o.shape[:-1]
+        ro = rays_o.float().reshape(-1, 3).contiguous()
+        rd = rays_d.float().reshape(-1, 3).contiguous()
+        N = ro.shape[0]
+        positions, face_id, depth = out
+        _check_out(positions, (N, 3), torch.float32, "positions")
+        _check_out(face_id, (N,), torch.int64, "face_id")
+        _check_out(depth, (N,), torch.float32, "depth")
+        dev = torch.device("cuda", torch.cuda.current_device())
+        with torch.cuda.device(dev):
+            check(lib().cubvh_ray_trace_host(self.impl.raw, _ptr(ro), _ptr(rd), N, _ptr(positions), _ptr(face_id),
+                                             _ptr(depth), _stream_ptr(dev)), "ray_trace")
+            torch.cuda.current_stream(dev).synchronize()
+        return positions.view(*prefix, 3), face_id.view(*prefix), depth.view(*prefix)
+
+    def _distance_host(self, positions, return_uvw, mode, out):
+        if positions.is_cuda or any(t is not None and t.is_cuda for t in out):
+            raise ValueError("out= takes host (CPU) points and host output tensors")
+        prefix = positions.shape[:-1]
+        p = positions.float().reshape(-1, 3).contiguous()
+        N = p.shape[0]
+        distances, face_id, uvw = (tuple(out) + (None,))[:3]
+        _check_out(distances, (N,), torch.float32, "distances")
+        _check_out(face_id, (N,), torch.int64, "face_id")
+        if return_uvw:
+            if uvw is None:
+                raise ValueError("return_uvw=True needs an uvw tensor in out")
+            _check_out(uvw, (N, 3), torch.float32, "uvw")
+        else:
+            uvw = None
+        dev = torch.device("cuda", torch.cuda.current_device())
+        with torch.cuda.device(dev):
+            check(lib().cubvh_signed_distance_host(self.impl.raw, _ptr(p), N, 0xFFFFFFFF if mode is None else mode,
+                                                   _ptr(distances), _ptr(face_id), _ptr(uvw), _stream_ptr(dev)),
+                  "signed_distance" if mode is not None else "unsigned_distance")
+            torch.cuda.current_stream(dev).synchronize()
+        return (distances.view(*prefix), face_id.view(*prefix),
+                uvw.view(*prefix, 3) if uvw is not None else None)
 
     def _query(self, positions, return_uvw, mode, vertices):
         positions = positions.float()
@@ -241,14 +297,25 @@ class cuBVH:
             check(rc, "signed_distance" if mode is not None else "unsigned_distance")
         return distances, face_id, uvw
 
-    def unsigned_distance(self, positions, return_uvw=False, vertices=None):
+    def unsigned_distance(self, positions, return_uvw=False, vertices=None, out=None):
         # positions: torch.Tensor, float, [N, 3]
         # vertices: optional CUDA [V, 3]: refit to them and differentiate
+        # out: optional (distances, face_id[, uvw]) host tensors for host
+        # points (as ray_trace's out; not differentiable)
+        if out is not None:
+            if vertices is not None:
+                raise ValueError("out= queries are not differentiable: pass no vertices")
+            return self._distance_host(positions, return_uvw, None, out)
         return self._query(positions, return_uvw, None, vertices)
 
-    def signed_distance(self, positions, return_uvw=False, mode="watertight", vertices=None):
+    def signed_distance(self, positions, return_uvw=False, mode="watertight", vertices=None, out=None):
         # positions: torch.Tensor, float, [N, 3]; inside is negative
-        return self._query(positions, return_uvw, _sdf_mode_to_id[mode], vertices)
+        m = _sdf_mode_to_id[mode]
+        if out is not None:
+            if vertices is not None:
+                raise ValueError("out= queries are not differentiable: pass no vertices")
+            return self._distance_host(positions, return_uvw, m, out)
+        return self._query(positions, return_uvw, m, vertices)
 
 
 def floodfill(grid, check_bounds: bool = False):

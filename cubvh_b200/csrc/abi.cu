@@ -19,8 +19,18 @@
 
 using namespace cubvh;
 
+// Streams and events of the host-buffer queries (one set per device copy,
+// created on first use): copy-in and copy-out streams beside the caller's.
+struct HostPipe {
+    cudaStream_t cin = nullptr, cout = nullptr, comp_s[2] = {nullptr, nullptr};
+    cudaEvent_t start = nullptr, in[2] = {nullptr, nullptr}, comp[2] = {nullptr, nullptr},
+                out[2] = {nullptr, nullptr};
+    bool ready = false;
+};
+
 struct DevCopy {
     int device = -1;
+    HostPipe pipe;
     CNode* nodes = nullptr;
     CTri* tris = nullptr;
     int32_t* face_vidx = nullptr;  // [F, 3] (meshes only), uploaded on first use
@@ -327,6 +337,14 @@ int cubvh_bvh_destroy(cubvh_bvh* h) {
             if (d.near_lst) cudaFree(d.near_lst);
             if (d.near_nrm) cudaFree(d.near_nrm);
             if (d.near_flag) cudaFree(d.near_flag);
+            if (d.pipe.ready) {
+                cudaStreamDestroy(d.pipe.cin); cudaStreamDestroy(d.pipe.cout);
+                cudaStreamDestroy(d.pipe.comp_s[0]); cudaStreamDestroy(d.pipe.comp_s[1]);
+                cudaEventDestroy(d.pipe.start);
+                for (int k = 0; k < 2; ++k) {
+                    cudaEventDestroy(d.pipe.in[k]); cudaEventDestroy(d.pipe.comp[k]); cudaEventDestroy(d.pipe.out[k]);
+                }
+            }
         }
     }
     if (have && !h->dev.empty()) cudaSetDevice(cur);
@@ -440,6 +458,165 @@ int cubvh_ray_trace(cubvh_bvh* h, const float* rays_o, const float* rays_d, int6
     if (e == cudaSuccess) e = e2;
     if (e != cudaSuccess) return cuda_fail(e, "ray kernel launch");
     return CUBVH_OK;
+    CUBVH_GUARD_END
+}
+
+// ------------------------------------------------------- host-buffer queries
+// Queries whose inputs and outputs are in host memory run in chunks of
+// kHostChunk queries through two device staging sets (inputs, outputs and a
+// query workspace each).  For chunk c (set k = c % 2) the copy-in stream
+// uploads its inputs once the kernels of chunk c - 2 (same set) are done,
+// compute stream k runs the kernels once the inputs are in and chunk c - 2's
+// outputs are downloaded, and the copy-out stream downloads the outputs once
+// the kernels are done: the upload of one chunk, the kernels of the previous
+// two and the download of the one before overlap, and a chunk's kernels fill
+// the SMs that the previous chunk's last packets leave idle.  Every internal
+// stream first waits for the caller's stream; the caller's stream then waits
+// for the last downloads and frees the staging memory (stream-ordered).  Host memory should be page-locked:
+// copies from or to pageable memory are staged by the driver and a download
+// to pageable memory blocks the enqueueing thread until it is done.
+}  // extern "C"
+
+namespace {
+constexpr int64_t kHostChunk = (int64_t)1 << 21;  // 2M: measured against 1M / 4M / 8M chunks
+struct HostArray {
+    void* host;
+    size_t bytes_per_query;
+};
+
+int host_pipe(DevCopy* d, HostPipe** out) {
+    HostPipe& p = d->pipe;
+    if (!p.ready) {
+        cudaError_t e = cudaSuccess;
+        auto ev = [&](cudaEvent_t* x) { if (e == cudaSuccess) e = cudaEventCreateWithFlags(x, cudaEventDisableTiming); };
+        if ((e = cudaStreamCreateWithFlags(&p.cin, cudaStreamNonBlocking)) == cudaSuccess)
+            e = cudaStreamCreateWithFlags(&p.cout, cudaStreamNonBlocking);
+        for (int k = 0; k < 2 && e == cudaSuccess; ++k) e = cudaStreamCreateWithFlags(&p.comp_s[k], cudaStreamNonBlocking);
+        ev(&p.start);
+        for (int k = 0; k < 2; ++k) { ev(&p.in[k]); ev(&p.comp[k]); ev(&p.out[k]); }
+        if (e != cudaSuccess) return cuda_fail(e, "host-buffer query streams");
+        p.ready = true;
+    }
+    *out = &p;
+    return CUBVH_OK;
+}
+
+// launch(in, out, ws, first, count, stream): the kernels of one chunk, in[i] /
+// out[i] the device copies of the i-th input / output array.
+template <class Launch>
+int run_host_pipeline(cubvh_bvh* h, DevCopy* d, cudaStream_t s, int64_t n, const std::vector<HostArray>& ins,
+                      const std::vector<HostArray>& outs, size_t ws_bytes, Launch launch) {
+    std::lock_guard<std::mutex> lk(h->mu);
+    HostPipe* p;
+    int rc = host_pipe(d, &p);
+    if (rc != CUBVH_OK) return rc;
+    const int64_t chunk = n < kHostChunk ? n : kHostChunk;
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    size_t per_set = 0;
+    for (const auto& a : ins) per_set += al(a.bytes_per_query * (size_t)chunk);
+    for (const auto& a : outs) per_set += al(a.bytes_per_query * (size_t)chunk);
+    char* base = nullptr;
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&base), 2 * (per_set + al(ws_bytes)), s);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync(host-query staging)");
+    std::vector<char*> dev_in[2], dev_out[2];
+    for (int k = 0; k < 2; ++k) {
+        char* q = base + k * per_set;
+        for (const auto& a : ins) { dev_in[k].push_back(q); q += al(a.bytes_per_query * (size_t)chunk); }
+        for (const auto& a : outs) { dev_out[k].push_back(q); q += al(a.bytes_per_query * (size_t)chunk); }
+    }
+    void* ws[2] = {base + 2 * per_set, base + 2 * per_set + al(ws_bytes)};
+    auto ok = [&](cudaError_t x) { if (e == cudaSuccess) e = x; return e == cudaSuccess; };
+    ok(cudaEventRecord(p->start, s));
+    ok(cudaStreamWaitEvent(p->cin, p->start, 0));
+    ok(cudaStreamWaitEvent(p->cout, p->start, 0));
+    ok(cudaStreamWaitEvent(p->comp_s[0], p->start, 0));
+    ok(cudaStreamWaitEvent(p->comp_s[1], p->start, 0));
+    const int64_t nchunks = (n + chunk - 1) / chunk;
+    for (int64_t c = 0; c < nchunks && e == cudaSuccess; ++c) {
+        const int k = (int)(c & 1);
+        const int64_t first = c * chunk, cnt = n - first < chunk ? n - first : chunk;
+        if (c >= 2) ok(cudaStreamWaitEvent(p->cin, p->comp[k], 0));
+        for (size_t i = 0; i < ins.size(); ++i)
+            ok(cudaMemcpyAsync(dev_in[k][i], static_cast<const char*>(ins[i].host) + first * ins[i].bytes_per_query,
+                               cnt * ins[i].bytes_per_query, cudaMemcpyHostToDevice, p->cin));
+        ok(cudaEventRecord(p->in[k], p->cin));
+        cudaStream_t cs = p->comp_s[k];
+        ok(cudaStreamWaitEvent(cs, p->in[k], 0));
+        if (c >= 2) ok(cudaStreamWaitEvent(cs, p->out[k], 0));
+        if (e == cudaSuccess) ok(launch(dev_in[k], dev_out[k], ws[k], first, cnt, cs));
+        ok(cudaEventRecord(p->comp[k], cs));
+        ok(cudaStreamWaitEvent(p->cout, p->comp[k], 0));
+        for (size_t i = 0; i < outs.size(); ++i)
+            ok(cudaMemcpyAsync(static_cast<char*>(outs[i].host) + first * outs[i].bytes_per_query, dev_out[k][i],
+                               cnt * outs[i].bytes_per_query, cudaMemcpyDeviceToHost, p->cout));
+        ok(cudaEventRecord(p->out[k], p->cout));
+    }
+    ok(cudaStreamWaitEvent(s, p->out[0], 0));
+    if (nchunks > 1) ok(cudaStreamWaitEvent(s, p->out[1], 0));
+    const cudaError_t ef = cudaFreeAsync(base, s);
+    if (e == cudaSuccess) e = ef;
+    if (e != cudaSuccess) return cuda_fail(e, "host-buffer query");
+    return CUBVH_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int cubvh_ray_trace_host(cubvh_bvh* h, const float* rays_o, const float* rays_d, int64_t n, float* positions,
+                         int64_t* face_id, float* depth, void* stream) {
+    CUBVH_GUARD_BEGIN
+    if (!h) return fail(CUBVH_ERR_INVALID, "bvh is null");
+    if (n < 0) return fail(CUBVH_ERR_INVALID, "negative ray count");
+    if (n == 0) return CUBVH_OK;
+    if (!rays_o || !rays_d || !positions || !face_id || !depth)
+        return fail(CUBVH_ERR_INVALID, "null ray or output pointer");
+    DevCopy* d;
+    const int rc = device_copy(h, &d);
+    if (rc != CUBVH_OK) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int64_t chunk = n < kHostChunk ? n : kHostChunk;
+    return run_host_pipeline(
+        h, d, s, n, {{const_cast<float*>(rays_o), 12}, {const_cast<float*>(rays_d), 12}},
+        {{positions, 12}, {face_id, 8}, {depth, 4}}, query_workspace_bytes(-1, chunk),
+        [&](const std::vector<char*>& in, const std::vector<char*>& out, void* ws, int64_t, int64_t cnt,
+            cudaStream_t cs) {
+            return launch_ray(cnt, reinterpret_cast<const float*>(in[0]), reinterpret_cast<const float*>(in[1]),
+                              reinterpret_cast<float*>(out[0]), reinterpret_cast<int64_t*>(out[1]),
+                              reinterpret_cast<float*>(out[2]), d->nodes, d->tris, ws, cs);
+        });
+    CUBVH_GUARD_END
+}
+
+int cubvh_signed_distance_host(cubvh_bvh* h, const float* points, int64_t n, uint32_t mode, float* distances,
+                               int64_t* face_id, float* uvw, void* stream) {
+    CUBVH_GUARD_BEGIN
+    if (!h) return fail(CUBVH_ERR_INVALID, "bvh is null");
+    if (n < 0) return fail(CUBVH_ERR_INVALID, "negative query count");
+    if (mode != 0 && mode != 1 && mode != 0xFFFFFFFFu)
+        return fail(CUBVH_ERR_INVALID, "mode must be 0 (watertight), 1 (raystab) or 0xFFFFFFFF (unsigned)");
+    if (n == 0) return CUBVH_OK;
+    if (!points || !distances || !face_id) return fail(CUBVH_ERR_INVALID, "points/distances/face_id is null");
+    if (n > (int64_t)UINT32_MAX) return fail(CUBVH_ERR_INVALID, "more than 2^32-1 queries in one call");
+    DevCopy* d;
+    int rc = device_copy(h, &d);
+    if (rc != CUBVH_OK) return rc;
+    const int kmode = mode == 0xFFFFFFFFu ? 0 : (int)mode + 1;
+    cudaStream_t s = (cudaStream_t)stream;
+    NearLists near;
+    if (kmode == 1 && (rc = near_lists(h, d, s, &near)) != CUBVH_OK) return rc;
+    const int64_t chunk = n < kHostChunk ? n : kHostChunk;
+    std::vector<HostArray> outs{{distances, 4}, {face_id, 8}};
+    if (uvw) outs.push_back({uvw, 12});
+    const int slot0 = (int)h->host.slot_of_face0;
+    return run_host_pipeline(
+        h, d, s, n, {{const_cast<float*>(points), 12}}, outs, query_workspace_bytes(kmode, chunk),
+        [&](const std::vector<char*>& in, const std::vector<char*>& out, void* ws, int64_t first, int64_t cnt,
+            cudaStream_t cs) {
+            return launch_distance(kmode, uvw != nullptr, cnt, reinterpret_cast<const float*>(in[0]),
+                                   reinterpret_cast<float*>(out[0]), reinterpret_cast<int64_t*>(out[1]),
+                                   uvw ? reinterpret_cast<float*>(out[2]) : nullptr, d->nodes, d->tris, slot0, near,
+                                   ws, cs, first);
+        });
     CUBVH_GUARD_END
 }
 

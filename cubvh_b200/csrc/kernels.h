@@ -59,9 +59,12 @@ struct NearLists {
     const int32_t* cnt = nullptr; const int32_t* lst = nullptr; const double* nrm = nullptr;
     bool ovf = false;
 };
+// qbase: index of query 0 within the caller's whole call (the raystab stab
+// directions follow the query index; a call split into chunks passes each
+// chunk's first index).
 cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts, float* dist, int64_t* fid,
                             float* uvw, const CNode* nodes, const CTri* tris, int slot_face0, NearLists near,
-                            void* ws, cudaStream_t stream);
+                            void* ws, cudaStream_t stream, int64_t qbase = 0);
 // any_ovf: one device int, set to 1 when some list overflowed.
 cudaError_t launch_near_lists(int64_t n_tris, const CNode* nodes, const CTri* tris, int32_t* cnt, int32_t* lst,
                               double* nrm, int* any_ovf, cudaStream_t stream);

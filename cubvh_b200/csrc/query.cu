@@ -325,6 +325,7 @@ struct Work {
     const MeshDesc* meshes;
     int64_t n;                // implicit: queries; table: packets
     int slot0;                // implicit: face-0 slot of the single BVH
+    int64_t qbase = 0;        // implicit: index of query 0 within its call (raystab streams)
     __device__ __forceinline__ int64_t packets() const { return table ? n : (n + 31) >> 5; }
     __device__ __forceinline__ void get(int64_t p, int64_t& start, int& count, int& root, int& s0,
                                         int64_t& qoff) const {
@@ -333,7 +334,7 @@ struct Work {
             const MeshDesc m = meshes[d.mesh];
             start = d.start; count = d.count; root = m.root; s0 = m.slot0; qoff = m.qoff;
         } else {
-            start = p * 32; count = (int)min((int64_t)32, n - start); root = 0; s0 = slot0; qoff = 0;
+            start = p * 32; count = (int)min((int64_t)32, n - start); root = 0; s0 = slot0; qoff = -qbase;
         }
     }
 };
@@ -1358,7 +1359,7 @@ int64_t chunk_for(int64_t n, unsigned grid) {
 
 cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts, float* dist, int64_t* fid,
                             float* uvw, const CNode* nodes, const CTri* tris, int slot_face0, NearLists near,
-                            void* ws, cudaStream_t stream) {
+                            void* ws, cudaStream_t stream, int64_t qbase) {
     if (n <= 0) return cudaSuccess;
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     char* w = static_cast<char*>(ws);
@@ -1387,7 +1388,7 @@ cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts
     if (mode == 1) w += al(sizeof(uint32_t) * n);
     uint2* heavy = reinterpret_cast<uint2*>(w);
     const int64_t hcap = heavy_cap_for(n);
-    const Work work{nullptr, nullptr, n, slot_face0};
+    const Work work{nullptr, nullptr, n, slot_face0, qbase};
 #define CUBVH_L(U, S) do { const unsigned g_ = persistent_grid(k_udf<U, S, false>, n); \
         const float ppw_ = packets_per_warp((n + 31) / 32, g_); \
         if (ppw_ >= kTailPpw) { \

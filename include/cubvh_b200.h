@@ -122,6 +122,22 @@ int cubvh_signed_distance(cubvh_bvh* bvh, const float* points, int64_t n, uint32
 int cubvh_ray_trace(cubvh_bvh* bvh, const float* rays_o, const float* rays_d, int64_t n, float* positions,
                     int64_t* face_id, float* depth, void* stream);
 
+/* Host-buffer variants of the three queries: every pointer except the
+ * handle is host memory (page-locked for asynchronous copies), the results
+ * are those of cubvh_ray_trace / cubvh_signed_distance on the same inputs,
+ * bit for bit.  The queries run in chunks of 2,097,152 whose upload, kernels
+ * and download overlap on four internal streams; on return the work is
+ * queued behind `stream` and `stream` waits for it: synchronize `stream`
+ * before reading the outputs.
+ * mode as cubvh_signed_distance, or 0xFFFFFFFF for unsigned distance.
+ * Replaces the reference's queries called with CPU tensors, which it copies
+ * to the GPU whole before tracing (cubvh/api.py:38-65, 67-126); the results
+ * stay on the GPU there. */
+int cubvh_ray_trace_host(cubvh_bvh* bvh, const float* rays_o, const float* rays_d, int64_t n, float* positions,
+                         int64_t* face_id, float* depth, void* stream);
+int cubvh_signed_distance_host(cubvh_bvh* bvh, const float* points, int64_t n, uint32_t mode, float* distances,
+                               int64_t* face_id, float* uvw, void* stream);
+
 /* Differentiable queries (no counterpart in the reference, whose cuBVH
  * detaches the vertices: cubvh/api.py:16-17).
  *

@@ -1,0 +1,92 @@
+"""Host-buffer queries (`out=`, C ABI cubvh_ray_trace_host /
+cubvh_signed_distance_host): the same results as the device-tensor calls,
+bit for bit, in one chunk and across several chunks (raystab included: its
+stab rays follow the query index within the whole call)."""
+
+import numpy as np
+import pytest
+import torch
+
+import cubvh_b200 as cubvh
+from cubvh_b200 import workloads as W
+
+CHUNK = 1 << 21   # queries per chunk of the host pipeline
+
+
+def _host_like(shape, dtype, pinned):
+    return torch.empty(shape, dtype=dtype, pin_memory=pinned)
+
+
+def _rays_equal(bvh, ro, rd, dev, pinned=True):
+    n = ro.shape[0]
+    want = bvh.ray_trace(ro.to(dev), rd.to(dev))
+    out = (_host_like((n, 3), torch.float32, pinned), _host_like((n,), torch.int64, pinned),
+           _host_like((n,), torch.float32, pinned))
+    got = bvh.ray_trace(ro, rd, out=out)
+    for a, b in zip(got, want):
+        assert torch.equal(a, b.cpu())
+
+
+def _dist_equal(bvh, pts, dev, mode, uvw=False, pinned=True):
+    n = pts.shape[0]
+    out = [_host_like((n,), torch.float32, pinned), _host_like((n,), torch.int64, pinned)]
+    if uvw:
+        out.append(_host_like((n, 3), torch.float32, pinned))
+    if mode is None:
+        want = bvh.unsigned_distance(pts.to(dev), return_uvw=uvw)
+        got = bvh.unsigned_distance(pts, return_uvw=uvw, out=out)
+    else:
+        want = bvh.signed_distance(pts.to(dev), return_uvw=uvw, mode=mode)
+        got = bvh.signed_distance(pts, return_uvw=uvw, mode=mode, out=out)
+    for a, b in zip(got, want):
+        if b is None:
+            assert a is None
+        else:
+            assert torch.equal(a, b.cpu())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("pinned", [True, False])
+def test_host_queries_one_chunk(dev, pinned):
+    v, f = W.displaced_icosphere(4, 1)
+    bvh = cubvh.cuBVH(v, f)
+    ro, rd = W.camera_rays(2, 64, 50.0, 2.5, 1)
+    _rays_equal(bvh, torch.from_numpy(ro), torch.from_numpy(rd), dev, pinned)
+    pts = torch.from_numpy(W.uniform_points(5000, 3))
+    _dist_equal(bvh, pts, dev, None, uvw=True, pinned=pinned)
+    _dist_equal(bvh, pts, dev, "watertight", pinned=pinned)
+    _dist_equal(bvh, pts, dev, "raystab", pinned=pinned)
+
+
+@pytest.mark.gpu
+def test_host_queries_several_chunks(dev):
+    n = 2 * CHUNK + 123_457          # three chunks, the last one partial
+    v, f = W.icosphere(3, 0.8)
+    bvh = cubvh.cuBVH(v, f)
+    rng = np.random.default_rng(17)
+    pts = torch.from_numpy(rng.uniform(-1, 1, (n, 3)).astype(np.float32))
+    _dist_equal(bvh, pts, dev, None)
+    _dist_equal(bvh, pts, dev, "raystab")
+    _dist_equal(bvh, pts, dev, "watertight")
+    ro = torch.from_numpy(np.repeat(np.array([[0.0, 0.0, 2.5]], np.float32), n, 0))
+    d = rng.standard_normal((n, 3)).astype(np.float32)
+    d[:, 2] = -np.abs(d[:, 2]) - 1.0
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    _rays_equal(bvh, ro, torch.from_numpy(d), dev)
+
+
+def test_host_queries_argument_checks():
+    """Host-buffer calls check their out= tensors before touching the GPU."""
+    v, f = W.icosphere(2, 0.8)
+    bvh = cubvh.cuBVH(v, f)
+    pts = torch.zeros(10, 3)
+    with pytest.raises(ValueError):
+        bvh.unsigned_distance(pts, out=(torch.empty(10, dtype=torch.float64), torch.empty(10, dtype=torch.int64)))
+    with pytest.raises(ValueError):
+        bvh.unsigned_distance(pts, out=(torch.empty(9), torch.empty(10, dtype=torch.int64)))
+    with pytest.raises(ValueError):
+        bvh.unsigned_distance(pts, return_uvw=True, out=(torch.empty(10), torch.empty(10, dtype=torch.int64)))
+    with pytest.raises(ValueError):
+        bvh.ray_trace(pts, pts, out=(torch.empty(10, 3), torch.empty(10, dtype=torch.int32), torch.empty(10)))
+    with pytest.raises(ValueError):
+        bvh.signed_distance(pts, vertices=torch.zeros(4, 3), out=(torch.empty(10), torch.empty(10, dtype=torch.int64)))
