@@ -13,9 +13,10 @@ than L2 (805 MB of rays), so no L2 flush is inserted between steps.
 
 ``value`` times the kernels with inputs and outputs resident in HBM; ``e2e``
 times the public API with host tensors (cuBVH.ray_trace / signed_distance /
-unsigned_distance with ``out=`` pinned host tensors): every input is copied
-to the GPU and every output back inside the timed region, the copies of one
-chunk overlapping the kernels of the next.  ``--impl reference`` times the reference's algorithm restated on the
+unsigned_distance with ``out=`` pinned host tensors, ``non_blocking`` on one
+stream per op): every input is copied to the GPU and every output back
+inside the timed region, the copies of one chunk (and of one op) overlapping
+the kernels of another.  ``--impl reference`` times the reference's algorithm restated on the
 CPU (the oracle's FP32 mirror of its BVH4 build and traversals) on all host
 cores, on a bounded sample of the same workload per step.
 
@@ -497,12 +498,15 @@ def run_ours(args):
     e2e_steps = max(2, min(args.steps, 5))
     pinned_out = {}
 
+    op_streams = [torch.cuda.Stream(dev) for _ in host_in]
+
     def e2e_step():
         # host tensors in and out: each call streams its queries through the GPU
-        # in chunks (upload, kernels and download overlapped) and returns with
-        # the results in the pinned output tensors
+        # in chunks (upload, kernels and download overlapped); the ops are issued
+        # non-blocking on one stream each, so one op's copies overlap another's
+        # kernels, and the step ends when every result is in its pinned tensor
         h2d = d2h = 0
-        for op, tensors in host_in:
+        for (op, tensors), ost in zip(host_in, op_streams):
             h2d += sum(t.numel() * t.element_size() for t in tensors)
             n = tensors[0].shape[0]
             if op not in pinned_out:
@@ -514,15 +518,18 @@ def run_ours(args):
                         shapes.append(((n, 3), torch.float32))
                 pinned_out[op] = [torch.empty(sh, dtype=dt, pin_memory=True) for sh, dt in shapes]
             outs = pinned_out[op]
-            if op == "ray":
-                bvh.ray_trace(tensors[0], tensors[1], out=outs)
-            elif op == "sdf_watertight":
-                bvh.signed_distance(tensors[0], mode="watertight", out=outs)
-            elif op == "sdf_raystab":
-                bvh.signed_distance(tensors[0], mode="raystab", out=outs)
-            else:
-                bvh.unsigned_distance(tensors[0], return_uvw=(op == "udf_uvw"), out=outs)
+            with torch.cuda.stream(ost):
+                if op == "ray":
+                    bvh.ray_trace(tensors[0], tensors[1], out=outs, non_blocking=True)
+                elif op == "sdf_watertight":
+                    bvh.signed_distance(tensors[0], mode="watertight", out=outs, non_blocking=True)
+                elif op == "sdf_raystab":
+                    bvh.signed_distance(tensors[0], mode="raystab", out=outs, non_blocking=True)
+                else:
+                    bvh.unsigned_distance(tensors[0], return_uvw=(op == "udf_uvw"), out=outs, non_blocking=True)
             d2h += sum(t.numel() * t.element_size() for t in outs)
+        for ost in op_streams:
+            ost.synchronize()
         return h2d, d2h
 
     for _ in range(3):  # warm-up: first calls grow the allocators' pools

@@ -42,6 +42,13 @@ def _ptr(t) -> ctypes.c_void_p:
     return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
 
 
+def _check_async_input(t, name):
+    """A non_blocking out= call reads its host inputs after returning: they
+    must not be temporaries of a dtype or layout conversion."""
+    if t.dtype != torch.float32 or not t.is_contiguous():
+        raise ValueError(f"non_blocking: {name} must be a contiguous float32 host tensor")
+
+
 def _check_out(t, shape, dtype, name):
     """An out= tensor: host, contiguous, of the query count's shape."""
     if t.is_cuda or t.dtype != dtype or not t.is_contiguous() or t.numel() != math.prod(shape):
@@ -186,14 +193,18 @@ class cuBVH:
         self._refit_key, self._refit_tensor = key, v
 
     # -------------------------------------------------------------- queries
-    def ray_trace(self, rays_o, rays_d, out=None):
+    def ray_trace(self, rays_o, rays_d, out=None, non_blocking=False):
         # rays_o, rays_d: torch.Tensor, float, [N, 3]
         # out: optional (positions, face_id, depth) host tensors (float32 [..., 3],
         # int64 [...], float32 [...]; page-locked for overlapped copies) for
         # host rays: the rays stream through the GPU in chunks whose copies
-        # overlap the tracing, and the results are written there
+        # overlap the tracing, and the results are written there.
+        # non_blocking (with out=): return once the work is queued on the
+        # current stream; the outputs are valid after that stream is
+        # synchronized, and the inputs must stay alive until then (they must
+        # be contiguous float32 already).  Calls on different streams overlap.
         if out is not None:
-            return self._ray_trace_host(rays_o, rays_d, out)
+            return self._ray_trace_host(rays_o, rays_d, out, non_blocking)
         rays_o = rays_o.float().contiguous()
         rays_d = rays_d.float().contiguous()
         if not rays_o.is_cuda: rays_o = rays_o.cuda()
@@ -214,9 +225,11 @@ class cuBVH:
 
         return positions.view(*prefix, 3), face_id.view(*prefix), depth.view(*prefix)
 
-    def _ray_trace_host(self, rays_o, rays_d, out):
+    def _ray_trace_host(self, rays_o, rays_d, out, non_blocking=False):
         if rays_o.is_cuda or rays_d.is_cuda or any(t.is_cuda for t in out):
             raise ValueError("out= takes host (CPU) rays and host output tensors")
+        if non_blocking:
+            _check_async_input(rays_o, "rays_o"); _check_async_input(rays_d, "rays_d")
         prefix = rays_o.shape[:-1]
         ro = rays_o.float().reshape(-1, 3).contiguous()
         rd = rays_d.float().reshape(-1, 3).contiguous()
@@ -229,12 +242,15 @@ class cuBVH:
         with torch.cuda.device(dev):
             check(lib().cubvh_ray_trace_host(self.impl.raw, _ptr(ro), _ptr(rd), N, _ptr(positions), _ptr(face_id),
                                              _ptr(depth), _stream_ptr(dev)), "ray_trace")
-            torch.cuda.current_stream(dev).synchronize()
+            if not non_blocking:
+                torch.cuda.current_stream(dev).synchronize()
         return positions.view(*prefix, 3), face_id.view(*prefix), depth.view(*prefix)
 
-    def _distance_host(self, positions, return_uvw, mode, out):
+    def _distance_host(self, positions, return_uvw, mode, out, non_blocking=False):
         if positions.is_cuda or any(t is not None and t.is_cuda for t in out):
             raise ValueError("out= takes host (CPU) points and host output tensors")
+        if non_blocking:
+            _check_async_input(positions, "positions")
         prefix = positions.shape[:-1]
         p = positions.float().reshape(-1, 3).contiguous()
         N = p.shape[0]
@@ -252,7 +268,8 @@ class cuBVH:
             check(lib().cubvh_signed_distance_host(self.impl.raw, _ptr(p), N, 0xFFFFFFFF if mode is None else mode,
                                                    _ptr(distances), _ptr(face_id), _ptr(uvw), _stream_ptr(dev)),
                   "signed_distance" if mode is not None else "unsigned_distance")
-            torch.cuda.current_stream(dev).synchronize()
+            if not non_blocking:
+                torch.cuda.current_stream(dev).synchronize()
         return (distances.view(*prefix), face_id.view(*prefix),
                 uvw.view(*prefix, 3) if uvw is not None else None)
 
@@ -297,24 +314,25 @@ class cuBVH:
             check(rc, "signed_distance" if mode is not None else "unsigned_distance")
         return distances, face_id, uvw
 
-    def unsigned_distance(self, positions, return_uvw=False, vertices=None, out=None):
+    def unsigned_distance(self, positions, return_uvw=False, vertices=None, out=None, non_blocking=False):
         # positions: torch.Tensor, float, [N, 3]
         # vertices: optional CUDA [V, 3]: refit to them and differentiate
-        # out: optional (distances, face_id[, uvw]) host tensors for host
-        # points (as ray_trace's out; not differentiable)
+        # out, non_blocking: optional (distances, face_id[, uvw]) host tensors
+        # for host points, as in ray_trace (not differentiable)
         if out is not None:
             if vertices is not None:
                 raise ValueError("out= queries are not differentiable: pass no vertices")
-            return self._distance_host(positions, return_uvw, None, out)
+            return self._distance_host(positions, return_uvw, None, out, non_blocking)
         return self._query(positions, return_uvw, None, vertices)
 
-    def signed_distance(self, positions, return_uvw=False, mode="watertight", vertices=None, out=None):
+    def signed_distance(self, positions, return_uvw=False, mode="watertight", vertices=None, out=None,
+                        non_blocking=False):
         # positions: torch.Tensor, float, [N, 3]; inside is negative
         m = _sdf_mode_to_id[mode]
         if out is not None:
             if vertices is not None:
                 raise ValueError("out= queries are not differentiable: pass no vertices")
-            return self._distance_host(positions, return_uvw, m, out)
+            return self._distance_host(positions, return_uvw, m, out, non_blocking)
         return self._query(positions, return_uvw, m, vertices)
 
 

@@ -19,18 +19,23 @@
 
 using namespace cubvh;
 
-// Streams and events of the host-buffer queries (one set per device copy,
-// created on first use): copy-in and copy-out streams beside the caller's.
+// Streams and events of the host-buffer queries: one set per caller stream
+// (up to kMaxPipes per device copy, created on first use), so that calls
+// issued on different streams overlap (one call's copies run beside another
+// call's kernels) while calls on one stream stay in order.
 struct HostPipe {
+    cudaStream_t caller = nullptr;
     cudaStream_t cin = nullptr, cout = nullptr, comp_s[2] = {nullptr, nullptr};
     cudaEvent_t start = nullptr, in[2] = {nullptr, nullptr}, comp[2] = {nullptr, nullptr},
                 out[2] = {nullptr, nullptr};
+    char* stage = nullptr;         // staging sets and workspaces, kept between calls
+    size_t stage_bytes = 0;
     bool ready = false;
 };
 
 struct DevCopy {
     int device = -1;
-    HostPipe pipe;
+    std::deque<HostPipe> pipes;
     CNode* nodes = nullptr;
     CTri* tris = nullptr;
     int32_t* face_vidx = nullptr;  // [F, 3] (meshes only), uploaded on first use
@@ -337,12 +342,14 @@ int cubvh_bvh_destroy(cubvh_bvh* h) {
             if (d.near_lst) cudaFree(d.near_lst);
             if (d.near_nrm) cudaFree(d.near_nrm);
             if (d.near_flag) cudaFree(d.near_flag);
-            if (d.pipe.ready) {
-                cudaStreamDestroy(d.pipe.cin); cudaStreamDestroy(d.pipe.cout);
-                cudaStreamDestroy(d.pipe.comp_s[0]); cudaStreamDestroy(d.pipe.comp_s[1]);
-                cudaEventDestroy(d.pipe.start);
+            for (auto& p : d.pipes) {
+                if (p.stage) cudaFree(p.stage);
+                if (!p.ready) continue;
+                cudaStreamDestroy(p.cin); cudaStreamDestroy(p.cout);
+                cudaStreamDestroy(p.comp_s[0]); cudaStreamDestroy(p.comp_s[1]);
+                cudaEventDestroy(p.start);
                 for (int k = 0; k < 2; ++k) {
-                    cudaEventDestroy(d.pipe.in[k]); cudaEventDestroy(d.pipe.comp[k]); cudaEventDestroy(d.pipe.out[k]);
+                    cudaEventDestroy(p.in[k]); cudaEventDestroy(p.comp[k]); cudaEventDestroy(p.out[k]);
                 }
             }
         }
@@ -472,7 +479,9 @@ int cubvh_ray_trace(cubvh_bvh* h, const float* rays_o, const float* rays_d, int6
 // two and the download of the one before overlap, and a chunk's kernels fill
 // the SMs that the previous chunk's last packets leave idle.  Every internal
 // stream first waits for the caller's stream; the caller's stream then waits
-// for the last downloads and frees the staging memory (stream-ordered).  Host memory should be page-locked:
+// for the last downloads.  The staging memory belongs to the pipe (one per
+// caller stream) and is kept for the next call: allocated on first use,
+// regrown when a call needs more, freed with the BVH handle.  Host memory should be page-locked:
 // copies from or to pageable memory are staged by the driver and a download
 // to pageable memory blocks the enqueueing thread until it is done.
 }  // extern "C"
@@ -484,8 +493,15 @@ struct HostArray {
     size_t bytes_per_query;
 };
 
-int host_pipe(DevCopy* d, HostPipe** out) {
-    HostPipe& p = d->pipe;
+constexpr size_t kMaxPipes = 8;
+// The caller stream's pipe (the last one is shared once kMaxPipes exist).
+int host_pipe(DevCopy* d, cudaStream_t caller, HostPipe** out) {
+    for (auto& q : d->pipes)
+        if (q.ready && q.caller == caller) { *out = &q; return CUBVH_OK; }
+    if (d->pipes.size() >= kMaxPipes) { *out = &d->pipes.back(); return CUBVH_OK; }
+    d->pipes.emplace_back();
+    HostPipe& p = d->pipes.back();
+    p.caller = caller;
     if (!p.ready) {
         cudaError_t e = cudaSuccess;
         auto ev = [&](cudaEvent_t* x) { if (e == cudaSuccess) e = cudaEventCreateWithFlags(x, cudaEventDisableTiming); };
@@ -494,7 +510,10 @@ int host_pipe(DevCopy* d, HostPipe** out) {
         for (int k = 0; k < 2 && e == cudaSuccess; ++k) e = cudaStreamCreateWithFlags(&p.comp_s[k], cudaStreamNonBlocking);
         ev(&p.start);
         for (int k = 0; k < 2; ++k) { ev(&p.in[k]); ev(&p.comp[k]); ev(&p.out[k]); }
-        if (e != cudaSuccess) return cuda_fail(e, "host-buffer query streams");
+        if (e != cudaSuccess) {
+            d->pipes.pop_back();
+            return cuda_fail(e, "host-buffer query streams");
+        }
         p.ready = true;
     }
     *out = &p;
@@ -507,17 +526,34 @@ template <class Launch>
 int run_host_pipeline(cubvh_bvh* h, DevCopy* d, cudaStream_t s, int64_t n, const std::vector<HostArray>& ins,
                       const std::vector<HostArray>& outs, size_t ws_bytes, Launch launch) {
     std::lock_guard<std::mutex> lk(h->mu);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(s, &cap);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamIsCapturing");
+    if (cap != cudaStreamCaptureStatusNone)
+        return fail(CUBVH_ERR_INVALID, "host-buffer queries cannot run while the stream is being captured");
     HostPipe* p;
-    int rc = host_pipe(d, &p);
+    int rc = host_pipe(d, s, &p);
     if (rc != CUBVH_OK) return rc;
     const int64_t chunk = n < kHostChunk ? n : kHostChunk;
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     size_t per_set = 0;
     for (const auto& a : ins) per_set += al(a.bytes_per_query * (size_t)chunk);
     for (const auto& a : outs) per_set += al(a.bytes_per_query * (size_t)chunk);
-    char* base = nullptr;
-    cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&base), 2 * (per_set + al(ws_bytes)), s);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync(host-query staging)");
+    const size_t need = 2 * (per_set + al(ws_bytes));
+    if (need > p->stage_bytes) {  // grow: wait until the previous calls on this pipe are done with it
+        if ((e = cudaStreamSynchronize(p->cout)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(p->comp_s[0])) != cudaSuccess ||
+            (e = cudaStreamSynchronize(p->comp_s[1])) != cudaSuccess ||
+            (e = cudaStreamSynchronize(p->cin)) != cudaSuccess)
+            return cuda_fail(e, "host-query staging");
+        if (p->stage) cudaFree(p->stage);
+        p->stage = nullptr;
+        p->stage_bytes = 0;
+        if ((e = cudaMalloc(reinterpret_cast<void**>(&p->stage), need)) != cudaSuccess)
+            return cuda_fail(e, "cudaMalloc(host-query staging)");
+        p->stage_bytes = need;
+    }
+    char* base = p->stage;
     std::vector<char*> dev_in[2], dev_out[2];
     for (int k = 0; k < 2; ++k) {
         char* q = base + k * per_set;
@@ -527,10 +563,14 @@ int run_host_pipeline(cubvh_bvh* h, DevCopy* d, cudaStream_t s, int64_t n, const
     void* ws[2] = {base + 2 * per_set, base + 2 * per_set + al(ws_bytes)};
     auto ok = [&](cudaError_t x) { if (e == cudaSuccess) e = x; return e == cudaSuccess; };
     ok(cudaEventRecord(p->start, s));
-    ok(cudaStreamWaitEvent(p->cin, p->start, 0));
-    ok(cudaStreamWaitEvent(p->cout, p->start, 0));
-    ok(cudaStreamWaitEvent(p->comp_s[0], p->start, 0));
-    ok(cudaStreamWaitEvent(p->comp_s[1], p->start, 0));
+    // every internal stream starts after the caller's earlier work and after
+    // the previous call on this pipe has downloaded its last chunks (its
+    // uploads and kernels come before those); an event never recorded is a no-op
+    for (cudaStream_t q : {p->cin, p->cout, p->comp_s[0], p->comp_s[1]}) {
+        ok(cudaStreamWaitEvent(q, p->start, 0));
+        ok(cudaStreamWaitEvent(q, p->out[0], 0));
+        ok(cudaStreamWaitEvent(q, p->out[1], 0));
+    }
     const int64_t nchunks = (n + chunk - 1) / chunk;
     for (int64_t c = 0; c < nchunks && e == cudaSuccess; ++c) {
         const int k = (int)(c & 1);
@@ -553,8 +593,6 @@ int run_host_pipeline(cubvh_bvh* h, DevCopy* d, cudaStream_t s, int64_t n, const
     }
     ok(cudaStreamWaitEvent(s, p->out[0], 0));
     if (nchunks > 1) ok(cudaStreamWaitEvent(s, p->out[1], 0));
-    const cudaError_t ef = cudaFreeAsync(base, s);
-    if (e == cudaSuccess) e = ef;
     if (e != cudaSuccess) return cuda_fail(e, "host-buffer query");
     return CUBVH_OK;
 }

@@ -128,7 +128,12 @@ int cubvh_ray_trace(cubvh_bvh* bvh, const float* rays_o, const float* rays_d, in
  * bit for bit.  The queries run in chunks of 2,097,152 whose upload, kernels
  * and download overlap on four internal streams; on return the work is
  * queued behind `stream` and `stream` waits for it: synchronize `stream`
- * before reading the outputs.
+ * before reading the outputs.  Calls on different streams overlap.  The
+ * device staging memory (two chunks of inputs, outputs and workspace:
+ * ~200 MB for rays) is kept per caller stream until the BVH is destroyed;
+ * a call that needs more than its stream's staging synchronizes that
+ * staging's earlier work and reallocates it.  A stream being captured into
+ * a graph is rejected (status 1).
  * mode as cubvh_signed_distance, or 0xFFFFFFFF for unsigned distance.
  * Replaces the reference's queries called with CPU tensors, which it copies
  * to the GPU whole before tracing (cubvh/api.py:38-65, 67-126); the results

@@ -90,3 +90,34 @@ def test_host_queries_argument_checks():
         bvh.ray_trace(pts, pts, out=(torch.empty(10, 3), torch.empty(10, dtype=torch.int32), torch.empty(10)))
     with pytest.raises(ValueError):
         bvh.signed_distance(pts, vertices=torch.zeros(4, 3), out=(torch.empty(10), torch.empty(10, dtype=torch.int64)))
+
+
+@pytest.mark.gpu
+def test_host_queries_non_blocking_two_streams(dev):
+    """non_blocking calls on two streams overlap (separate internal streams
+    per caller stream) and give the blocking results once synchronized."""
+    v, f = W.displaced_icosphere(4, 1)
+    bvh = cubvh.cuBVH(v, f)
+    ro, rd = (torch.from_numpy(x).pin_memory() for x in W.camera_rays(4, 512, 50.0, 2.5, 1))
+    pts = torch.from_numpy(W.uniform_points(3 * CHUNK // 2, 5)).pin_memory()
+    n, m = ro.shape[0], pts.shape[0]
+    want_r = bvh.ray_trace(ro.to(dev), rd.to(dev))
+    want_s = bvh.signed_distance(pts.to(dev), mode="watertight")
+    out_r = (torch.empty((n, 3), pin_memory=True), torch.empty(n, dtype=torch.int64, pin_memory=True),
+             torch.empty(n, pin_memory=True))
+    out_s = (torch.empty(m, pin_memory=True), torch.empty(m, dtype=torch.int64, pin_memory=True))
+    s1, s2 = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    for _ in range(2):
+        for t in out_r + out_s:
+            t.zero_()
+        with torch.cuda.stream(s1):
+            bvh.ray_trace(ro, rd, out=out_r, non_blocking=True)
+        with torch.cuda.stream(s2):
+            bvh.signed_distance(pts, mode="watertight", out=out_s, non_blocking=True)
+        s1.synchronize(); s2.synchronize()
+        for a, b in zip(out_r, want_r):
+            assert torch.equal(a, b.cpu())
+        for a, b in zip(out_s, want_s):
+            assert torch.equal(a, b.cpu())
+    with pytest.raises(ValueError):
+        bvh.ray_trace(ro.double(), rd, out=out_r, non_blocking=True)
