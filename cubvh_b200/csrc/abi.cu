@@ -59,6 +59,19 @@ struct cubvh_bvh {
 };
 
 namespace {
+std::mutex g_const_mu;
+std::vector<int> g_const_ready;  // devices whose __constant__ tables are set
+}  // namespace
+
+cudaError_t cubvh::ensure_constants(int device) {
+    std::lock_guard<std::mutex> lk(g_const_mu);
+    for (int d : g_const_ready) if (d == device) return cudaSuccess;
+    const cudaError_t e = upload_constants();
+    if (e == cudaSuccess) g_const_ready.push_back(device);
+    return e;
+}
+
+namespace {
 
 thread_local std::string g_err;
 
@@ -70,16 +83,6 @@ int cuda_fail(cudaError_t e, const char* what) {
     return fail(CUBVH_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-std::mutex g_const_mu;
-std::vector<int> g_const_ready;  // devices whose __constant__ tables are set
-
-cudaError_t ensure_constants(int device) {
-    std::lock_guard<std::mutex> lk(g_const_mu);
-    for (int d : g_const_ready) if (d == device) return cudaSuccess;
-    const cudaError_t e = upload_constants();
-    if (e == cudaSuccess) g_const_ready.push_back(device);
-    return e;
-}
 
 // Device copy of the BVH on the current device (uploaded on first use).
 int device_copy(cubvh_bvh* h, DevCopy** out) {

@@ -83,6 +83,9 @@ int arena_device(cubvh_arena* a) {
         (e = cudaMemcpy(a->d_gslot, a->gslot.data(), sb, cudaMemcpyHostToDevice)) != cudaSuccess)
         return cuda_err(e, "arena upload");
     a->device = dev;
+    // the raystab sign pass reads the stab-direction tables: set them on this
+    // device even when no single-BVH query has run on it yet
+    if ((e = ensure_constants(dev)) != cudaSuccess) return cuda_err(e, "constant upload");
     return CUBVH_OK;
 }
 
@@ -227,6 +230,10 @@ int cubvh_arena_create_device(int32_t n_meshes, const float* const* vertices, co
         return cuda_err(e, "arena face offsets");
     }
     a->device = dev;
+    if ((e = ensure_constants(dev)) != cudaSuccess) {
+        cubvh_arena_destroy(a);
+        return cuda_err(e, "constant upload");
+    }
     *out = a;
     return CUBVH_OK;
     ARENA_GUARD_END

@@ -10,6 +10,9 @@
 namespace cubvh {
 
 cudaError_t upload_constants();
+// upload_constants() once per device (the current one must be `device`):
+// every entry point that launches query kernels on a device calls it first.
+cudaError_t ensure_constants(int device);
 
 // Arena work descriptors (query.cu): a packet is up to 32 consecutive
 // positions of the (sorted) query order, all on one mesh.

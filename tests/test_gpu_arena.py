@@ -121,3 +121,35 @@ def test_autotuner_picks_leaf_sizes(dev):
     ref.set_queries([len(q) for q in qs], modes)
     d2, f2, _ = ref.distance(torch.from_numpy(np.concatenate(qs)).to(dev))
     assert torch.equal(d, d2) and torch.equal(fid, f2)     # leaf size never changes results
+
+
+_FIRST_IN_PROCESS = r"""
+import sys
+import numpy as np
+import torch
+sys.path.insert(0, sys.argv[1])
+import cubvh_b200 as cubvh
+from cubvh_b200 import workloads as W
+v, f = W.displaced_icosphere(3, 1)
+rng = np.random.default_rng(3)
+lo, hi = v.min(0), v.max(0)
+q = ((lo + hi) / 2 + rng.uniform(-1, 1, (3000, 3)) * (hi - lo) / 2 * 1.1).astype(np.float32)
+arena = cubvh.BVHArena([(v, f)])          # the process's first GPU work
+arena.set_queries([3000], ["raystab"])
+d, fid, _ = arena.distance(torch.from_numpy(q).cuda())
+rd, rf, _ = cubvh.cuBVH(v, f).signed_distance(torch.from_numpy(q).cuda(), mode="raystab")
+assert torch.equal(d, rd) and torch.equal(fid, rf), "arena raystab differs from cuBVH"
+assert (d < 0).any() and (d > 0).any()
+print("ok")
+"""
+
+
+def test_arena_raystab_first_in_process():
+    """An arena's raystab pass in a process where no single-BVH query ran
+    before: the stab-direction tables must be set by the arena itself."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", _FIRST_IN_PROCESS, root], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout + r.stderr
