@@ -694,11 +694,14 @@ def run_ours_fwd_bwd(args):
         arena = cubvh.BVHArena(meshes, leaf_sizes=leaves)
         arena_host_s = time.perf_counter() - t0
         cubvh.BVHArena(meshes[:2], leaf_sizes=leaves[:2], device_build=True)  # warm-up
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        arena_dev = cubvh.BVHArena(meshes, leaf_sizes=leaves, device_build=True)
-        torch.cuda.synchronize()
-        arena_dev_s = time.perf_counter() - t0
+        arena_dev, arena_dev_s = None, float("inf")
+        for _ in range(3):  # best of 3 whole-arena builds (host concatenation, upload, GPU build)
+            del arena_dev
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            arena_dev = cubvh.BVHArena(meshes, leaf_sizes=leaves, device_build=True)
+            torch.cuda.synchronize()
+            arena_dev_s = min(arena_dev_s, time.perf_counter() - t0)
         counts = [len(q) for q in qs]
         arena.set_queries(counts, modes, device=dev)
         pts = torch.from_numpy(np.concatenate(qs)).to(dev)
