@@ -596,7 +596,12 @@ int run_host_pipeline(cubvh_bvh* h, DevCopy* d, cudaStream_t s, int64_t n, const
     }
     ok(cudaStreamWaitEvent(s, p->out[0], 0));
     if (nchunks > 1) ok(cudaStreamWaitEvent(s, p->out[1], 0));
-    if (e != cudaSuccess) return cuda_fail(e, "host-buffer query");
+    if (e != cudaSuccess) {
+        // copies already queued may still read or write the caller's host
+        // buffers: let them finish before reporting the error
+        for (cudaStream_t q : {p->cin, p->comp_s[0], p->comp_s[1], p->cout}) cudaStreamSynchronize(q);
+        return cuda_fail(e, "host-buffer query");
+    }
     return CUBVH_OK;
 }
 }  // namespace
