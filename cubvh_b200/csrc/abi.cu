@@ -506,11 +506,15 @@ int host_pipe(DevCopy* d, cudaStream_t caller, HostPipe** out) {
     HostPipe& p = d->pipes.back();
     p.caller = caller;
     if (!p.ready) {
-        cudaError_t e = cudaSuccess;
+        // the internal streams take the caller stream's priority: a caller can
+        // give a transfer-bound batch's kernels precedence over others
+        int prio = 0;
+        cudaError_t e = cudaStreamGetPriority(caller, &prio);
         auto ev = [&](cudaEvent_t* x) { if (e == cudaSuccess) e = cudaEventCreateWithFlags(x, cudaEventDisableTiming); };
-        if ((e = cudaStreamCreateWithFlags(&p.cin, cudaStreamNonBlocking)) == cudaSuccess)
-            e = cudaStreamCreateWithFlags(&p.cout, cudaStreamNonBlocking);
-        for (int k = 0; k < 2 && e == cudaSuccess; ++k) e = cudaStreamCreateWithFlags(&p.comp_s[k], cudaStreamNonBlocking);
+        auto mk = [&](cudaStream_t* x) {
+            if (e == cudaSuccess) e = cudaStreamCreateWithPriority(x, cudaStreamNonBlocking, prio);
+        };
+        mk(&p.cin); mk(&p.cout); mk(&p.comp_s[0]); mk(&p.comp_s[1]);
         ev(&p.start);
         for (int k = 0; k < 2; ++k) { ev(&p.in[k]); ev(&p.comp[k]); ev(&p.out[k]); }
         if (e != cudaSuccess) {
