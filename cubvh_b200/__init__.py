@@ -10,7 +10,7 @@
 """
 
 from ._lib import version
-from .api import cuBVH, floodfill, udf_to_sdf
+from .api import cuBVH, floodfill, sparse_marching_cubes, udf_to_sdf
 from .arena import BVHArena
 
-__all__ = ["cuBVH", "floodfill", "udf_to_sdf", "BVHArena", "version"]
+__all__ = ["cuBVH", "floodfill", "udf_to_sdf", "sparse_marching_cubes", "BVHArena", "version"]

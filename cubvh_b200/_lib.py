@@ -43,6 +43,10 @@ _SIGS = {
     "cubvh_floodfill_check": [c_vp, c_int, c_int, c_int, c_int, c_vp],
     "cubvh_udf_to_sdf": [c_vp, c_int, c_int, c_int, c_int, ctypes.c_float, c_vp, c_vp, c_sz, c_vp],
     "cubvh_bvh_refit": [c_vp, c_vp, c_i64, c_vp],
+    "cubvh_sparse_marching_cubes": [c_vp, c_vp, c_i64, ctypes.c_float, c_int, c_vp, ctypes.POINTER(c_vp),
+                                    ctypes.POINTER(c_i64), ctypes.POINTER(c_i64)],
+    "cubvh_sparse_mc_fetch": [c_vp, c_vp, c_vp, c_vp],
+    "cubvh_sparse_mc_free": [c_vp],
     "cubvh_arena_create": [ctypes.c_int32, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(c_vp)],
     "cubvh_arena_create_device": [ctypes.c_int32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(c_vp)],
     "cubvh_arena_destroy": [c_vp],

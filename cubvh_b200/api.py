@@ -26,7 +26,7 @@ import torch
 from . import _lib
 from ._lib import check, lib
 
-__all__ = ["cuBVH", "floodfill"]
+__all__ = ["cuBVH", "floodfill", "udf_to_sdf", "sparse_marching_cubes"]
 
 _sdf_mode_to_id = {
     "watertight": 0,
@@ -361,6 +361,43 @@ def floodfill(grid, check_bounds: bool = False):
         if check_bounds:
             check(lib().cubvh_floodfill_check(_ptr(ws), B, H, W, D, stream), "floodfill")
     return mask.squeeze(0) if squeeze else mask
+
+
+def sparse_marching_cubes(coords, corners, iso, ensure_consistency=False):
+    # coords: torch.Tensor, int32, [N, 3] voxel coordinates
+    # corners: torch.Tensor, float32, [N, 8] corner values, corner order
+    #   (0,0,0), (1,0,0), (1,1,0), (0,1,0), (0,0,1), (1,0,1), (1,1,1), (0,1,1)
+    # iso: float; ensure_consistency: average the values of shared corners first
+    # return: vertices float32 [M, 3] (voxel units), triangles int32 [T, 3], on
+    # the GPU.  Same vertex array as the reference (one vertex per cut voxel
+    # edge, merged, sorted by edge); the triangulation is this library's own
+    # (closed and consistently oriented where the corner values agree; may
+    # split 4+-vertex polygons and ambiguous faces differently from the
+    # reference's table).  Mirrors cubvh/api.py:173-187.
+    coords = coords.int().contiguous()
+    corners = corners.float().contiguous()
+    if not coords.is_cuda: coords = coords.cuda()
+    if not corners.is_cuda: corners = corners.to(coords.device)
+    if coords.dim() != 2 or coords.shape[1] != 3 or corners.dim() != 2 or corners.shape[1] != 8 \
+            or coords.shape[0] != corners.shape[0]:
+        raise RuntimeError(f"sparse_marching_cubes expects coords [N, 3] and corners [N, 8], got "
+                           f"{tuple(coords.shape)} and {tuple(corners.shape)}")
+    N = coords.shape[0]
+    dev = coords.device
+    with torch.cuda.device(dev):
+        res = ctypes.c_void_p()
+        nv, nt = ctypes.c_int64(), ctypes.c_int64()
+        check(lib().cubvh_sparse_marching_cubes(_ptr(coords), _ptr(corners), N, float(iso),
+                                                1 if ensure_consistency else 0, _stream_ptr(dev),
+                                                ctypes.byref(res), ctypes.byref(nv), ctypes.byref(nt)),
+              "sparse_marching_cubes")
+        try:
+            verts = torch.empty(nv.value, 3, dtype=torch.float32, device=dev)
+            tris = torch.empty(nt.value, 3, dtype=torch.int32, device=dev)
+            check(lib().cubvh_sparse_mc_fetch(res, _ptr(verts), _ptr(tris), _stream_ptr(dev)), "sparse_marching_cubes")
+        finally:
+            lib().cubvh_sparse_mc_free(res)
+    return verts, tris
 
 
 def udf_to_sdf(udf, eps: float = None, check_bounds: bool = False):

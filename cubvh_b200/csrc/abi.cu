@@ -670,6 +670,64 @@ int cubvh_signed_distance_host(cubvh_bvh* h, const float* points, int64_t n, uin
     CUBVH_GUARD_END
 }
 
+// ---------------------------------------------------- sparse marching cubes
+struct cubvh_smc {
+    SparseMCResult r;
+    int device = -1;
+};
+
+int cubvh_sparse_marching_cubes(const int32_t* coords, const float* corners, int64_t n, float iso,
+                                int ensure_consistency, void* stream, cubvh_smc** out, int64_t* n_verts,
+                                int64_t* n_tris) {
+    CUBVH_GUARD_BEGIN
+    if (!out || !n_verts || !n_tris) return fail(CUBVH_ERR_INVALID, "out/n_verts/n_tris is null");
+    *out = nullptr; *n_verts = 0; *n_tris = 0;
+    if (n < 0) return fail(CUBVH_ERR_INVALID, "negative voxel count");
+    if (n > 0 && (!coords || !corners)) return fail(CUBVH_ERR_INVALID, "coords/corners is null");
+    auto* m = new cubvh_smc();
+    cudaGetDevice(&m->device);
+    std::string err;
+    const int rc = sparse_mc_run(coords, corners, n, iso, ensure_consistency != 0, (cudaStream_t)stream, m->r, err);
+    if (rc != 0) {
+        cubvh_sparse_mc_free(m);
+        return fail(rc == 1 ? CUBVH_ERR_INVALID : CUBVH_ERR_CUDA, err);
+    }
+    *out = m;
+    *n_verts = m->r.n_verts;
+    *n_tris = m->r.n_tris;
+    return CUBVH_OK;
+    CUBVH_GUARD_END
+}
+
+int cubvh_sparse_mc_fetch(cubvh_smc* m, float* verts, int32_t* tris, void* stream) {
+    CUBVH_GUARD_BEGIN
+    if (!m) return fail(CUBVH_ERR_INVALID, "result is null");
+    if ((m->r.n_verts && !verts) || (m->r.n_tris && !tris)) return fail(CUBVH_ERR_INVALID, "verts/tris is null");
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaSuccess;
+    if (m->r.n_verts)
+        e = cudaMemcpyAsync(verts, m->r.verts, sizeof(float) * 3 * m->r.n_verts, cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess && m->r.n_tris)
+        e = cudaMemcpyAsync(tris, m->r.tris, sizeof(int32_t) * 3 * m->r.n_tris, cudaMemcpyDeviceToDevice, s);
+    if (e != cudaSuccess) return cuda_fail(e, "sparse marching cubes fetch");
+    return CUBVH_OK;
+    CUBVH_GUARD_END
+}
+
+int cubvh_sparse_mc_free(cubvh_smc* m) {
+    if (!m) return CUBVH_OK;
+    int cur = 0;
+    const bool have = cudaGetDevice(&cur) == cudaSuccess;
+    if (m->device >= 0 && cudaSetDevice(m->device) == cudaSuccess) {
+        cudaDeviceSynchronize();  // a fetch may still be reading the buffers
+        if (m->r.verts) cudaFree(m->r.verts);
+        if (m->r.tris) cudaFree(m->r.tris);
+    }
+    if (have) cudaSetDevice(cur);
+    delete m;
+    return CUBVH_OK;
+}
+
 static int check_grid_dims(int B, int H, int W, int D) {
     if (B < 0 || H < 0 || W < 0 || D < 0) return fail(CUBVH_ERR_INVALID, "negative grid dimension");
     const int64_t ntot = (int64_t)B * H * W * D;

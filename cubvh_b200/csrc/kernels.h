@@ -99,4 +99,16 @@ size_t floodfill_status_offset(int B, int H, int W, int D);
 int floodfill_noalloc(const uint8_t* grid, int B, int H, int W, int D, int32_t* labels, cudaStream_t stream,
                       std::string& err);
 
+// Sparse marching cubes (sparse_mc.cu): device coords int32 [n, 3] and
+// corners float32 [n, 8]; the merged vertices float32 [n_verts, 3] and
+// triangles int32 [n_tris, 3] are cudaMalloc'd into `out` (the caller frees
+// them).  Returns 0, 1 (bad input, err set) or 2 (CUDA error, err set).
+struct SparseMCResult {
+    float* verts = nullptr;
+    int32_t* tris = nullptr;
+    int64_t n_verts = 0, n_tris = 0;
+};
+int sparse_mc_run(const int32_t* coords, const float* corners, int64_t n, float iso, bool ensure_consistency,
+                  cudaStream_t stream, SparseMCResult& out, std::string& err);
+
 }  // namespace cubvh

@@ -143,6 +143,28 @@ int cubvh_ray_trace_host(cubvh_bvh* bvh, const float* rays_o, const float* rays_
 int cubvh_signed_distance_host(cubvh_bvh* bvh, const float* points, int64_t n, uint32_t mode, float* distances,
                                int64_t* face_id, float* uvw, void* stream);
 
+/* Sparse marching cubes.  coords int32 [n, 3] voxel coordinates and
+ * corners float32 [n, 8] corner values (corner order (0,0,0), (1,0,0),
+ * (1,1,0), (0,1,0), (0,0,1), (1,0,1), (1,1,1), (0,1,1) from the voxel's
+ * coordinate), both device memory; iso the level; ensure_consistency != 0
+ * first replaces every corner value by its mean over the voxels sharing
+ * the corner.  Runs on `stream` and waits for it (the output sizes depend on
+ * the data); *out receives a result holding *n_verts vertices (float32
+ * [n_verts, 3], voxel units) and *n_tris triangles (int32 [n_tris, 3]);
+ * cubvh_sparse_mc_fetch copies them into device arrays of those sizes,
+ * cubvh_sparse_mc_free releases the result.  The vertex array equals the
+ * reference's (one vertex per cut voxel edge, merged across voxels, sorted
+ * by edge); the triangulation is this library's own (see sparse_mc.cu): a
+ * closed, consistently oriented surface where the corner values agree.
+ * Replaces sparse_marching_cubes (src/api_gpu.cu:154-215,
+ * include/gpu/spcumc.cuh `_sparse_marching_cubes`). */
+typedef struct cubvh_smc cubvh_smc;
+int cubvh_sparse_marching_cubes(const int32_t* coords, const float* corners, int64_t n, float iso,
+                                int ensure_consistency, void* stream, cubvh_smc** out, int64_t* n_verts,
+                                int64_t* n_tris);
+int cubvh_sparse_mc_fetch(cubvh_smc* result, float* verts, int32_t* tris, void* stream);
+int cubvh_sparse_mc_free(cubvh_smc* result);
+
 /* Differentiable queries (no counterpart in the reference, whose cuBVH
  * detaches the vertices: cubvh/api.py:16-17).
  *

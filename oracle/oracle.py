@@ -191,6 +191,101 @@ def ref_floodfill(grid):
     return out[0] if squeeze else out
 
 
+# ------------------------------------------------------ sparse marching cubes
+_SMC_CORNER_OFF = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0],
+                            [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]], np.int64)
+_SMC_EDGE_CORNERS = np.array([[0, 1], [1, 2], [2, 3], [3, 0], [4, 5], [5, 6],
+                              [6, 7], [7, 4], [0, 4], [1, 5], [2, 6], [3, 7]], np.int64)
+
+
+def sparse_mc_vertices(coords, corners, iso, return_ids=False):
+    """The reference's sparse-marching-cubes vertex array
+    (include/gpu/spcumc.cuh generateVertices and the sort / unique that
+    follows): for every voxel (in order) and every edge (in edge order) with
+    one corner below iso, t = clamp((iso - va) / (vb - va), 0, 1) (0.5 when
+    |vb - va| < 1e-30) in float32 and the point pA + t (pB - pA); vertices
+    with the same edge key (lower corner, axis) merged keeping the first,
+    sorted by key (x, y, z, axis).  The corner offsets are 0 or 1, so t (pB -
+    pA) is exact and one float64 sum rounded to float32 equals the device's
+    fused multiply-add.  Returns float32 [M, 3]; with return_ids also the
+    (voxel, edge, merged vertex id) of every cut voxel edge."""
+    coords = np.asarray(coords, np.int64)
+    v = np.asarray(corners, np.float32)
+    iso = np.float32(iso)
+    inside = v < iso
+    a, b = _SMC_EDGE_CORNERS[:, 0], _SMC_EDGE_CORNERS[:, 1]
+    cut = inside[:, a] != inside[:, b]                      # [N, 12]
+    vi, ei = np.nonzero(cut)                                # voxel-major, edges ascending
+    if len(vi) == 0:
+        z = np.zeros((0, 3), np.float32)
+        return (z, vi, ei, vi) if return_ids else z
+    ca, cb = a[ei], b[ei]
+    va, vb = v[vi, ca], v[vi, cb]
+    den = (vb - va).astype(np.float32)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        t = ((iso - va).astype(np.float32) / den).astype(np.float32)
+    t = np.minimum(np.maximum(t, np.float32(0)), np.float32(1))
+    t = np.where(np.abs(den) < np.float32(1e-30), np.float32(0.5), t).astype(np.float32)
+    pa = coords[vi] + _SMC_CORNER_OFF[ca]
+    pb = coords[vi] + _SMC_CORNER_OFF[cb]
+    pos = (pa.astype(np.float64) + t.astype(np.float64)[:, None] * (pb - pa).astype(np.float64)).astype(np.float32)
+    lo = np.minimum(pa, pb)
+    axis = np.where(pa[:, 0] != pb[:, 0], 0, np.where(pa[:, 1] != pb[:, 1], 1, 2))
+    order = np.lexsort((np.arange(len(vi)), axis, lo[:, 2], lo[:, 1], lo[:, 0]))
+    keys = np.stack([lo[order, 0], lo[order, 1], lo[order, 2], axis[order]], 1)
+    head = np.ones(len(order), bool)
+    head[1:] = np.any(keys[1:] != keys[:-1], axis=1)
+    if not return_ids:
+        return pos[order[head]]
+    ids = np.empty(len(order), np.int64)
+    ids[order] = np.cumsum(head) - 1
+    return pos[order[head]], vi, ei, ids
+
+
+_REF_SMC_PATH = os.path.join(_HERE, "_ref", "libref_sparse_mc.so")
+_ref_smc = None
+
+
+def ref_sparse_mc_available() -> bool:
+    """True when the reference's own CUDA sparse marching cubes has been
+    compiled into oracle/_ref (oracle/Makefile target `ref`)."""
+    return os.path.exists(_REF_SMC_PATH)
+
+
+def ref_sparse_mc(coords, corners, iso, ensure_consistency=False):
+    """The reference's own CUDA sparse marching cubes
+    (include/gpu/spcumc.cuh `_sparse_marching_cubes`) on host arrays:
+    -> vertices float32 [M, 3], triangles int32 [T, 3].  Needs a GPU."""
+    global _ref_smc
+    if _ref_smc is None:
+        if not ref_sparse_mc_available():
+            raise FileNotFoundError(_REF_SMC_PATH + " not built (make -C oracle ref)")
+        _ref_smc = ctypes.CDLL(_REF_SMC_PATH)
+        _ref_smc.ref_sparse_mc.restype = ctypes.c_int
+        _ref_smc.ref_sparse_mc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_float,
+                                           ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+                                           ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_void_p),
+                                           ctypes.POINTER(ctypes.c_int)]
+        _ref_smc.ref_sparse_mc_free.argtypes = [ctypes.c_void_p]
+    c = np.ascontiguousarray(coords, np.int32)
+    v = np.ascontiguousarray(corners, np.float32)
+    pv, pt = ctypes.c_void_p(), ctypes.c_void_p()
+    nv, nt = ctypes.c_int(), ctypes.c_int()
+    rc = _ref_smc.ref_sparse_mc(_p(c), _p(v), len(c), float(iso), 1 if ensure_consistency else 0,
+                                ctypes.byref(pv), ctypes.byref(nv), ctypes.byref(pt), ctypes.byref(nt))
+    try:
+        if rc != 0:
+            raise RuntimeError("reference sparse marching cubes failed (code %d)" % rc)
+        verts = np.ctypeslib.as_array(ctypes.cast(pv, ctypes.POINTER(ctypes.c_float)), (max(nv.value, 1) * 3,))
+        tris = np.ctypeslib.as_array(ctypes.cast(pt, ctypes.POINTER(ctypes.c_int32)), (max(nt.value, 1) * 3,))
+        return (verts[:3 * nv.value].reshape(-1, 3).copy(), tris[:3 * nt.value].reshape(-1, 3).copy())
+    finally:
+        if pv.value:
+            _ref_smc.ref_sparse_mc_free(pv)
+        if pt.value:
+            _ref_smc.ref_sparse_mc_free(pt)
+
+
 def udf_to_sdf(udf, eps):
     """The reference's occupancy -> SDF recipe (test/benchmark_watertight.py:
     98-143, readme.md:95-102) on float32 numpy grids [B,H,W,D] or [H,W,D]:

@@ -1,0 +1,143 @@
+"""Sparse marching cubes against the reference's own outputs.
+
+tests/golden/ref_sparse_mc.npz holds the vertex and triangle arrays that the
+reference's CUDA sparse marching cubes (include/gpu/spcumc.cuh, built from the
+reference tree into oracle/_ref) returned for three voxel sets
+(make_ref_sparse_mc.py beside it).  The vertex arrays must be equal bit for
+bit (the oracle's restatement on the CPU, the CUDA kernels on the GPU).  The
+triangulation is this library's own: a cube with one corner on its own side
+gives the reference's triangle; otherwise the tests check what holds for any
+correct triangulation: closed and consistently oriented where the corner
+values agree, no edge in more than two triangles, the same enclosed volume."""
+
+import os
+import sys
+
+import numpy as np
+import pytest
+import torch
+
+import cubvh_b200 as cubvh
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+import make_ref_sparse_mc as M  # noqa: E402
+
+R = np.load(os.path.join(HERE, "golden", "ref_sparse_mc.npz"))
+CASES = M.cases()
+
+
+def _edges(t):
+    e = np.concatenate([t[:, [0, 1]], t[:, [1, 2]], t[:, [2, 0]]])
+    _, cnt = np.unique(np.sort(e, 1), axis=0, return_counts=True)
+    _, dcnt = np.unique(e, axis=0, return_counts=True)
+    return e, cnt, dcnt
+
+
+def _volume(v, t):
+    a, b, c = (v[t[:, k]].astype(np.float64) for k in range(3))
+    return np.einsum("ij,ij->i", a, np.cross(b, c)).sum() / 6
+
+
+def _rot(t):
+    k = np.argmin(t, 1)
+    r = np.arange(len(t))
+    return np.stack([t[r, k], t[r, (k + 1) % 3], t[r, (k + 2) % 3]], 1)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_oracle_vertices_match_reference(oracle, name):
+    coords, corners, iso = CASES[name]
+    assert np.array_equal(oracle.sparse_mc_vertices(coords, corners, iso), R[name + "_verts"])
+
+
+def _run(name, dev, ensure=False):
+    coords, corners, iso = CASES[name]
+    v, t = cubvh.sparse_marching_cubes(torch.from_numpy(coords).to(dev), torch.from_numpy(corners).to(dev), iso,
+                                       ensure_consistency=ensure)
+    assert v.dtype == torch.float32 and t.dtype == torch.int32 and v.is_cuda and t.is_cuda
+    return v.cpu().numpy(), t.cpu().numpy()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_vertices_match_reference(dev, name):
+    v, t = _run(name, dev)
+    assert np.array_equal(v, R[name + "_verts"])
+    assert t.min() >= 0 and t.max() < len(v)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_single_triangle_cubes_match_reference(oracle, dev, name):
+    """A cube with exactly three cut edges (one corner on its own side) has a
+    single triangle: the reference's, with the same orientation."""
+    coords, corners, iso = CASES[name]
+    _, vi, ei, ids = oracle.sparse_mc_vertices(coords, corners, iso, return_ids=True)
+    ncut = np.bincount(vi, minlength=len(coords))
+    single = np.nonzero(ncut == 3)[0]
+    assert len(single) > 50
+    want = {tuple(sorted(ids[vi == s])) for s in single}
+    _, t = _run(name, dev)
+    ours = {tuple(sorted(x)): tuple(r) for x, r in zip(t, _rot(t))}
+    ref = {tuple(sorted(x)): tuple(r) for x, r in zip(R[name + "_tris"], _rot(R[name + "_tris"]))}
+    for key in want:
+        assert key in ours and key in ref and ours[key] == ref[key]
+
+
+@pytest.mark.gpu
+def test_sphere_closed_oriented_same_volume(dev):
+    v, t = _run("sphere", dev)
+    _, cnt, dcnt = _edges(t)
+    assert (cnt == 2).all() and (dcnt == 1).all()        # closed, each edge once each way
+    assert len(t) == len(R["sphere_tris"])
+    vol, ref_vol = _volume(v, t), _volume(R["sphere_verts"], R["sphere_tris"])
+    assert vol > 0 and abs(vol - ref_vol) < 1e-3 * ref_vol   # normals from inside to outside
+
+
+@pytest.mark.gpu
+def test_lattice_manifold(dev):
+    """Random values on a full 12^3 block (many ambiguous faces): every edge
+    inside the block is in exactly two triangles, once in each direction;
+    open edges lie on the block's outer faces only."""
+    v, t = _run("lattice", dev)
+    e, cnt, dcnt = _edges(t)
+    assert (cnt <= 2).all() and (dcnt == 1).all()
+    und, c2 = np.unique(np.sort(e, 1), axis=0, return_counts=True)
+    open_v = v[und[c2 == 1].reshape(-1)]
+    assert np.all(np.any((open_v == 0) | (open_v == 12), axis=1))
+
+
+@pytest.mark.gpu
+def test_ensure_consistency(oracle, dev):
+    """Averaged shared corners: the vertices the reference gives, up to the
+    order of the sums (1 ulp of the corner values)."""
+    if not oracle.ref_sparse_mc_available():
+        pytest.skip("oracle/_ref/libref_sparse_mc.so not built")
+    coords, corners, iso = CASES["random"]
+    rv, _ = oracle.ref_sparse_mc(coords, corners, iso, True)
+    v, t = _run("random", dev, ensure=True)
+    assert v.shape == rv.shape and np.abs(v - rv).max() < 4e-6
+
+
+@pytest.mark.gpu
+def test_live_reference_larger(oracle, dev):
+    if not oracle.ref_sparse_mc_available():
+        pytest.skip("oracle/_ref/libref_sparse_mc.so not built")
+    for coords, corners, iso in (M.sphere_band(n=64, c=(31.7, 32.2, 30.9), r=25.3) + (0.0,),
+                                 M.random_subset(seed=9, n=40, frac=0.3) + (-0.2,)):
+        rv, rt = oracle.ref_sparse_mc(coords, corners, iso)
+        v, t = cubvh.sparse_marching_cubes(torch.from_numpy(coords).to(dev), torch.from_numpy(corners).to(dev), iso)
+        assert np.array_equal(v.cpu().numpy(), rv)
+
+
+@pytest.mark.gpu
+def test_empty_and_errors(dev):
+    v, t = cubvh.sparse_marching_cubes(torch.zeros(0, 3, dtype=torch.int32, device=dev),
+                                       torch.zeros(0, 8, device=dev), 0.0)
+    assert v.shape == (0, 3) and t.shape == (0, 3)
+    v, t = cubvh.sparse_marching_cubes(torch.zeros(5, 3, dtype=torch.int32, device=dev),
+                                       torch.ones(5, 8, device=dev), 0.0)
+    assert v.shape == (0, 3) and t.shape == (0, 3)
+    with pytest.raises(RuntimeError):
+        cubvh.sparse_marching_cubes(torch.zeros(5, 3, dtype=torch.int32, device=dev), torch.ones(5, 7, device=dev), 0.0)
