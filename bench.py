@@ -2,7 +2,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload rays_displaced|udf_icosphere|dense_tori|raystab_displaced|
-                                grad_displaced|batch_256]
+                                grad_displaced|batch_256|sparse_mc_band]
 
 Default workload (``rays_displaced``): displaced icosphere level 6 (81,920
 faces); one step = ray_trace of 33,554,432 camera rays (8 poses x 2048^2,
@@ -819,6 +819,95 @@ def run_ours_fwd_bwd(args):
         torch.distributed.destroy_process_group()
 
 
+# ------------------------------------------------ sparse marching cubes arm
+def smc_band(n=192, r=80.2):
+    """The voxels of a band around a sphere (radius r in voxel units, centre
+    near n/2) with the sphere's signed distance at their corners: int32
+    coords [N, 3], float32 corners [N, 8] in the corner order of the API."""
+    off = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0], [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]])
+    c = np.array([n / 2 + 0.3, n / 2 - 0.2, n / 2 + 0.1])
+    g = np.stack(np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij"), -1).reshape(-1, 3)
+    keep = np.abs(np.linalg.norm(g + 0.5 - c, axis=1) - r) < 2.5
+    g = g[keep]
+    f = (np.linalg.norm(g[:, None, :] + off[None] - c, axis=-1) - r).astype(np.float32)
+    return g.astype(np.int32), f
+
+
+SMC_METRIC = "voxels/s (sparse marching cubes), 1 B200"
+SMC_DESC = "voxels of a band around a sphere of radius 80.2 on a 192^3 grid, its signed distance at the corners, iso 0"
+
+
+def run_smc(args):
+    """Sparse marching cubes on the sphere band: `value` times the public call
+    on device tensors (its host round trips for the output sizes included);
+    `e2e` adds the upload of the voxels and the download of the mesh."""
+    import torch
+    import cubvh_b200 as cubvh
+    rank, world, local = _rank_info()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    coords, corners = smc_band()
+    n = len(coords)
+    ct, ft = torch.from_numpy(coords).to(dev), torch.from_numpy(corners).to(dev)
+    for _ in range(args.warmup):
+        v, t = cubvh.sparse_marching_cubes(ct, ft, 0.0)
+    torch.cuda.synchronize()
+    n_launch0 = _launches()
+    with ClockSampler(local) as clk:
+        w0 = time.perf_counter()
+        for _ in range(args.steps):
+            v, t = cubvh.sparse_marching_cubes(ct, ft, 0.0)
+        torch.cuda.synchronize()
+        ms = (time.perf_counter() - w0) * 1e3 / args.steps
+    gpu_launches = _launches() - n_launch0
+    ch, fh = torch.from_numpy(coords).pin_memory(), torch.from_numpy(corners).pin_memory()
+    w0 = time.perf_counter()
+    for _ in range(args.steps):
+        v, t = cubvh.sparse_marching_cubes(ch, fh, 0.0)
+        vh, th = v.cpu(), t.cpu()
+    e2e_ms = (time.perf_counter() - w0) * 1e3 / args.steps
+    line = {"metric": SMC_METRIC, "value": n / (ms / 1e3), "unit": "voxels/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (analytic sphere distance)",
+            "config": {"workload": "sparse_mc_band", "description": SMC_DESC, "voxels": n,
+                       "vertices": int(vh.shape[0]), "triangles": int(th.shape[0])},
+            "e2e": {"value": n / (e2e_ms / 1e3), "unit": "voxels/s", "h2d_bytes_per_step": n * (12 + 32),
+                    "d2h_bytes_per_step": int(vh.numel() * 4 + th.numel() * 4)},
+            "gpu_launches": gpu_launches, "clocks": clk.summary()}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_reference_smc(args):
+    """The reference's own CUDA sparse marching cubes (oracle/_ref, compiled
+    from its include/gpu/spcumc.cuh) on the same voxels, host arrays in and
+    out (its device allocations and copies included)."""
+    rank, _, _ = _rank_info()
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    coords, corners = smc_band()
+    if not O.ref_sparse_mc_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_sparse_mc.so not built"}))
+        return
+    for _ in range(args.warmup):
+        O.ref_sparse_mc(coords, corners, 0.0)
+    w0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.ref_sparse_mc(coords, corners, 0.0)
+    ms = (time.perf_counter() - w0) * 1e3 / args.steps
+    val = len(coords) / (ms / 1e3)
+    print(json.dumps({"impl": "reference", "metric": SMC_METRIC, "value": val, "unit": "voxels/s", "n_gpus": 1,
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                      "data": "synthetic (analytic sphere distance)",
+                      "config": {"workload": "sparse_mc_band", "description": SMC_DESC, "voxels": len(coords)},
+                      "reference_cuda": {"sparse_mc": {"e2e_ms": ms, "host_buffers": "numpy arrays"}},
+                      "cpu_baseline": None,
+                      "e2e": {"value": val, "unit": "voxels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+          flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -827,7 +916,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="rays_displaced",
                     choices=["rays_displaced", "udf_icosphere", "dense_tori", "raystab_displaced",
-                             "grad_displaced", "batch_256"])
+                             "grad_displaced", "batch_256", "sparse_mc_band"])
     ap.add_argument("--adam-steps", type=int, default=200, help="grad_displaced: sphere-fitting steps")
     ap.add_argument("--meshes", type=int, default=256, help="batch_256: number of meshes")
     ap.add_argument("--res", type=int, default=2048, help="camera resolution (rays_displaced)")
@@ -836,7 +925,9 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.workload == "sparse_mc_band":
+        run_reference_smc(args) if args.impl == "reference" else run_smc(args)
+    elif args.impl == "reference":
         run_reference(args)
     elif args.workload in ("grad_displaced", "batch_256"):
         run_ours_fwd_bwd(args)
