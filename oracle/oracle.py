@@ -4,9 +4,10 @@ TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke(), the
 CPU-baseline leg and the reference arm of bench.py, never by the cubvh_b200
 package.  See the header
 of oracle.cpp for what is restated from which reference file, and for the
-pinning status (floodfill: pinned to the reference's own CUDA floodfill,
-compiled into oracle/_ref; distance, ray and sign queries: unpinned against
-the reference's outputs, whose BVH code cannot be built in this image).
+pinning status (floodfill and the sparse-marching-cubes vertices: pinned to
+the reference's own CUDA code, compiled into oracle/_ref; distance, ray and
+sign queries: unpinned against the reference's outputs, whose BVH code
+cannot be built in this image).
 """
 
 from __future__ import annotations
