@@ -141,3 +141,45 @@ def test_empty_and_errors(dev):
     assert v.shape == (0, 3) and t.shape == (0, 3)
     with pytest.raises(RuntimeError):
         cubvh.sparse_marching_cubes(torch.zeros(5, 3, dtype=torch.int32, device=dev), torch.ones(5, 7, device=dev), 0.0)
+
+
+def _model_tris(oracle, coords, corners, iso):
+    import smc_model
+    _, vi, ei, ids = oracle.sparse_mc_vertices(coords, corners, iso, return_ids=True)
+    return smc_model.mesh_triangles(coords, corners, iso, vi, ei, ids)
+
+
+@pytest.mark.parametrize("seed", range(25))
+def test_model_closed_on_random_lattices(oracle, seed):
+    """The triangulation rules (tests/smc_model.py, the kernels' rules) on a
+    random field over a 6^3 block: every edge inside the block in exactly two
+    triangles, once in each direction."""
+    coords, corners = M.lattice_field(seed=100 + seed, n=6)
+    v = oracle.sparse_mc_vertices(coords, corners, 0.0)
+    t = _model_tris(oracle, coords, corners, 0.0)
+    e, cnt, dcnt = _edges(t)
+    assert (cnt <= 2).all() and (dcnt == 1).all()
+    und, c2 = np.unique(np.sort(e, 1), axis=0, return_counts=True)
+    open_v = v[und[c2 == 1].reshape(-1)]
+    assert np.all(np.any((open_v == 0) | (open_v == 6), axis=1))
+
+
+def test_model_single_triangles_match_reference(oracle):
+    for name in sorted(CASES):
+        coords, corners, iso = CASES[name]
+        t = _model_tris(oracle, coords, corners, iso)
+        ref = set(map(tuple, _rot(R[name + "_tris"])))
+        _, vi, ei, ids = oracle.sparse_mc_vertices(coords, corners, iso, return_ids=True)
+        ncut = np.bincount(vi, minlength=len(coords))
+        single = set(np.nonzero(ncut == 3)[0])
+        own = {tuple(sorted(ids[vi == s])) for s in single}
+        mine = [tuple(r) for x, r in zip(t, _rot(t)) if tuple(sorted(x)) in own]
+        assert len(mine) == len(own) and all(m in ref for m in mine)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_kernels_match_model(oracle, dev, name):
+    coords, corners, iso = CASES[name]
+    _, t = _run(name, dev)
+    assert np.array_equal(t, _model_tris(oracle, coords, corners, iso))
