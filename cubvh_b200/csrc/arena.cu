@@ -72,16 +72,23 @@ int arena_device(cubvh_arena* a) {
     }
     const size_t nb = a->nodes.size() * sizeof(CNode), tb = a->tris.size() * sizeof(CTri);
     const size_t fb = a->face_off.size() * sizeof(int64_t), sb = a->gslot.size() * sizeof(int32_t);
+    // a failed upload leaves the arena host-only (device stays -1, pointers
+    // null), so a later call retries from scratch instead of leaking
+    auto drop = [&](cudaError_t err, const char* what) {
+        for (void** q : {(void**)&a->d_nodes, (void**)&a->d_tris, (void**)&a->d_face_off, (void**)&a->d_gslot})
+            if (*q) { cudaFree(*q); *q = nullptr; }
+        return cuda_err(err, what);
+    };
     if ((e = cudaMalloc(&a->d_nodes, nb)) != cudaSuccess ||
         (e = cudaMalloc(&a->d_tris, tb)) != cudaSuccess ||
         (e = cudaMalloc(&a->d_face_off, fb)) != cudaSuccess ||
         (e = cudaMalloc(&a->d_gslot, sb)) != cudaSuccess)
-        return cuda_err(e, "cudaMalloc(arena)");
+        return drop(e, "cudaMalloc(arena)");
     if ((e = cudaMemcpy(a->d_nodes, a->nodes.data(), nb, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(a->d_tris, a->tris.data(), tb, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(a->d_face_off, a->face_off.data(), fb, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(a->d_gslot, a->gslot.data(), sb, cudaMemcpyHostToDevice)) != cudaSuccess)
-        return cuda_err(e, "arena upload");
+        return drop(e, "arena upload");
     a->device = dev;
     // the raystab sign pass reads the stab-direction tables: set them on this
     // device even when no single-BVH query has run on it yet

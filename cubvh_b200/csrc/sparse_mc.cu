@@ -23,14 +23,21 @@
 // face when the saddle value is below iso.  Both cubes sharing a face take the
 // same decision, so the surface is closed wherever the corner values agree.
 // Every cut edge is entered on one of its faces and left on the other, so the
-// segments form closed loops; each loop, started at its lowest edge, is cut
-// into a triangle fan.  Triangles face from the inside (values below iso) to
+// segments form closed loops.  Each loop, started at its lowest edge, is cut
+// into a triangle fan from the first vertex none of whose diagonals joins two
+// edges of one face that the loop crosses twice (such a diagonal would lie in
+// that face and be shared with the neighbouring cube's triangles); when no
+// vertex qualifies, ears whose closing diagonal avoids such faces are clipped
+// one by one.  Triangles face from the inside (values below iso) to
 // the outside.  A cube with one corner inside gives the same triangle as the
 // reference; cubes whose polygons have four or more vertices, or that have
 // ambiguous faces, may be triangulated differently.
+#include <cstddef>
 #include <cstdint>
 #include <cub/cub.cuh>
 #include <cuda_runtime.h>
+#include <string>
+#include <vector>
 
 #include "launches.h"
 #include "kernels.h"
@@ -366,10 +373,34 @@ int bits_for(uint64_t v) {  // bits to hold values below v
     return b;
 }
 
+// Stream-ordered temporaries of one call: every buffer taken from `get` is
+// returned with cudaFreeAsync on the same stream, early through `put` or at
+// scope exit, so an error return in the middle of the pipeline leaks nothing.
+struct AsyncTemps {
+    cudaStream_t s;
+    std::vector<void*> p;
+    explicit AsyncTemps(cudaStream_t st) : s(st) {}
+    AsyncTemps(const AsyncTemps&) = delete;
+    AsyncTemps& operator=(const AsyncTemps&) = delete;
+    ~AsyncTemps() { for (void* q : p) cudaFreeAsync(q, s); }
+    template <class T>
+    cudaError_t get(T** out, size_t count) {
+        void* q = nullptr;
+        const cudaError_t e = cudaMallocAsync(&q, count * sizeof(T) > 0 ? count * sizeof(T) : 16, s);
+        if (e == cudaSuccess) { p.push_back(q); *out = static_cast<T*>(q); }
+        return e;
+    }
+    void put(void* q) {
+        for (size_t i = 0; i < p.size(); ++i)
+            if (p[i] == q) { cudaFreeAsync(q, s); p.erase(p.begin() + (std::ptrdiff_t)i); return; }
+    }
+};
+
 }  // namespace
 
 // All temporaries come from cudaMallocAsync on `stream`; the results stay in
-// `out` (device, owned by the caller through cubvh_sparse_mc_*).
+// `out` (device, owned by the caller through cubvh_sparse_mc_*, which frees
+// them on an error return as well).
 int sparse_mc_run(const int32_t* coords, const float* corners, int64_t n, float iso, bool ensure_consistency,
                   cudaStream_t s, SparseMCResult& out, std::string& err) {
     out = SparseMCResult{};
@@ -377,16 +408,17 @@ int sparse_mc_run(const int32_t* coords, const float* corners, int64_t n, float 
     if (n > (int64_t)INT32_MAX / 12) { err = "too many voxels (the vertex count must fit in int32)"; return 1; }
     cudaError_t e;
     auto fail = [&](cudaError_t x, const char* what) { err = std::string(what) + ": " + cudaGetErrorString(x); return 2; };
+    AsyncTemps tmp(s);
     // coordinate bounds -> key packing (host round trip)
     int32_t* d_b = nullptr;
-    if ((e = cudaMallocAsync(&d_b, 6 * sizeof(int32_t), s)) != cudaSuccess) return fail(e, "cudaMallocAsync");
+    if ((e = tmp.get(&d_b, 6)) != cudaSuccess) return fail(e, "cudaMallocAsync");
     k_smc_bounds_init<<<1, 32, 0, s>>>(d_b); count_launch();
     k_smc_bounds<<<grid_for(n), 256, 0, s>>>(n, coords, d_b); count_launch();
     int32_t b[6];
     if ((e = cudaMemcpyAsync(b, d_b, sizeof(b), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
         (e = cudaStreamSynchronize(s)) != cudaSuccess)
         return fail(e, "sparse marching cubes bounds");
-    cudaFreeAsync(d_b, s);
+    tmp.put(d_b);
     const uint64_t rx = (uint64_t)((int64_t)b[3] - b[0] + 2), ry = (uint64_t)((int64_t)b[4] - b[1] + 2),
                    rz = (uint64_t)((int64_t)b[5] - b[2] + 2);
     const int key_bits = bits_for(rx) + bits_for(ry) + bits_for(rz) + 2;
@@ -395,39 +427,34 @@ int sparse_mc_run(const int32_t* coords, const float* corners, int64_t n, float 
     const unsigned g = grid_for(n);
 
     const float* use = corners;
-    float* avg = nullptr;
-    void* cub_tmp = nullptr;
-    size_t cub_bytes = 0;
     if (ensure_consistency) {
         const int64_t m8 = 8 * n;
+        float* avg = nullptr;
         uint64_t *ck = nullptr, *ck2 = nullptr;
         int32_t *ci = nullptr, *ci2 = nullptr;
         const int cbits = bits_for(rx) + bits_for(ry) + bits_for(rz);
-        if ((e = cudaMallocAsync(&avg, sizeof(float) * m8, s)) != cudaSuccess ||
-            (e = cudaMallocAsync(&ck, sizeof(uint64_t) * m8, s)) != cudaSuccess ||
-            (e = cudaMallocAsync(&ck2, sizeof(uint64_t) * m8, s)) != cudaSuccess ||
-            (e = cudaMallocAsync(&ci, sizeof(int32_t) * m8, s)) != cudaSuccess ||
-            (e = cudaMallocAsync(&ci2, sizeof(int32_t) * m8, s)) != cudaSuccess)
+        if ((e = tmp.get(&avg, m8)) != cudaSuccess || (e = tmp.get(&ck, m8)) != cudaSuccess ||
+            (e = tmp.get(&ck2, m8)) != cudaSuccess || (e = tmp.get(&ci, m8)) != cudaSuccess ||
+            (e = tmp.get(&ci2, m8)) != cudaSuccess)
             return fail(e, "cudaMallocAsync");
         k_smc_corner_keys<<<grid_for(m8), 256, 0, s>>>(n, coords, kp, ck, ci); count_launch();
         size_t tb = 0;
+        char* cub_tmp = nullptr;
         cub::DeviceRadixSort::SortPairs(nullptr, tb, ck, ck2, ci, ci2, (int)m8, 0, cbits, s);
-        if ((e = cudaMallocAsync(&cub_tmp, tb, s)) != cudaSuccess) return fail(e, "cudaMallocAsync");
+        if ((e = tmp.get(&cub_tmp, tb)) != cudaSuccess) return fail(e, "cudaMallocAsync");
         if ((e = cub::DeviceRadixSort::SortPairs(cub_tmp, tb, ck, ck2, ci, ci2, (int)m8, 0, cbits, s)) != cudaSuccess)
             return fail(e, "corner sort");
         count_launch();
-        cudaFreeAsync(cub_tmp, s);
-        cub_tmp = nullptr;
+        tmp.put(cub_tmp);
         k_smc_corner_mean<<<grid_for(m8), 256, 0, s>>>(m8, ck2, ci2, corners, avg); count_launch();
-        cudaFreeAsync(ck, s); cudaFreeAsync(ck2, s); cudaFreeAsync(ci, s); cudaFreeAsync(ci2, s);
-        use = avg;
+        tmp.put(ck); tmp.put(ck2); tmp.put(ci); tmp.put(ci2);
+        use = avg;  // freed at scope exit, after the kernels that read it
     }
 
     uint32_t *nv = nullptr, *nt = nullptr, *bs = nullptr;
     const int64_t nb = scan::num_chunks(n) + 1;
-    if ((e = cudaMallocAsync(&nv, sizeof(uint32_t) * (n + 1), s)) != cudaSuccess ||
-        (e = cudaMallocAsync(&nt, sizeof(uint32_t) * (n + 1), s)) != cudaSuccess ||
-        (e = cudaMallocAsync(&bs, sizeof(uint32_t) * nb, s)) != cudaSuccess)
+    if ((e = tmp.get(&nv, n + 1)) != cudaSuccess || (e = tmp.get(&nt, n + 1)) != cudaSuccess ||
+        (e = tmp.get(&bs, nb)) != cudaSuccess)
         return fail(e, "cudaMallocAsync");
     k_smc_count<<<g, 256, 0, s>>>(n, use, iso, nv, nt); count_launch();
     scan::exclusive(nv, bs, n, s);   // nv[n] = total
@@ -444,25 +471,20 @@ int sparse_mc_run(const int32_t* coords, const float* corners, int64_t n, float 
     uint32_t *head = nullptr, *ids = nullptr, *bs2 = nullptr;
     if (m > 0) {
         const int64_t nb2 = scan::num_chunks(m) + 1;
-        if ((e = cudaMallocAsync(&pos, sizeof(float) * 3 * m, s)) != cudaSuccess ||
-            (e = cudaMallocAsync(&key, sizeof(uint64_t) * m, s)) != cudaSuccess ||
-            (e = cudaMallocAsync(&key2, sizeof(uint64_t) * m, s)) != cudaSuccess ||
-            (e = cudaMallocAsync(&ord, sizeof(int32_t) * m, s)) != cudaSuccess ||
-            (e = cudaMallocAsync(&ord2, sizeof(int32_t) * m, s)) != cudaSuccess ||
-            (e = cudaMallocAsync(&map, sizeof(int32_t) * m, s)) != cudaSuccess ||
-            (e = cudaMallocAsync(&head, sizeof(uint32_t) * (m + 1), s)) != cudaSuccess ||
-            (e = cudaMallocAsync(&ids, sizeof(uint32_t) * (m + 1), s)) != cudaSuccess ||
-            (e = cudaMallocAsync(&bs2, sizeof(uint32_t) * nb2, s)) != cudaSuccess ||
+        if ((e = tmp.get(&pos, 3 * m)) != cudaSuccess || (e = tmp.get(&key, m)) != cudaSuccess ||
+            (e = tmp.get(&key2, m)) != cudaSuccess || (e = tmp.get(&ord, m)) != cudaSuccess ||
+            (e = tmp.get(&ord2, m)) != cudaSuccess || (e = tmp.get(&map, m)) != cudaSuccess ||
+            (e = tmp.get(&head, m + 1)) != cudaSuccess || (e = tmp.get(&ids, m + 1)) != cudaSuccess ||
+            (e = tmp.get(&bs2, nb2)) != cudaSuccess ||
             (e = cudaMalloc(&out.tris, sizeof(int32_t) * 3 * (t > 0 ? t : 1))) != cudaSuccess)
             return fail(e, "sparse marching cubes buffers");
-    }
-    if (m > 0) {
         k_smc_emit<<<g, 256, 0, s>>>(n, coords, use, iso, nv, nt, kp, pos, key, out.tris); count_launch();
         // emission index as the value: the stable sort keeps each key's lowest first
         k_smc_iota<<<grid_for(m), 256, 0, s>>>(m, ord); count_launch();
         size_t tb = 0;
+        char* cub_tmp = nullptr;
         cub::DeviceRadixSort::SortPairs(nullptr, tb, key, key2, ord, ord2, (int)m, 0, key_bits, s);
-        if ((e = cudaMallocAsync(&cub_tmp, tb, s)) != cudaSuccess) return fail(e, "cudaMallocAsync");
+        if ((e = tmp.get(&cub_tmp, tb)) != cudaSuccess) return fail(e, "cudaMallocAsync");
         if ((e = cub::DeviceRadixSort::SortPairs(cub_tmp, tb, key, key2, ord, ord2, (int)m, 0, key_bits, s)) !=
             cudaSuccess)
             return fail(e, "edge key sort");
@@ -481,13 +503,7 @@ int sparse_mc_run(const int32_t* coords, const float* corners, int64_t n, float 
         if (t > 0) { k_smc_remap<<<grid_for(3 * t), 256, 0, s>>>(3 * t, map, out.tris); count_launch(); }
         out.n_verts = u;
         out.n_tris = t;
-        cudaFreeAsync(cub_tmp, s);
-        cudaFreeAsync(pos, s); cudaFreeAsync(key, s); cudaFreeAsync(key2, s); cudaFreeAsync(ord, s);
-        cudaFreeAsync(ord2, s); cudaFreeAsync(map, s); cudaFreeAsync(head, s); cudaFreeAsync(ids, s);
-        cudaFreeAsync(bs2, s);
     }
-    cudaFreeAsync(nv, s); cudaFreeAsync(nt, s); cudaFreeAsync(bs, s);
-    if (avg) cudaFreeAsync(avg, s);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "sparse marching cubes launch");
     return 0;
 }
