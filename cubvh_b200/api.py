@@ -377,7 +377,7 @@ def sparse_marching_cubes(coords, corners, iso, ensure_consistency=False):
     coords = coords.int().contiguous()
     corners = corners.float().contiguous()
     if not coords.is_cuda: coords = coords.cuda()
-    if not corners.is_cuda: corners = corners.to(coords.device)
+    corners = corners.to(coords.device)  # one device for both (a no-op when it already is)
     if coords.dim() != 2 or coords.shape[1] != 3 or corners.dim() != 2 or corners.shape[1] != 8 \
             or coords.shape[0] != corners.shape[0]:
         raise RuntimeError(f"sparse_marching_cubes expects coords [N, 3] and corners [N, 8], got "

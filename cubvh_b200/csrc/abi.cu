@@ -518,6 +518,10 @@ int host_pipe(DevCopy* d, cudaStream_t caller, HostPipe** out) {
         ev(&p.start);
         for (int k = 0; k < 2; ++k) { ev(&p.in[k]); ev(&p.comp[k]); ev(&p.out[k]); }
         if (e != cudaSuccess) {
+            for (cudaStream_t x : {p.cin, p.cout, p.comp_s[0], p.comp_s[1]})
+                if (x) cudaStreamDestroy(x);
+            for (cudaEvent_t x : {p.start, p.in[0], p.in[1], p.comp[0], p.comp[1], p.out[0], p.out[1]})
+                if (x) cudaEventDestroy(x);
             d->pipes.pop_back();
             return cuda_fail(e, "host-buffer query streams");
         }
@@ -674,6 +678,7 @@ int cubvh_signed_distance_host(cubvh_bvh* h, const float* points, int64_t n, uin
 struct cubvh_smc {
     SparseMCResult r;
     int device = -1;
+    cudaEvent_t done = nullptr;  // recorded on the building stream after its last kernel
 };
 
 int cubvh_sparse_marching_cubes(const int32_t* coords, const float* corners, int64_t n, float iso,
@@ -692,6 +697,13 @@ int cubvh_sparse_marching_cubes(const int32_t* coords, const float* corners, int
         cubvh_sparse_mc_free(m);
         return fail(rc == 1 ? CUBVH_ERR_INVALID : CUBVH_ERR_CUDA, err);
     }
+    // the merge and remap kernels may still run: a fetch on another stream waits for them
+    cudaError_t e = cudaEventCreateWithFlags(&m->done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(m->done, (cudaStream_t)stream);
+    if (e != cudaSuccess) {
+        cubvh_sparse_mc_free(m);
+        return cuda_fail(e, "sparse marching cubes event");
+    }
     *out = m;
     *n_verts = m->r.n_verts;
     *n_tris = m->r.n_tris;
@@ -704,8 +716,8 @@ int cubvh_sparse_mc_fetch(cubvh_smc* m, float* verts, int32_t* tris, void* strea
     if (!m) return fail(CUBVH_ERR_INVALID, "result is null");
     if ((m->r.n_verts && !verts) || (m->r.n_tris && !tris)) return fail(CUBVH_ERR_INVALID, "verts/tris is null");
     cudaStream_t s = (cudaStream_t)stream;
-    cudaError_t e = cudaSuccess;
-    if (m->r.n_verts)
+    cudaError_t e = m->done ? cudaStreamWaitEvent(s, m->done, 0) : cudaSuccess;
+    if (e == cudaSuccess && m->r.n_verts)
         e = cudaMemcpyAsync(verts, m->r.verts, sizeof(float) * 3 * m->r.n_verts, cudaMemcpyDeviceToDevice, s);
     if (e == cudaSuccess && m->r.n_tris)
         e = cudaMemcpyAsync(tris, m->r.tris, sizeof(int32_t) * 3 * m->r.n_tris, cudaMemcpyDeviceToDevice, s);
@@ -722,6 +734,7 @@ int cubvh_sparse_mc_free(cubvh_smc* m) {
         cudaDeviceSynchronize();  // a fetch may still be reading the buffers
         if (m->r.verts) cudaFree(m->r.verts);
         if (m->r.tris) cudaFree(m->r.tris);
+        if (m->done) cudaEventDestroy(m->done);
     }
     if (have) cudaSetDevice(cur);
     delete m;

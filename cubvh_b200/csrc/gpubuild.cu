@@ -242,7 +242,6 @@ struct TreeView {
     const int32_t* leaf_size;  // per mesh
     int32_t M;
     __device__ __forceinline__ int32_t mesh(int32_t r) const { return mesh_of_face(foff, M, lo_of(r)); }
-    __device__ __forceinline__ bool is_leaf(int32_t r) const { return count(r) <= leaf_size[mesh(r)]; }
     __device__ __forceinline__ int64_t lo_of(int32_t r) const { return r < n - 1 ? first[r] : r - (n - 1); }
     __device__ __forceinline__ int64_t hi_of(int32_t r) const { return r < n - 1 ? last[r] : r - (n - 1); }
     __device__ __forceinline__ int count(int32_t r) const { return (int)(hi_of(r) - lo_of(r) + 1); }

@@ -183,3 +183,32 @@ def test_kernels_match_model(oracle, dev, name):
     coords, corners, iso = CASES[name]
     _, t = _run(name, dev)
     assert np.array_equal(t, _model_tris(oracle, coords, corners, iso))
+
+
+@pytest.mark.gpu
+def test_fetch_on_another_stream(dev):
+    """C ABI: a result built on one stream and fetched on another equals the
+    one-stream result (the fetch waits for the building stream's kernels)."""
+    import ctypes
+    from cubvh_b200 import api
+    from cubvh_b200._lib import check, lib
+    coords, corners, iso = M.sphere_band(n=64, c=(31.7, 32.2, 30.9), r=25.3) + (0.0,)
+    c = torch.from_numpy(coords).to(dev)
+    v = torch.from_numpy(corners).to(dev)
+    want_v, want_t = cubvh.sparse_marching_cubes(c, v, iso)
+    build, fetch = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    torch.cuda.synchronize(dev)
+    res, nv, nt = ctypes.c_void_p(), ctypes.c_int64(), ctypes.c_int64()
+    check(lib().cubvh_sparse_marching_cubes(api._ptr(c), api._ptr(v), len(coords), float(iso), 0,
+                                            ctypes.c_void_p(build.cuda_stream), ctypes.byref(res),
+                                            ctypes.byref(nv), ctypes.byref(nt)), "sparse_marching_cubes")
+    try:
+        with torch.cuda.stream(fetch):
+            got_v = torch.empty(nv.value, 3, dtype=torch.float32, device=dev)
+            got_t = torch.empty(nt.value, 3, dtype=torch.int32, device=dev)
+        check(lib().cubvh_sparse_mc_fetch(res, api._ptr(got_v), api._ptr(got_t), ctypes.c_void_p(fetch.cuda_stream)),
+              "sparse_mc_fetch")
+        fetch.synchronize()
+    finally:
+        check(lib().cubvh_sparse_mc_free(res), "sparse_mc_free")
+    assert torch.equal(got_v, want_v) and torch.equal(got_t, want_t)
