@@ -678,7 +678,8 @@ int cubvh_signed_distance_host(cubvh_bvh* h, const float* points, int64_t n, uin
 struct cubvh_smc {
     SparseMCResult r;
     int device = -1;
-    cudaEvent_t done = nullptr;  // recorded on the building stream after its last kernel
+    cudaEvent_t done = nullptr;          // recorded on the building stream after its last kernel
+    std::vector<cudaEvent_t> fetched;    // recorded on each fetch's stream after its copies
 };
 
 int cubvh_sparse_marching_cubes(const int32_t* coords, const float* corners, int64_t n, float iso,
@@ -694,6 +695,7 @@ int cubvh_sparse_marching_cubes(const int32_t* coords, const float* corners, int
     std::string err;
     const int rc = sparse_mc_run(coords, corners, n, iso, ensure_consistency != 0, (cudaStream_t)stream, m->r, err);
     if (rc != 0) {
+        cudaStreamSynchronize((cudaStream_t)stream);  // kernels may still write the result buffers
         cubvh_sparse_mc_free(m);
         return fail(rc == 1 ? CUBVH_ERR_INVALID : CUBVH_ERR_CUDA, err);
     }
@@ -701,6 +703,7 @@ int cubvh_sparse_marching_cubes(const int32_t* coords, const float* corners, int
     cudaError_t e = cudaEventCreateWithFlags(&m->done, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventRecord(m->done, (cudaStream_t)stream);
     if (e != cudaSuccess) {
+        cudaStreamSynchronize((cudaStream_t)stream);
         cubvh_sparse_mc_free(m);
         return cuda_fail(e, "sparse marching cubes event");
     }
@@ -721,7 +724,16 @@ int cubvh_sparse_mc_fetch(cubvh_smc* m, float* verts, int32_t* tris, void* strea
         e = cudaMemcpyAsync(verts, m->r.verts, sizeof(float) * 3 * m->r.n_verts, cudaMemcpyDeviceToDevice, s);
     if (e == cudaSuccess && m->r.n_tris)
         e = cudaMemcpyAsync(tris, m->r.tris, sizeof(int32_t) * 3 * m->r.n_tris, cudaMemcpyDeviceToDevice, s);
-    if (e != cudaSuccess) return cuda_fail(e, "sparse marching cubes fetch");
+    cudaEvent_t ev = nullptr;
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) {
+        m->fetched.push_back(ev);  // owned by the result from here on
+        e = cudaEventRecord(ev, s);
+    }
+    if (e != cudaSuccess) {
+        cudaStreamSynchronize(s);  // the free must not overtake copies already queued
+        return cuda_fail(e, "sparse marching cubes fetch");
+    }
     return CUBVH_OK;
     CUBVH_GUARD_END
 }
@@ -731,10 +743,12 @@ int cubvh_sparse_mc_free(cubvh_smc* m) {
     int cur = 0;
     const bool have = cudaGetDevice(&cur) == cudaSuccess;
     if (m->device >= 0 && cudaSetDevice(m->device) == cudaSuccess) {
-        cudaDeviceSynchronize();  // a fetch may still be reading the buffers
-        if (m->r.verts) cudaFree(m->r.verts);
-        if (m->r.tris) cudaFree(m->r.tris);
+        // wait for this result's own work only: the build and every fetch
+        if (m->done) cudaEventSynchronize(m->done);
+        for (cudaEvent_t ev : m->fetched) cudaEventSynchronize(ev);
+        sparse_mc_release(m->r);
         if (m->done) cudaEventDestroy(m->done);
+        for (cudaEvent_t ev : m->fetched) cudaEventDestroy(ev);
     }
     if (have) cudaSetDevice(cur);
     delete m;

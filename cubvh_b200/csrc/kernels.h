@@ -101,8 +101,10 @@ int floodfill_noalloc(const uint8_t* grid, int B, int H, int W, int D, int32_t* 
 
 // Sparse marching cubes (sparse_mc.cu): device coords int32 [n, 3] and
 // corners float32 [n, 8]; the merged vertices float32 [n_verts, 3] and
-// triangles int32 [n_tris, 3] are cudaMalloc'd into `out` (the caller frees
-// them).  Returns 0, 1 (bad input, err set) or 2 (CUDA error, err set).
+// triangles int32 [n_tris, 3] are allocated into `out` from the library's
+// stream-ordered pool of the current device (released with
+// sparse_mc_release once no stream reads them any more).  Returns 0, 1 (bad
+// input, err set) or 2 (CUDA error, err set).
 struct SparseMCResult {
     float* verts = nullptr;
     int32_t* tris = nullptr;
@@ -110,5 +112,6 @@ struct SparseMCResult {
 };
 int sparse_mc_run(const int32_t* coords, const float* corners, int64_t n, float iso, bool ensure_consistency,
                   cudaStream_t stream, SparseMCResult& out, std::string& err);
+void sparse_mc_release(SparseMCResult& r);
 
 }  // namespace cubvh

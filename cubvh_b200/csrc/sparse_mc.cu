@@ -36,6 +36,7 @@
 #include <cstdint>
 #include <cub/cub.cuh>
 #include <cuda_runtime.h>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -349,9 +350,17 @@ __global__ void k_smc_bounds(int64_t n, const int32_t* __restrict__ coords, int3
         lo[k] = __reduce_min_sync(0xFFFFFFFFu, lo[k]);
         hi[k] = __reduce_max_sync(0xFFFFFFFFu, hi[k]);
     }
+    // warps meet in shared memory, then one atomic per block and bound (the
+    // six global words are the only addresses every block updates)
+    __shared__ int32_t sb[6];
+    if (threadIdx.x < 6) sb[threadIdx.x] = threadIdx.x < 3 ? INT32_MAX : INT32_MIN;
+    __syncthreads();
     if ((threadIdx.x & 31) == 0)
 #pragma unroll
-        for (int k = 0; k < 3; ++k) { atomicMin(&b[k], lo[k]); atomicMax(&b[3 + k], hi[k]); }
+        for (int k = 0; k < 3; ++k) { atomicMin(&sb[k], lo[k]); atomicMax(&sb[3 + k], hi[k]); }
+    __syncthreads();
+    if (threadIdx.x < 3) atomicMin(&b[threadIdx.x], sb[threadIdx.x]);
+    else if (threadIdx.x < 6) atomicMax(&b[threadIdx.x], sb[threadIdx.x]);
 }
 __global__ void k_smc_bounds_init(int32_t* b) {
     if (threadIdx.x < 3) b[threadIdx.x] = INT32_MAX;
@@ -373,21 +382,63 @@ int bits_for(uint64_t v) {  // bits to hold values below v
     return b;
 }
 
+// The library's stream-ordered pool on the current device.  A call waits
+// for its stream three times (the output sizes depend on the data); with the
+// default pool's release threshold of 0 every such wait hands the freed
+// temporaries back to the driver and the next allocation maps them again,
+// which cost more than the kernels.  This pool keeps up to kPoolKeep bytes
+// between calls and returns what is above that at each wait.
+constexpr uint64_t kPoolKeep = 256ull << 20;
+cudaError_t smc_pool(cudaMemPool_t* out) {
+    static std::mutex mu;
+    static std::vector<cudaMemPool_t> pools;  // by device ordinal, created on first use
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    if ((int)pools.size() <= dev) pools.resize((size_t)dev + 1, nullptr);
+    if (!pools[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        if ((e = cudaMemPoolCreate(&p, &props)) != cudaSuccess) return e;
+        uint64_t keep = kPoolKeep;
+        if ((e = cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) {
+            cudaMemPoolDestroy(p);
+            return e;
+        }
+        pools[dev] = p;
+    }
+    *out = pools[dev];
+    return cudaSuccess;
+}
+
+template <class T>
+cudaError_t pool_get(cudaMemPool_t pool, cudaStream_t s, T** out, size_t count) {
+    void* q = nullptr;
+    const cudaError_t e = cudaMallocFromPoolAsync(&q, count * sizeof(T) > 0 ? count * sizeof(T) : 16, pool, s);
+    if (e == cudaSuccess) *out = static_cast<T*>(q);
+    return e;
+}
+
 // Stream-ordered temporaries of one call: every buffer taken from `get` is
 // returned with cudaFreeAsync on the same stream, early through `put` or at
 // scope exit, so an error return in the middle of the pipeline leaks nothing.
 struct AsyncTemps {
+    cudaMemPool_t pool;
     cudaStream_t s;
     std::vector<void*> p;
-    explicit AsyncTemps(cudaStream_t st) : s(st) {}
+    AsyncTemps(cudaMemPool_t pl, cudaStream_t st) : pool(pl), s(st) {}
     AsyncTemps(const AsyncTemps&) = delete;
     AsyncTemps& operator=(const AsyncTemps&) = delete;
     ~AsyncTemps() { for (void* q : p) cudaFreeAsync(q, s); }
     template <class T>
     cudaError_t get(T** out, size_t count) {
-        void* q = nullptr;
-        const cudaError_t e = cudaMallocAsync(&q, count * sizeof(T) > 0 ? count * sizeof(T) : 16, s);
-        if (e == cudaSuccess) { p.push_back(q); *out = static_cast<T*>(q); }
+        const cudaError_t e = pool_get(pool, s, out, count);
+        if (e == cudaSuccess) p.push_back(*out);
         return e;
     }
     void put(void* q) {
@@ -398,9 +449,9 @@ struct AsyncTemps {
 
 }  // namespace
 
-// All temporaries come from cudaMallocAsync on `stream`; the results stay in
-// `out` (device, owned by the caller through cubvh_sparse_mc_*, which frees
-// them on an error return as well).
+// Temporaries and results come from the library's pool on `stream`; the
+// results stay in `out` (owned by the caller through cubvh_sparse_mc_*,
+// which releases them on an error return as well).
 int sparse_mc_run(const int32_t* coords, const float* corners, int64_t n, float iso, bool ensure_consistency,
                   cudaStream_t s, SparseMCResult& out, std::string& err) {
     out = SparseMCResult{};
@@ -408,10 +459,12 @@ int sparse_mc_run(const int32_t* coords, const float* corners, int64_t n, float 
     if (n > (int64_t)INT32_MAX / 12) { err = "too many voxels (the vertex count must fit in int32)"; return 1; }
     cudaError_t e;
     auto fail = [&](cudaError_t x, const char* what) { err = std::string(what) + ": " + cudaGetErrorString(x); return 2; };
-    AsyncTemps tmp(s);
+    cudaMemPool_t pool = nullptr;
+    if ((e = smc_pool(&pool)) != cudaSuccess) return fail(e, "memory pool");
+    AsyncTemps tmp(pool, s);
     // coordinate bounds -> key packing (host round trip)
     int32_t* d_b = nullptr;
-    if ((e = tmp.get(&d_b, 6)) != cudaSuccess) return fail(e, "cudaMallocAsync");
+    if ((e = tmp.get(&d_b, 6)) != cudaSuccess) return fail(e, "pool allocation");
     k_smc_bounds_init<<<1, 32, 0, s>>>(d_b); count_launch();
     k_smc_bounds<<<grid_for(n), 256, 0, s>>>(n, coords, d_b); count_launch();
     int32_t b[6];
@@ -436,12 +489,12 @@ int sparse_mc_run(const int32_t* coords, const float* corners, int64_t n, float 
         if ((e = tmp.get(&avg, m8)) != cudaSuccess || (e = tmp.get(&ck, m8)) != cudaSuccess ||
             (e = tmp.get(&ck2, m8)) != cudaSuccess || (e = tmp.get(&ci, m8)) != cudaSuccess ||
             (e = tmp.get(&ci2, m8)) != cudaSuccess)
-            return fail(e, "cudaMallocAsync");
+            return fail(e, "pool allocation");
         k_smc_corner_keys<<<grid_for(m8), 256, 0, s>>>(n, coords, kp, ck, ci); count_launch();
         size_t tb = 0;
         char* cub_tmp = nullptr;
         cub::DeviceRadixSort::SortPairs(nullptr, tb, ck, ck2, ci, ci2, (int)m8, 0, cbits, s);
-        if ((e = tmp.get(&cub_tmp, tb)) != cudaSuccess) return fail(e, "cudaMallocAsync");
+        if ((e = tmp.get(&cub_tmp, tb)) != cudaSuccess) return fail(e, "pool allocation");
         if ((e = cub::DeviceRadixSort::SortPairs(cub_tmp, tb, ck, ck2, ci, ci2, (int)m8, 0, cbits, s)) != cudaSuccess)
             return fail(e, "corner sort");
         count_launch();
@@ -455,7 +508,7 @@ int sparse_mc_run(const int32_t* coords, const float* corners, int64_t n, float 
     const int64_t nb = scan::num_chunks(n) + 1;
     if ((e = tmp.get(&nv, n + 1)) != cudaSuccess || (e = tmp.get(&nt, n + 1)) != cudaSuccess ||
         (e = tmp.get(&bs, nb)) != cudaSuccess)
-        return fail(e, "cudaMallocAsync");
+        return fail(e, "pool allocation");
     k_smc_count<<<g, 256, 0, s>>>(n, use, iso, nv, nt); count_launch();
     scan::exclusive(nv, bs, n, s);   // nv[n] = total
     scan::exclusive(nt, bs, n, s);
@@ -476,7 +529,7 @@ int sparse_mc_run(const int32_t* coords, const float* corners, int64_t n, float 
             (e = tmp.get(&ord2, m)) != cudaSuccess || (e = tmp.get(&map, m)) != cudaSuccess ||
             (e = tmp.get(&head, m + 1)) != cudaSuccess || (e = tmp.get(&ids, m + 1)) != cudaSuccess ||
             (e = tmp.get(&bs2, nb2)) != cudaSuccess ||
-            (e = cudaMalloc(&out.tris, sizeof(int32_t) * 3 * (t > 0 ? t : 1))) != cudaSuccess)
+            (e = pool_get(pool, s, &out.tris, (size_t)(3 * t))) != cudaSuccess)
             return fail(e, "sparse marching cubes buffers");
         k_smc_emit<<<g, 256, 0, s>>>(n, coords, use, iso, nv, nt, kp, pos, key, out.tris); count_launch();
         // emission index as the value: the stable sort keeps each key's lowest first
@@ -484,7 +537,7 @@ int sparse_mc_run(const int32_t* coords, const float* corners, int64_t n, float 
         size_t tb = 0;
         char* cub_tmp = nullptr;
         cub::DeviceRadixSort::SortPairs(nullptr, tb, key, key2, ord, ord2, (int)m, 0, key_bits, s);
-        if ((e = tmp.get(&cub_tmp, tb)) != cudaSuccess) return fail(e, "cudaMallocAsync");
+        if ((e = tmp.get(&cub_tmp, tb)) != cudaSuccess) return fail(e, "pool allocation");
         if ((e = cub::DeviceRadixSort::SortPairs(cub_tmp, tb, key, key2, ord, ord2, (int)m, 0, key_bits, s)) !=
             cudaSuccess)
             return fail(e, "edge key sort");
@@ -497,8 +550,8 @@ int sparse_mc_run(const int32_t* coords, const float* corners, int64_t n, float 
         if ((e = cudaMemcpyAsync(&u, ids + m, sizeof(uint32_t), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
             (e = cudaStreamSynchronize(s)) != cudaSuccess)
             return fail(e, "sparse marching cubes merge");
-        if ((e = cudaMalloc(&out.verts, sizeof(float) * 3 * (u > 0 ? u : 1))) != cudaSuccess)
-            return fail(e, "cudaMalloc(vertices)");
+        if ((e = pool_get(pool, s, &out.verts, (size_t)3 * u)) != cudaSuccess)
+            return fail(e, "vertex buffer");
         k_smc_merge<<<grid_for(m), 256, 0, s>>>(m, head, ids, ord2, pos, map, out.verts); count_launch();
         if (t > 0) { k_smc_remap<<<grid_for(3 * t), 256, 0, s>>>(3 * t, map, out.tris); count_launch(); }
         out.n_verts = u;
@@ -506,6 +559,14 @@ int sparse_mc_run(const int32_t* coords, const float* corners, int64_t n, float 
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "sparse marching cubes launch");
     return 0;
+}
+
+// The caller has waited for every stream that used the buffers (host-side),
+// so the frees need no ordering: the per-thread stream takes them.
+void sparse_mc_release(SparseMCResult& r) {
+    if (r.verts) cudaFreeAsync(r.verts, cudaStreamPerThread);
+    if (r.tris) cudaFreeAsync(r.tris, cudaStreamPerThread);
+    r = SparseMCResult{};
 }
 
 }  // namespace cubvh

@@ -153,8 +153,10 @@ int cubvh_signed_distance_host(cubvh_bvh* bvh, const float* points, int64_t n, u
  * [n_verts, 3], voxel units) and *n_tris triangles (int32 [n_tris, 3]);
  * cubvh_sparse_mc_fetch copies them into device arrays of those sizes on
  * its own `stream` (any stream: the copies wait for the building stream's
- * last kernels), cubvh_sparse_mc_free releases the result (it waits for the
- * device first, as a fetch may still be reading).  The vertex array equals the
+ * last kernels), cubvh_sparse_mc_free releases the result (it waits for this
+ * result's build and fetches first, not for other work on the device).  The
+ * result's memory, and the call's temporaries, come from a stream-ordered
+ * pool of the library's own that keeps up to 256 MiB between calls.  The vertex array equals the
  * reference's (one vertex per cut voxel edge, merged across voxels, sorted
  * by edge); the triangulation is this library's own (see sparse_mc.cu): a
  * closed, consistently oriented surface where the corner values agree.
