@@ -691,6 +691,10 @@ int cubvh_sparse_marching_cubes(const int32_t* coords, const float* corners, int
     if (n < 0) return fail(CUBVH_ERR_INVALID, "negative voxel count");
     if (n > 0 && (!coords || !corners)) return fail(CUBVH_ERR_INVALID, "coords/corners is null");
     auto* m = new cubvh_smc();
+    if (n == 0) {  // empty result: no device work, no buffers, no event
+        *out = m;
+        return CUBVH_OK;
+    }
     cudaGetDevice(&m->device);
     std::string err;
     const int rc = sparse_mc_run(coords, corners, n, iso, ensure_consistency != 0, (cudaStream_t)stream, m->r, err);
@@ -718,6 +722,7 @@ int cubvh_sparse_mc_fetch(cubvh_smc* m, float* verts, int32_t* tris, void* strea
     CUBVH_GUARD_BEGIN
     if (!m) return fail(CUBVH_ERR_INVALID, "result is null");
     if ((m->r.n_verts && !verts) || (m->r.n_tris && !tris)) return fail(CUBVH_ERR_INVALID, "verts/tris is null");
+    if (!m->r.n_verts && !m->r.n_tris) return CUBVH_OK;  // nothing to copy
     cudaStream_t s = (cudaStream_t)stream;
     cudaError_t e = m->done ? cudaStreamWaitEvent(s, m->done, 0) : cudaSuccess;
     if (e == cudaSuccess && m->r.n_verts)
@@ -740,9 +745,13 @@ int cubvh_sparse_mc_fetch(cubvh_smc* m, float* verts, int32_t* tris, void* strea
 
 int cubvh_sparse_mc_free(cubvh_smc* m) {
     if (!m) return CUBVH_OK;
+    if (m->device < 0) {  // empty result: nothing on a device
+        delete m;
+        return CUBVH_OK;
+    }
     int cur = 0;
     const bool have = cudaGetDevice(&cur) == cudaSuccess;
-    if (m->device >= 0 && cudaSetDevice(m->device) == cudaSuccess) {
+    if (cudaSetDevice(m->device) == cudaSuccess) {
         // wait for this result's own work only: the build and every fetch
         if (m->done) cudaEventSynchronize(m->done);
         for (cudaEvent_t ev : m->fetched) cudaEventSynchronize(ev);

@@ -203,3 +203,25 @@ def test_max_over_ranks_gloo_world2():
     for p in procs:
         p.join(timeout=60)
     assert res == {0: 15.0, 1: 15.0}
+
+
+def test_sparse_mc_abi_without_device_work():
+    """Argument checks and the empty result of the sparse marching cubes
+    entry points need no GPU: errors come back as status 1, an empty voxel
+    set gives an empty result that fetches and frees without device work."""
+    L = _lib.lib()
+    res, nv, nt = ctypes.c_void_p(), ctypes.c_int64(7), ctypes.c_int64(7)
+    assert L.cubvh_sparse_marching_cubes(None, None, 5, 0.0, 0, None, ctypes.byref(res), ctypes.byref(nv),
+                                         ctypes.byref(nt)) == 1
+    assert b"null" in L.cubvh_last_error() and not res.value and nv.value == 0 and nt.value == 0
+    assert L.cubvh_sparse_marching_cubes(None, None, -1, 0.0, 0, None, ctypes.byref(res), ctypes.byref(nv),
+                                         ctypes.byref(nt)) == 1
+    assert b"negative" in L.cubvh_last_error()
+    assert L.cubvh_sparse_marching_cubes(None, None, 0, 0.0, 0, None, None, ctypes.byref(nv), ctypes.byref(nt)) == 1
+    assert L.cubvh_sparse_mc_fetch(None, None, None, None) == 1
+    assert L.cubvh_sparse_mc_free(None) == 0
+    assert L.cubvh_sparse_marching_cubes(None, None, 0, 0.0, 0, None, ctypes.byref(res), ctypes.byref(nv),
+                                         ctypes.byref(nt)) == 0
+    assert res.value and nv.value == 0 and nt.value == 0
+    assert L.cubvh_sparse_mc_fetch(res, None, None, None) == 0
+    assert L.cubvh_sparse_mc_free(res) == 0
