@@ -15,7 +15,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
+#include <numeric>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -136,15 +138,28 @@ int cubvh_arena_create(int32_t n_meshes, const float* const* vertices, const int
                 std::memcpy(&xyz[m][(size_t)f * 9 + 3 * k], vertices[m] + 3 * v, 3 * sizeof(float));
             }
     }
-    // build every mesh, in parallel
+    // build every mesh, in parallel: one thread per mesh at a time (each
+    // build single-threaded), largest meshes first from a shared queue so the
+    // last builds to finish are small ones
     const int nthr = std::max(1, std::min<int>(M, (int)std::thread::hardware_concurrency()));
+    std::vector<int> order(M);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return n_faces[a] > n_faces[b]; });
+    std::atomic<int> next{0};
     std::vector<std::thread> pool;
     for (int t = 0; t < nthr; ++t)
-        pool.emplace_back([&, t] {
-            for (int m = t; m < M; m += nthr) {
+        pool.emplace_back([&] {
+            for (int i; (i = next.fetch_add(1)) < M;) {
+                const int m = order[i];
                 const int leaf = max_leaf ? max_leaf[m] : kMaxLeafTris;
-                if (!build_bvh(xyz[m].data(), n_faces[m], hb[m], errs[m], leaf) && errs[m].empty())
-                    errs[m] = "build failed";
+                try {  // an exception must not leave the worker thread
+                    if (!build_bvh(xyz[m].data(), n_faces[m], hb[m], errs[m], leaf, 1) && errs[m].empty())
+                        errs[m] = "build failed";
+                } catch (const std::bad_alloc&) {
+                    errs[m] = "host allocation failed";
+                } catch (const std::exception& ex) {
+                    errs[m] = ex.what();
+                }
             }
         });
     for (auto& th : pool) th.join();

@@ -8,11 +8,14 @@
 #include "build.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <functional>
 #include <limits>
 #include <numeric>
+#include <exception>
+#include <thread>
 
 namespace cubvh {
 namespace {
@@ -39,90 +42,166 @@ struct Node2 {
     int begin = 0, count = 0;      // leaf range (count > 0 for leaves)
 };
 
+// One triangle's box, centroid and face index: the builder keeps these
+// records in the order it partitions them, so every pass over a range reads
+// memory sequentially.
+struct Prim {
+    Box box;
+    float c[3];
+    int id;
+};
+
 struct Builder {
-    const float* xyz;              // [F, 9]
-    std::vector<Box> pbox;
-    std::vector<float> cen;        // [F, 3]
-    std::vector<int> idx;
-    std::vector<Node2> nodes;
+    std::vector<Prim> prim;
 
     static constexpr int kBins = 32;
     static constexpr float kTrav = 1.0f, kIsect = 1.0f;
+    // ranges at least this large may build their left half on another thread
+    static constexpr int kParMin = 4096;
     int max_leaf = kMaxLeafTris;
+    std::atomic<int> spare{0};     // threads that may still be started
 
-    int make_leaf(int b, int e, const Box& box) {
+    bool take_thread() {
+        int s = spare.load();
+        while (s > 0 && !spare.compare_exchange_weak(s, s - 1)) {}
+        return s > 0;
+    }
+
+    static int make_leaf(std::vector<Node2>& nodes, int b, int e, const Box& box) {
         Node2 n; n.box = box; n.begin = b; n.count = e - b;
         nodes.push_back(n);
         return (int)nodes.size() - 1;
     }
 
-    int build(int b, int e) {
-        Box box, cb;
-        for (int i = b; i < e; ++i) { box.grow(pbox[idx[i]]); cb.grow(&cen[3 * idx[i]]); }
-        const int n = e - b;
-        if (n == 1) return make_leaf(b, e, box);
+    static int bin_of(float c, float lo, float k) {
+        const int bi = (int)((c - lo) * k);
+        return std::min(std::max(bi, 0), kBins - 1);
+    }
 
-        // binned SAH over the three axes
-        float best_cost = INFINITY; int best_axis = -1, best_split = -1;
+    // Binary node for prim[b, e) and its subtree, appended to `nodes`; the
+    // returned index is the subtree's root.  The tree depends only on the
+    // range's contents, not on which thread or vector builds it.
+    int build(int b, int e, std::vector<Node2>& nodes) {
+        Box box, cb;
+        for (int i = b; i < e; ++i) { box.grow(prim[i].box); cb.grow(prim[i].c); }
+        const int n = e - b;
+        if (n == 1) return make_leaf(nodes, b, e, box);
+
+        // binned SAH over the three axes, all binned in one pass.  Only
+        // non-empty bins are visited: every split between two consecutive
+        // non-empty bins puts the same triangles on each side at the same
+        // cost, and the lowest such split (the one just after the lower
+        // bin) is the one a sweep over all bins keeps.
+        bool act[3];
+        float kk[3];
         for (int ax = 0; ax < 3; ++ax) {
             const float ext = cb.hi[ax] - cb.lo[ax];
-            if (!(ext > 0.f)) continue;
-            Box bb[kBins]; int bc[kBins] = {0};
-            const float k = (float)kBins * (1.f - 1e-6f) / ext;
-            for (int i = b; i < e; ++i) {
-                int bi = (int)((cen[3 * idx[i] + ax] - cb.lo[ax]) * k);
-                bi = std::min(std::max(bi, 0), kBins - 1);
-                bb[bi].grow(pbox[idx[i]]); bc[bi]++;
+            act[ax] = ext > 0.f;
+            kk[ax] = act[ax] ? (float)kBins * (1.f - 1e-6f) / ext : 0.f;
+        }
+        Box bb[3][kBins];  // valid where bc > 0
+        int bc[3][kBins] = {};
+        for (int i = b; i < e; ++i) {
+            const Prim& p = prim[i];
+            for (int ax = 0; ax < 3; ++ax) {
+                if (!act[ax]) continue;
+                const int bi = bin_of(p.c[ax], cb.lo[ax], kk[ax]);
+                if (bc[ax][bi]++ == 0) bb[ax][bi] = p.box;
+                else bb[ax][bi].grow(p.box);
             }
-            float ra[kBins]; int rc[kBins];
-            Box acc; int cnt = 0;
-            for (int i = kBins - 1; i > 0; --i) {
-                acc.grow(bb[i]); cnt += bc[i];
-                ra[i] = acc.area(); rc[i] = cnt;
+        }
+        float best_cost = INFINITY; int best_axis = -1, best_split = -1;
+        for (int ax = 0; ax < 3; ++ax) {
+            if (!act[ax]) continue;
+            int ne[kBins], nb = 0;
+            for (int i = 0; i < kBins; ++i)
+                if (bc[ax][i]) ne[nb++] = i;
+            if (nb < 2) continue;
+            float ra[kBins]; int rc[kBins];  // suffix area / count from non-empty bin j up
+            Box acc = bb[ax][ne[nb - 1]]; int cnt = bc[ax][ne[nb - 1]];
+            for (int j = nb - 2; j >= 1; --j) {
+                acc.grow(bb[ax][ne[j]]); cnt += bc[ax][ne[j]];
+                ra[j] = acc.area(); rc[j] = cnt;
             }
+            ra[nb - 1] = bb[ax][ne[nb - 1]].area(); rc[nb - 1] = bc[ax][ne[nb - 1]];
             acc = Box(); cnt = 0;
-            for (int i = 0; i < kBins - 1; ++i) {
-                acc.grow(bb[i]); cnt += bc[i];
-                if (cnt == 0 || rc[i + 1] == 0) continue;
-                const float c = acc.area() * cnt + ra[i + 1] * rc[i + 1];
-                if (c < best_cost) { best_cost = c; best_axis = ax; best_split = i; }
+            for (int j = 0; j < nb - 1; ++j) {
+                acc.grow(bb[ax][ne[j]]); cnt += bc[ax][ne[j]];
+                const float c = acc.area() * cnt + ra[j + 1] * rc[j + 1];
+                if (c < best_cost) { best_cost = c; best_axis = ax; best_split = ne[j]; }
             }
         }
         const float parea = std::max(box.area(), 1e-30f);
         const float split_cost = kTrav + kIsect * best_cost / parea;
         if (n <= max_leaf && (best_axis < 0 || kIsect * n <= split_cost))
-            return make_leaf(b, e, box);
+            return make_leaf(nodes, b, e, box);
 
         int mid;
         if (best_axis < 0) {
             mid = b + n / 2;  // all centroids coincide: split the range
         } else {
-            const float ext = cb.hi[best_axis] - cb.lo[best_axis];
-            const float k = (float)kBins * (1.f - 1e-6f) / ext;
-            auto it = std::partition(idx.begin() + b, idx.begin() + e, [&](int t) {
-                int bi = (int)((cen[3 * t + best_axis] - cb.lo[best_axis]) * k);
-                bi = std::min(std::max(bi, 0), kBins - 1);
-                return bi <= best_split;
-            });
-            mid = (int)(it - idx.begin());
+            const float lo = cb.lo[best_axis], k = kk[best_axis];
+            auto it = std::partition(prim.begin() + b, prim.begin() + e,
+                                     [&](const Prim& p) { return bin_of(p.c[best_axis], lo, k) <= best_split; });
+            mid = (int)(it - prim.begin());
             if (mid == b || mid == e) mid = b + n / 2;
         }
         const int me = (int)nodes.size();
         nodes.emplace_back();
         nodes[me].box = box;
-        const int l = build(b, mid);
-        const int r = build(mid, e);
+        int l, r;
+        if (n >= kParMin && take_thread()) {
+            // left half on a thread of its own, into its own vector, spliced
+            // after the right half (child indices shifted by the splice point)
+            std::vector<Node2> ln;
+            ln.reserve(2 * (size_t)(mid - b));
+            int lroot = -1;
+            std::exception_ptr fail;
+            std::thread t([&] {
+                try { lroot = build(b, mid, ln); } catch (...) { fail = std::current_exception(); }
+            });
+            try {
+                r = build(mid, e, nodes);
+            } catch (...) {
+                t.join();
+                throw;
+            }
+            t.join();
+            spare.fetch_add(1);
+            if (fail) std::rethrow_exception(fail);
+            const int off = (int)nodes.size();
+            for (Node2 nd : ln) {
+                if (nd.count == 0) { nd.left += off; nd.right += off; }
+                nodes.push_back(nd);
+            }
+            l = lroot + off;
+        } else {
+            l = build(b, mid, nodes);
+            r = build(mid, e, nodes);
+        }
         nodes[me].left = l; nodes[me].right = r;
         return me;
     }
 };
+
+// 2^e as a float: built from its exponent bits where 2^e is a normal float
+// (the same value std::ldexp(1.0f, e) returns), std::ldexp elsewhere.
+float pow2f(int e) {
+    if (e >= -126 && e <= 127) {
+        const uint32_t bits = (uint32_t)(e + 127) << 23;
+        float f;
+        std::memcpy(&f, &bits, sizeof(f));
+        return f;
+    }
+    return std::ldexp(1.0f, e);
+}
 
 // Smallest e such that o + 255 * 2^e >= hi in float arithmetic.
 int pick_exponent(float o, float hi) {
     if (!(hi > o)) return -100;
     int e = (int)std::ceil(std::log2((double)(hi - o) / 255.0)) - 1;
     e = std::max(e, -100);
-    while (o + 255.0f * std::ldexp(1.0f, e) < hi) ++e;
+    while (o + 255.0f * pow2f(e) < hi) ++e;
     return e;
 }
 
@@ -132,7 +211,7 @@ void quantise_child(const CNode& nd, int j, const Box& cb, CNode& out) {
     uint8_t* qlo[3] = {out.qlo_x, out.qlo_y, out.qlo_z};
     uint8_t* qhi[3] = {out.qhi_x, out.qhi_y, out.qhi_z};
     for (int k = 0; k < 3; ++k) {
-        const float s = std::ldexp(1.0f, ex[k]);
+        const float s = pow2f(ex[k]);
         int ql = (int)std::floor((double)(cb.lo[k] - o[k]) / (double)s);
         int qh = (int)std::ceil((double)(cb.hi[k] - o[k]) / (double)s);
         ql = std::min(std::max(ql, 0), 255); qh = std::min(std::max(qh, 0), 255);
@@ -172,7 +251,7 @@ Box tri_box(const CTri& t) {
 
 }  // namespace
 
-bool build_bvh(const float* xyz, int64_t nf, HostBvh& out, std::string& err, int max_leaf) {
+bool build_bvh(const float* xyz, int64_t nf, HostBvh& out, std::string& err, int max_leaf, int threads) {
     if (nf <= 0) { err = "mesh has no faces"; return false; }
     if (nf > (int64_t)(1 << 28)) { err = "too many faces (limit 2^28)"; return false; }
     for (int64_t i = 0; i < nf * 9; ++i)
@@ -180,71 +259,72 @@ bool build_bvh(const float* xyz, int64_t nf, HostBvh& out, std::string& err, int
 
     if (max_leaf < 1 || max_leaf > kMaxLeafTris) { err = "leaf size must be in [1, 4]"; return false; }
     Builder B;
-    B.xyz = xyz;
     B.max_leaf = max_leaf;
-    B.pbox.resize(nf); B.cen.resize(3 * nf); B.idx.resize(nf);
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    B.spare = threads - 1;
+    B.prim.resize(nf);
     for (int64_t f = 0; f < nf; ++f) {
+        Prim& p = B.prim[f];
         Box b; b.grow(xyz + 9 * f); b.grow(xyz + 9 * f + 3); b.grow(xyz + 9 * f + 6);
-        B.pbox[f] = b;
-        for (int k = 0; k < 3; ++k) B.cen[3 * f + k] = 0.5f * (b.lo[k] + b.hi[k]);
-        B.idx[f] = (int)f;
+        p.box = b;
+        for (int k = 0; k < 3; ++k) p.c[k] = 0.5f * (b.lo[k] + b.hi[k]);
+        p.id = (int)f;
     }
-    B.nodes.reserve(2 * nf);
-    const int root = B.build(0, (int)nf);
+    std::vector<Node2> nodes;
+    nodes.reserve(2 * nf);
+    const int root = B.build(0, (int)nf, nodes);
 
     // collapse to 8-wide: each wide node lists binary-tree nodes as children
-    auto expand = [&](int r) {
-        std::vector<int> ch;
-        if (B.nodes[r].count > 0) { ch.push_back(r); return ch; }
-        ch.push_back(B.nodes[r].left); ch.push_back(B.nodes[r].right);
-        while ((int)ch.size() < kWidth) {
+    // children of wide node r: open the largest-area internal child in place
+    // (its two children take its position) until kWidth children or leaves only
+    auto expand = [&](int r, int* ch) {
+        if (nodes[r].count > 0) { ch[0] = r; return 1; }
+        int m = 2;
+        ch[0] = nodes[r].left; ch[1] = nodes[r].right;
+        while (m < kWidth) {
             int bi = -1; float ba = -1.f;
-            for (int i = 0; i < (int)ch.size(); ++i) {
-                const Node2& n = B.nodes[ch[i]];
+            for (int i = 0; i < m; ++i) {
+                const Node2& n = nodes[ch[i]];
                 if (n.count > 0) continue;
                 const float a = n.box.area();
                 if (a > ba) { ba = a; bi = i; }
             }
             if (bi < 0) break;
             const int c = ch[bi];
-            ch[bi] = B.nodes[c].left;
-            ch.insert(ch.begin() + bi + 1, B.nodes[c].right);
+            for (int i = m; i > bi + 1; --i) ch[i] = ch[i - 1];
+            ch[bi] = nodes[c].left;
+            ch[bi + 1] = nodes[c].right;
+            ++m;
         }
-        return ch;
+        return m;
     };
 
     out.nodes.clear(); out.tris.clear();
-    out.tris.reserve(nf);
+    std::vector<int32_t> soup((size_t)nf);  // soup slot -> face id, filled in leaf order
+    int64_t n_soup = 0;
     struct Item { int bin; int level; };
     std::vector<Item> queue{{root, 1}};
+    queue.reserve(nodes.size());       // wide nodes <= binary nodes
+    out.nodes.reserve(nodes.size());
     out.nodes.emplace_back();
     int max_depth = 1;
     for (size_t qi = 0; qi < queue.size(); ++qi) {
         const Item it = queue[qi];
-        const std::vector<int> ch = expand(it.bin);
+        int ch[kWidth];
+        const int nch = expand(it.bin, ch);
         CNode nd;
         std::memset(&nd, 0, sizeof(nd));
         std::memset(nd.meta, kEmpty, sizeof(nd.meta));
-        set_frame(nd, B.nodes[it.bin].box);
+        set_frame(nd, nodes[it.bin].box);
         nd.child_base = (int32_t)out.nodes.size();
-        nd.tri_base = (int32_t)out.tris.size();
+        nd.tri_base = (int32_t)n_soup;
         int slot = 0;
-        for (int j = 0; j < (int)ch.size(); ++j) {
-            const Node2& c = B.nodes[ch[j]];
+        for (int j = 0; j < nch; ++j) {
+            const Node2& c = nodes[ch[j]];
             quantise_child(nd, j, c.box, nd);
             if (c.count > 0) {
-                const int off = (int)out.tris.size() - nd.tri_base;
-                for (int t = c.begin; t < c.begin + c.count; ++t) {
-                    const int f = B.idx[t];
-                    const float* p = xyz + 9 * (int64_t)f;
-                    CTri tr;
-                    tr.ax = p[0]; tr.ay = p[1]; tr.az = p[2]; tr.id = f;
-                    tr.bx = p[3]; tr.by = p[4]; tr.bz = p[5];
-                    tr.cx = p[6]; tr.cy = p[7]; tr.cz = p[8];
-                    set_error_scales(tr);
-                    if (f == 0) out.slot_of_face0 = (int64_t)out.tris.size();
-                    out.tris.push_back(tr);
-                }
+                const int off = (int)(n_soup - nd.tri_base);
+                for (int t = c.begin; t < c.begin + c.count; ++t) soup[(size_t)n_soup++] = B.prim[t].id;
                 nd.meta[j] = (uint8_t)(((c.count - 1) << 5) | off);
             } else {
                 nd.meta[j] = (uint8_t)(0x80 | slot);
@@ -257,12 +337,32 @@ bool build_bvh(const float* xyz, int64_t nf, HostBvh& out, std::string& err, int
         nd.n_internal = (uint8_t)slot;
         out.nodes[qi] = nd;
     }
+    // triangle records in soup order; the vertex reads follow the leaves, not
+    // the input order, so they are prefetched a few slots ahead
+    out.tris.resize((size_t)n_soup);
+    constexpr int64_t kAhead = 16;
+    for (int64_t t = 0; t < n_soup; ++t) {
+        if (t + kAhead < n_soup) {
+            const float* q = xyz + 9 * (int64_t)soup[(size_t)(t + kAhead)];
+            __builtin_prefetch(q);
+            __builtin_prefetch(q + 8);
+        }
+        const int f = soup[(size_t)t];
+        const float* p = xyz + 9 * (int64_t)f;
+        CTri tr;
+        tr.ax = p[0]; tr.ay = p[1]; tr.az = p[2]; tr.id = f;
+        tr.bx = p[3]; tr.by = p[4]; tr.bz = p[5];
+        tr.cx = p[6]; tr.cy = p[7]; tr.cz = p[8];
+        set_error_scales(tr);
+        if (f == 0) out.slot_of_face0 = t;
+        out.tris[(size_t)t] = tr;
+    }
     out.depth = max_depth;
     out.level_start.assign(1, 0);
     for (size_t qi = 1; qi < queue.size(); ++qi)
         if (queue[qi].level != queue[qi - 1].level) out.level_start.push_back((int32_t)qi);
     out.level_start.push_back((int32_t)queue.size());
-    const Box& rb = B.nodes[root].box;
+    const Box& rb = nodes[root].box;
     for (int k = 0; k < 3; ++k) { out.lo[k] = rb.lo[k]; out.hi[k] = rb.hi[k]; }
     if (out.depth > kMaxDepth) {
         err = "BVH deeper than the traversal stack supports (" + std::to_string(out.depth) + " levels)";

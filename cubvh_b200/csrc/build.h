@@ -25,8 +25,10 @@ struct HostBvh {
 
 // Builds the wide BVH over triangles (a, b, c per face, original face index
 // = position).  tri_xyz: [F, 9] floats.  Returns false and sets err on bad input.
+// threads: host threads the build may use (0 = all cores); the tree is the
+// same for any count.
 bool build_bvh(const float* tri_xyz, int64_t n_faces, HostBvh& out, std::string& err,
-               int max_leaf = kMaxLeafTris);
+               int max_leaf = kMaxLeafTris, int threads = 0);
 
 // Recomputes the quantised boxes of every node from the current triangle
 // soup, keeping the topology (used after the soup's vertices moved).

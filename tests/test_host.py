@@ -225,3 +225,23 @@ def test_sparse_mc_abi_without_device_work():
     assert res.value and nv.value == 0 and nt.value == 0
     assert L.cubvh_sparse_mc_fetch(res, None, None, None) == 0
     assert L.cubvh_sparse_mc_free(res) == 0
+
+
+LAYOUT_SHA256 = {
+    # sha256 of the node and triangle arrays (cubvh_bvh_layout) of the host
+    # build; the build splits large ranges across threads, and the tree must
+    # not depend on how they are scheduled
+    "ico6": "d6f798fcb377fbc07b62e2d818314a1ed15ab49483290a3d1db4a90e1639aa18",
+    "tori": "ff842ae599bcdd508be50c66afc69923de7f22d936805246ae9e7bbb345da908",
+    "ico3": "7dd8dd1e51f207b2e627fd6a9eb2e309ba2d859a6c51110806558832f9d8a9dc",
+}
+
+
+@pytest.mark.parametrize("mesh", sorted(LAYOUT_SHA256))
+def test_host_build_is_deterministic(mesh):
+    import hashlib
+    v, f = {"ico6": lambda: W.displaced_icosphere(6, 1), "tori": lambda: W.random_tori(2),
+            "ico3": lambda: W.displaced_icosphere(3, 1)}[mesh]()
+    for _ in range(2):
+        nodes, tris, _ = layout(cubvh.cuBVH(v, f))
+        assert hashlib.sha256(nodes.tobytes() + tris.tobytes()).hexdigest() == LAYOUT_SHA256[mesh]
