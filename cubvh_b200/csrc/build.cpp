@@ -15,6 +15,7 @@
 #include <limits>
 #include <numeric>
 #include <exception>
+#include <system_error>
 #include <thread>
 
 namespace cubvh {
@@ -150,16 +151,23 @@ struct Builder {
         nodes.emplace_back();
         nodes[me].box = box;
         int l, r;
+        std::vector<Node2> ln;
+        int lroot = -1;
+        std::exception_ptr fail;
+        std::thread t;
         if (n >= kParMin && take_thread()) {
             // left half on a thread of its own, into its own vector, spliced
             // after the right half (child indices shifted by the splice point)
-            std::vector<Node2> ln;
             ln.reserve(2 * (size_t)(mid - b));
-            int lroot = -1;
-            std::exception_ptr fail;
-            std::thread t([&] {
-                try { lroot = build(b, mid, ln); } catch (...) { fail = std::current_exception(); }
-            });
+            try {
+                t = std::thread([&] {
+                    try { lroot = build(b, mid, ln); } catch (...) { fail = std::current_exception(); }
+                });
+            } catch (const std::system_error&) {  // no thread to be had: build it here
+                spare.fetch_add(1);
+            }
+        }
+        if (t.joinable()) {
             try {
                 r = build(mid, e, nodes);
             } catch (...) {
