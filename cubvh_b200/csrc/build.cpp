@@ -257,6 +257,29 @@ Box tri_box(const CTri& t) {
     return b;
 }
 
+// fn(lo, hi) over [0, n) split into contiguous ranges of at least `grain`
+// items on up to `threads` threads (the caller's thread takes the first
+// range; a range whose thread cannot be started runs on the caller's thread).
+// fn must not throw.
+template <class F>
+void parallel_for(int64_t n, int threads, int64_t grain, F fn) {
+    const int64_t parts = std::max<int64_t>(1, std::min<int64_t>(threads, (n + grain - 1) / grain));
+    if (parts <= 1) { fn(0, n); return; }
+    std::vector<std::thread> pool;
+    std::vector<int64_t> inline_parts;
+    for (int64_t i = 1; i < parts; ++i) {
+        const int64_t lo = n * i / parts, hi = n * (i + 1) / parts;
+        try {
+            pool.emplace_back([=, &fn] { fn(lo, hi); });
+        } catch (const std::system_error&) {
+            inline_parts.push_back(i);
+        }
+    }
+    fn(0, n / parts);
+    for (int64_t i : inline_parts) fn(n * i / parts, n * (i + 1) / parts);
+    for (auto& t : pool) t.join();
+}
+
 }  // namespace
 
 bool build_bvh(const float* xyz, int64_t nf, HostBvh& out, std::string& err, int max_leaf, int threads) {
@@ -311,25 +334,28 @@ bool build_bvh(const float* xyz, int64_t nf, HostBvh& out, std::string& err, int
     std::vector<int32_t> soup((size_t)nf);  // soup slot -> face id, filled in leaf order
     int64_t n_soup = 0;
     struct Item { int bin; int level; };
+    struct Kids { int ch[kWidth]; int n; };
     std::vector<Item> queue{{root, 1}};
+    std::vector<Kids> kids;
     queue.reserve(nodes.size());       // wide nodes <= binary nodes
+    kids.reserve(nodes.size());
     out.nodes.reserve(nodes.size());
     out.nodes.emplace_back();
     int max_depth = 1;
+    // breadth-first pass: children, slots, child and triangle bases, soup
+    // order (the indices depend on the order, so this pass is serial)
     for (size_t qi = 0; qi < queue.size(); ++qi) {
         const Item it = queue[qi];
-        int ch[kWidth];
-        const int nch = expand(it.bin, ch);
+        Kids k;
+        k.n = expand(it.bin, k.ch);
         CNode nd;
         std::memset(&nd, 0, sizeof(nd));
         std::memset(nd.meta, kEmpty, sizeof(nd.meta));
-        set_frame(nd, nodes[it.bin].box);
         nd.child_base = (int32_t)out.nodes.size();
         nd.tri_base = (int32_t)n_soup;
         int slot = 0;
-        for (int j = 0; j < nch; ++j) {
-            const Node2& c = nodes[ch[j]];
-            quantise_child(nd, j, c.box, nd);
+        for (int j = 0; j < k.n; ++j) {
+            const Node2& c = nodes[k.ch[j]];
             if (c.count > 0) {
                 const int off = (int)(n_soup - nd.tri_base);
                 for (int t = c.begin; t < c.begin + c.count; ++t) soup[(size_t)n_soup++] = B.prim[t].id;
@@ -337,34 +363,47 @@ bool build_bvh(const float* xyz, int64_t nf, HostBvh& out, std::string& err, int
             } else {
                 nd.meta[j] = (uint8_t)(0x80 | slot);
                 ++slot;
-                queue.push_back({ch[j], it.level + 1});
+                queue.push_back({k.ch[j], it.level + 1});
                 out.nodes.emplace_back();
                 max_depth = std::max(max_depth, it.level + 1);
             }
         }
         nd.n_internal = (uint8_t)slot;
         out.nodes[qi] = nd;
+        kids.push_back(k);
     }
-    // triangle records in soup order; the vertex reads follow the leaves, not
-    // the input order, so they are prefetched a few slots ahead
-    out.tris.resize((size_t)n_soup);
-    constexpr int64_t kAhead = 16;
-    for (int64_t t = 0; t < n_soup; ++t) {
-        if (t + kAhead < n_soup) {
-            const float* q = xyz + 9 * (int64_t)soup[(size_t)(t + kAhead)];
-            __builtin_prefetch(q);
-            __builtin_prefetch(q + 8);
+    // every node's frame and quantised child boxes depend on its own boxes
+    // only: nodes in parallel
+    parallel_for((int64_t)queue.size(), threads, 2048, [&](int64_t lo, int64_t hi) {
+        for (int64_t qi = lo; qi < hi; ++qi) {
+            CNode& nd = out.nodes[(size_t)qi];
+            set_frame(nd, nodes[queue[(size_t)qi].bin].box);
+            const Kids& k = kids[(size_t)qi];
+            for (int j = 0; j < k.n; ++j) quantise_child(nd, j, nodes[k.ch[j]].box, nd);
         }
-        const int f = soup[(size_t)t];
-        const float* p = xyz + 9 * (int64_t)f;
-        CTri tr;
-        tr.ax = p[0]; tr.ay = p[1]; tr.az = p[2]; tr.id = f;
-        tr.bx = p[3]; tr.by = p[4]; tr.bz = p[5];
-        tr.cx = p[6]; tr.cy = p[7]; tr.cz = p[8];
-        set_error_scales(tr);
-        if (f == 0) out.slot_of_face0 = t;
-        out.tris[(size_t)t] = tr;
-    }
+    });
+    // triangle records in soup order, slots in parallel; the vertex reads
+    // follow the leaves, not the input order, so they are prefetched ahead
+    out.tris.resize((size_t)n_soup);
+    parallel_for(n_soup, threads, 16384, [&](int64_t lo, int64_t hi) {
+        constexpr int64_t kAhead = 16;
+        for (int64_t t = lo; t < hi; ++t) {
+            if (t + kAhead < hi) {
+                const float* q = xyz + 9 * (int64_t)soup[(size_t)(t + kAhead)];
+                __builtin_prefetch(q);
+                __builtin_prefetch(q + 8);
+            }
+            const int f = soup[(size_t)t];
+            const float* p = xyz + 9 * (int64_t)f;
+            CTri tr;
+            tr.ax = p[0]; tr.ay = p[1]; tr.az = p[2]; tr.id = f;
+            tr.bx = p[3]; tr.by = p[4]; tr.bz = p[5];
+            tr.cx = p[6]; tr.cy = p[7]; tr.cz = p[8];
+            set_error_scales(tr);
+            if (f == 0) out.slot_of_face0 = t;  // one slot holds face 0: one writer
+            out.tris[(size_t)t] = tr;
+        }
+    });
     out.depth = max_depth;
     out.level_start.assign(1, 0);
     for (size_t qi = 1; qi < queue.size(); ++qi)
