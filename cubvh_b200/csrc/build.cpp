@@ -11,6 +11,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <immintrin.h>
 #include <functional>
 #include <limits>
 #include <numeric>
@@ -37,6 +38,30 @@ struct Box {
     }
 };
 
+// The same box in SSE registers (lane 3 unused).  Every operation gives the
+// bits Box's gives: std::min(a, b) is (b < a ? b : a), which is
+// _mm_min_ps(b, a), and std::max(a, b) is (a < b ? b : a), _mm_max_ps(b, a);
+// the area is computed from the lanes with Box::area's expression.
+struct Box4 {
+    __m128 lo = _mm_set1_ps(INFINITY), hi = _mm_set1_ps(-INFINITY);
+    void grow(const Box4& b) { lo = _mm_min_ps(b.lo, lo); hi = _mm_max_ps(b.hi, hi); }
+    void grow_point(__m128 p) { lo = _mm_min_ps(p, lo); hi = _mm_max_ps(p, hi); }
+    Box box() const {
+        alignas(16) float l[4], h[4];
+        _mm_store_ps(l, lo); _mm_store_ps(h, hi);
+        Box r;
+        for (int k = 0; k < 3; ++k) { r.lo[k] = l[k]; r.hi[k] = h[k]; }
+        return r;
+    }
+    float area() const {  // Box::area on the lanes: the same rounded hi - lo
+        alignas(16) float d[4];
+        _mm_store_ps(d, _mm_sub_ps(hi, lo));
+        const float dx = d[0], dy = d[1], dz = d[2];
+        if (!(dx >= 0.f)) return 0.f;
+        return 2.f * (dx * dy + dy * dz + dz * dx);
+    }
+};
+
 struct Node2 {
     Box box;
     int left = -1, right = -1;     // internal children
@@ -46,8 +71,8 @@ struct Node2 {
 // One triangle's box, centroid and face index: the builder keeps these
 // records in the order it partitions them, so every pass over a range reads
 // memory sequentially.
-struct Prim {
-    Box box;
+struct alignas(16) Prim {
+    Box4 box;
     float c[3];
     int id;
 };
@@ -83,8 +108,12 @@ struct Builder {
     // returned index is the subtree's root.  The tree depends only on the
     // range's contents, not on which thread or vector builds it.
     int build(int b, int e, std::vector<Node2>& nodes) {
-        Box box, cb;
-        for (int i = b; i < e; ++i) { box.grow(prim[i].box); cb.grow(prim[i].c); }
+        Box4 box4, cb4;
+        for (int i = b; i < e; ++i) {
+            box4.grow(prim[i].box);
+            cb4.grow_point(_mm_loadu_ps(prim[i].c));  // lane 3 reads id: unused
+        }
+        const Box box = box4.box(), cb = cb4.box();
         const int n = e - b;
         if (n == 1) return make_leaf(nodes, b, e, box);
 
@@ -100,32 +129,40 @@ struct Builder {
             act[ax] = ext > 0.f;
             kk[ax] = act[ax] ? (float)kBins * (1.f - 1e-6f) / ext : 0.f;
         }
-        Box bb[3][kBins];  // valid where bc > 0
+        Box4 bb[3][kBins];
         int bc[3][kBins] = {};
+        uint32_t used[3] = {0u, 0u, 0u};  // bit i: bin i of the axis is non-empty
+        // bin indices of the three axes at once: per lane the same rounded
+        // subtract and multiply and the same truncation as bin_of
+        const __m128 lo4 = _mm_setr_ps(cb.lo[0], cb.lo[1], cb.lo[2], 0.f);
+        const __m128 k4 = _mm_setr_ps(kk[0], kk[1], kk[2], 0.f);
         for (int i = b; i < e; ++i) {
             const Prim& p = prim[i];
+            alignas(16) int32_t q[4];
+            _mm_store_si128(reinterpret_cast<__m128i*>(q),
+                            _mm_cvttps_epi32(_mm_mul_ps(_mm_sub_ps(_mm_loadu_ps(p.c), lo4), k4)));
             for (int ax = 0; ax < 3; ++ax) {
                 if (!act[ax]) continue;
-                const int bi = bin_of(p.c[ax], cb.lo[ax], kk[ax]);
-                if (bc[ax][bi]++ == 0) bb[ax][bi] = p.box;
-                else bb[ax][bi].grow(p.box);
+                const int bi = std::min(std::max(q[ax], 0), kBins - 1);
+                bc[ax][bi]++;
+                used[ax] |= 1u << bi;
+                bb[ax][bi].grow(p.box);
             }
         }
         float best_cost = INFINITY; int best_axis = -1, best_split = -1;
         for (int ax = 0; ax < 3; ++ax) {
             if (!act[ax]) continue;
             int ne[kBins], nb = 0;
-            for (int i = 0; i < kBins; ++i)
-                if (bc[ax][i]) ne[nb++] = i;
+            for (uint32_t m = used[ax]; m; m &= m - 1) ne[nb++] = __builtin_ctz(m);
             if (nb < 2) continue;
             float ra[kBins]; int rc[kBins];  // suffix area / count from non-empty bin j up
-            Box acc = bb[ax][ne[nb - 1]]; int cnt = bc[ax][ne[nb - 1]];
+            Box4 acc = bb[ax][ne[nb - 1]]; int cnt = bc[ax][ne[nb - 1]];
             for (int j = nb - 2; j >= 1; --j) {
                 acc.grow(bb[ax][ne[j]]); cnt += bc[ax][ne[j]];
                 ra[j] = acc.area(); rc[j] = cnt;
             }
             ra[nb - 1] = bb[ax][ne[nb - 1]].area(); rc[nb - 1] = bc[ax][ne[nb - 1]];
-            acc = Box(); cnt = 0;
+            acc = Box4(); cnt = 0;
             for (int j = 0; j < nb - 1; ++j) {
                 acc.grow(bb[ax][ne[j]]); cnt += bc[ax][ne[j]];
                 const float c = acc.area() * cnt + ra[j + 1] * rc[j + 1];
@@ -297,7 +334,8 @@ bool build_bvh(const float* xyz, int64_t nf, HostBvh& out, std::string& err, int
     for (int64_t f = 0; f < nf; ++f) {
         Prim& p = B.prim[f];
         Box b; b.grow(xyz + 9 * f); b.grow(xyz + 9 * f + 3); b.grow(xyz + 9 * f + 6);
-        p.box = b;
+        p.box.lo = _mm_setr_ps(b.lo[0], b.lo[1], b.lo[2], 0.f);
+        p.box.hi = _mm_setr_ps(b.hi[0], b.hi[1], b.hi[2], 0.f);
         for (int k = 0; k < 3; ++k) p.c[k] = 0.5f * (b.lo[k] + b.hi[k]);
         p.id = (int)f;
     }
