@@ -5,6 +5,13 @@
 // (src/bvh.cu:515-620) and stores 36-byte nodes; this builder targets the
 // 80-byte compressed node instead.  export_reference_format() writes the
 // reference's own record format for state_dict compatibility.
+//
+// The binary tree is built by recursion over triangle ranges; large ranges
+// hand their left half to another thread, and the breadth-first collapse
+// fills node boxes and triangle records in parallel.  The output does not
+// depend on the thread count.  Box arithmetic uses SSE (part of the x86-64
+// base instruction set) in the operand order that reproduces std::min /
+// std::max bit for bit.
 #include "build.h"
 
 #include <algorithm>
