@@ -17,9 +17,11 @@
 #include <algorithm>
 #include <atomic>
 #include <cstring>
+#include <memory>
 #include <numeric>
 #include <mutex>
 #include <string>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -34,13 +36,26 @@ int set_error(int code, const std::string& msg);
 }
 using namespace cubvh;
 
+// std::allocator whose resize leaves trivially constructible elements
+// uninitialised, so the threads that fill a vector are the first to touch
+// its pages (first touch of fresh memory costs more than the copy itself)
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+    NoInitAlloc() = default;
+    template <class U> NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
+    template <class U> struct rebind { using other = NoInitAlloc<U>; };
+    template <class U> void construct(U* p) noexcept { ::new ((void*)p) U; }
+    template <class U, class... A> void construct(U* p, A&&... a) { ::new ((void*)p) U(std::forward<A>(a)...); }
+};
+template <class T> using RawVec = std::vector<T, NoInitAlloc<T>>;
+
 struct cubvh_arena {
     int32_t M = 0;
-    std::vector<CNode> nodes;
-    std::vector<CTri> tris;
+    RawVec<CNode> nodes;
+    RawVec<CTri> tris;
     std::vector<int32_t> root, slot0;
     std::vector<int64_t> face_off;   // [M + 1]
-    std::vector<int32_t> gslot;      // [total faces] soup slot of (mesh, face)
+    RawVec<int32_t> gslot;           // [total faces] soup slot of (mesh, face)
     std::vector<float> box;          // [M][6]
     int64_t n_nodes = 0, n_tris = 0;
     std::mutex mu;
@@ -62,6 +77,24 @@ int cuda_err(cudaError_t e, const char* what) {
     return set_error(CUBVH_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// fn() on up to n threads, the caller's included; fn takes its own work from
+// a shared counter and must not throw.  Threads that cannot be started are
+// not used, and every started thread is joined before returning.
+template <class F>
+void run_workers(int n, F fn) {
+    std::vector<std::thread> pool;
+    pool.reserve((size_t)std::max(0, n - 1));
+    for (int t = 1; t < n; ++t) {
+        try {
+            pool.emplace_back(fn);
+        } catch (const std::system_error&) {
+            break;
+        }
+    }
+    fn();
+    for (auto& th : pool) th.join();
+}
 
 int arena_device(cubvh_arena* a) {
     int dev = 0;
@@ -119,76 +152,103 @@ int cubvh_arena_create(int32_t n_meshes, const float* const* vertices, const int
     if (n_meshes <= 0 || !vertices || !n_vertices || !faces || !n_faces)
         return set_error(CUBVH_ERR_INVALID, "arena needs at least one mesh and non-null arrays");
     const int M = n_meshes;
-    std::vector<HostBvh> hb(M);
-    std::vector<std::string> errs(M);
-    std::vector<std::vector<float>> xyz(M);
     for (int m = 0; m < M; ++m) {
         if (!vertices[m] || !faces[m] || n_vertices[m] <= 0 || n_faces[m] <= 0)
             return set_error(CUBVH_ERR_INVALID, "mesh " + std::to_string(m) + " is empty or null");
         const int leaf = max_leaf ? max_leaf[m] : kMaxLeafTris;
         if (leaf < 1 || leaf > kMaxLeafTris)
             return set_error(CUBVH_ERR_INVALID, "mesh " + std::to_string(m) + ": leaf size must be in [1, 4]");
-        xyz[m].resize((size_t)n_faces[m] * 9);
-        for (int64_t f = 0; f < n_faces[m]; ++f)
-            for (int k = 0; k < 3; ++k) {
-                const int64_t v = faces[m][3 * f + k];
-                if (v < 0 || v >= n_vertices[m])
-                    return set_error(CUBVH_ERR_INVALID, "mesh " + std::to_string(m) + " face " + std::to_string(f) +
-                                                            " has a vertex index out of range");
-                std::memcpy(&xyz[m][(size_t)f * 9 + 3 * k], vertices[m] + 3 * v, 3 * sizeof(float));
-            }
     }
-    // build every mesh, in parallel: one thread per mesh at a time (each
-    // build single-threaded), largest meshes first from a shared queue so the
-    // last builds to finish are small ones
+    // gather and build every mesh, in parallel: one thread per mesh at a
+    // time (each build single-threaded), largest meshes first from a shared
+    // queue so the last builds to finish are small ones.  Errors are reported
+    // as a serial pass would: a bad vertex index (lowest mesh, first face)
+    // before any build error (lowest mesh); once an index error is known,
+    // the remaining meshes are still checked but not built.
+    std::vector<HostBvh> hb(M);
+    std::vector<std::string> index_err(M), build_err(M);
+    std::atomic<bool> any_index_err{false};
     const int nthr = std::max(1, std::min<int>(M, (int)std::thread::hardware_concurrency()));
     std::vector<int> order(M);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return n_faces[a] > n_faces[b]; });
     std::atomic<int> next{0};
-    std::vector<std::thread> pool;
-    for (int t = 0; t < nthr; ++t)
-        pool.emplace_back([&] {
-            for (int i; (i = next.fetch_add(1)) < M;) {
-                const int m = order[i];
-                const int leaf = max_leaf ? max_leaf[m] : kMaxLeafTris;
-                try {  // an exception must not leave the worker thread
-                    if (!build_bvh(xyz[m].data(), n_faces[m], hb[m], errs[m], leaf, 1) && errs[m].empty())
-                        errs[m] = "build failed";
-                } catch (const std::bad_alloc&) {
-                    errs[m] = "host allocation failed";
-                } catch (const std::exception& ex) {
-                    errs[m] = ex.what();
+    run_workers(nthr, [&] {
+        for (int i; (i = next.fetch_add(1)) < M;) {
+            const int m = order[i];
+            try {  // an exception must not leave the worker thread
+                std::vector<float> xyz((size_t)n_faces[m] * 9);
+                int64_t bad = -1;
+                for (int64_t f = 0; f < n_faces[m] && bad < 0; ++f)
+                    for (int k = 0; k < 3; ++k) {
+                        const int64_t v = faces[m][3 * f + k];
+                        if (v < 0 || v >= n_vertices[m]) { bad = f; break; }
+                        std::memcpy(&xyz[(size_t)f * 9 + 3 * k], vertices[m] + 3 * v, 3 * sizeof(float));
+                    }
+                if (bad >= 0) {
+                    index_err[m] = "mesh " + std::to_string(m) + " face " + std::to_string(bad) +
+                                   " has a vertex index out of range";
+                    any_index_err = true;
+                    continue;
                 }
+                if (any_index_err) continue;
+                const int leaf = max_leaf ? max_leaf[m] : kMaxLeafTris;
+                std::string err;
+                if (!build_bvh(xyz.data(), n_faces[m], hb[m], err, leaf, 1))
+                    build_err[m] = "mesh " + std::to_string(m) + ": " + (err.empty() ? "build failed" : err);
+            } catch (const std::bad_alloc&) {
+                build_err[m] = "mesh " + std::to_string(m) + ": host allocation failed";
+            } catch (const std::exception& ex) {
+                build_err[m] = "mesh " + std::to_string(m) + ": " + ex.what();
             }
-        });
-    for (auto& th : pool) th.join();
+        }
+    });
     for (int m = 0; m < M; ++m)
-        if (!errs[m].empty()) return set_error(CUBVH_ERR_INVALID, "mesh " + std::to_string(m) + ": " + errs[m]);
-    auto* a = new cubvh_arena();
+        if (!index_err[m].empty()) return set_error(CUBVH_ERR_INVALID, index_err[m]);
+    for (int m = 0; m < M; ++m)
+        if (!build_err[m].empty()) return set_error(CUBVH_ERR_INVALID, build_err[m]);
+    std::unique_ptr<cubvh_arena> a(new cubvh_arena());  // released to the caller on success
     a->M = M;
     a->root.resize(M); a->slot0.resize(M); a->face_off.assign(M + 1, 0); a->box.resize((size_t)M * 6);
     size_t nn = 0, nt = 0;
     for (int m = 0; m < M; ++m) { nn += hb[m].nodes.size(); nt += hb[m].tris.size(); }
-    if (nn >= (size_t)INT32_MAX || nt >= (size_t)(1u << 28)) {
-        delete a;
+    if (nn >= (size_t)INT32_MAX || nt >= (size_t)(1u << 28))
         return set_error(CUBVH_ERR_INVALID, "arena too large (2^31 nodes / 2^28 triangles)");
-    }
-    a->nodes.reserve(nn); a->tris.reserve(nt); a->gslot.assign(nt, -1);
+    // offsets of every mesh in the concatenated arrays, then each mesh's
+    // rebased nodes, triangles and face -> slot map written in parallel into
+    // its own ranges (every face of a mesh is in its soup, so every gslot
+    // entry is written)
+    std::vector<size_t> node_off(M + 1, 0), tri_off(M + 1, 0);
     for (int m = 0; m < M; ++m) {
-        const int32_t no = (int32_t)a->nodes.size(), to = (int32_t)a->tris.size();
-        for (CNode nd : hb[m].nodes) { nd.child_base += no; nd.tri_base += to; a->nodes.push_back(nd); }
-        for (const CTri& t : hb[m].tris) a->tris.push_back(t);
-        a->root[m] = no;
-        a->slot0[m] = to + (int32_t)hb[m].slot_of_face0;
+        node_off[m + 1] = node_off[m] + hb[m].nodes.size();
+        tri_off[m + 1] = tri_off[m] + hb[m].tris.size();
         a->face_off[m + 1] = a->face_off[m] + n_faces[m];
-        for (size_t s = 0; s < hb[m].tris.size(); ++s)
-            a->gslot[(size_t)a->face_off[m] + (size_t)hb[m].tris[s].id] = to + (int32_t)s;
+        a->root[m] = (int32_t)node_off[m];
+        a->slot0[m] = (int32_t)tri_off[m] + (int32_t)hb[m].slot_of_face0;
         for (int k = 0; k < 3; ++k) { a->box[6 * m + k] = hb[m].lo[k]; a->box[6 * m + 3 + k] = hb[m].hi[k]; }
     }
+    a->nodes.resize(nn); a->tris.resize(nt); a->gslot.resize(nt);
+    next = 0;
+    run_workers(nthr, [&] {
+            for (int i; (i = next.fetch_add(1)) < M;) {
+                const int m = order[i];
+                const int32_t no = (int32_t)node_off[m], to = (int32_t)tri_off[m];
+                CNode* dn = a->nodes.data() + node_off[m];
+                for (const CNode& src : hb[m].nodes) {
+                    CNode nd = src;
+                    nd.child_base += no; nd.tri_base += to;
+                    *dn++ = nd;
+                }
+                std::memcpy(a->tris.data() + tri_off[m], hb[m].tris.data(), hb[m].tris.size() * sizeof(CTri));
+                int32_t* gs = a->gslot.data() + a->face_off[m];
+                for (size_t s = 0; s < hb[m].tris.size(); ++s) gs[hb[m].tris[s].id] = to + (int32_t)s;
+                HostBvh().nodes.swap(hb[m].nodes);  // release the per-mesh copy early
+                HostBvh().tris.swap(hb[m].tris);
+            }
+        });
     a->n_nodes = (int64_t)a->nodes.size();
     a->n_tris = (int64_t)a->tris.size();
-    *out = a;
+    *out = a.release();
     return CUBVH_OK;
     ARENA_GUARD_END
 }
