@@ -36,19 +36,7 @@ int set_error(int code, const std::string& msg);
 }
 using namespace cubvh;
 
-// std::allocator whose resize leaves trivially constructible elements
-// uninitialised, so the threads that fill a vector are the first to touch
-// its pages (first touch of fresh memory costs more than the copy itself)
-template <class T>
-struct NoInitAlloc : std::allocator<T> {
-    NoInitAlloc() = default;
-    template <class U> NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
-    template <class U> struct rebind { using other = NoInitAlloc<U>; };
-    template <class U> void construct(U* p) noexcept { ::new ((void*)p) U; }
-    template <class U, class... A> void construct(U* p, A&&... a) { ::new ((void*)p) U(std::forward<A>(a)...); }
-};
-template <class T> using RawVec = std::vector<T, NoInitAlloc<T>>;
-
+// host arrays are RawVec (build.h): filled in parallel after sizing
 struct cubvh_arena {
     int32_t M = 0;
     RawVec<CNode> nodes;

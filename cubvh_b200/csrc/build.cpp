@@ -50,7 +50,8 @@ struct Box {
 // _mm_min_ps(b, a), and std::max(a, b) is (a < b ? b : a), _mm_max_ps(b, a);
 // the area is computed from the lanes with Box::area's expression.
 struct Box4 {
-    __m128 lo = _mm_set1_ps(INFINITY), hi = _mm_set1_ps(-INFINITY);
+    __m128 lo, hi;  // no initialiser, so arrays of records stay trivial: see empty()
+    static Box4 empty() { return Box4{_mm_set1_ps(INFINITY), _mm_set1_ps(-INFINITY)}; }
     void grow(const Box4& b) { lo = _mm_min_ps(b.lo, lo); hi = _mm_max_ps(b.hi, hi); }
     void grow_point(__m128 p) { lo = _mm_min_ps(p, lo); hi = _mm_max_ps(p, hi); }
     Box box() const {
@@ -85,7 +86,7 @@ struct alignas(16) Prim {
 };
 
 struct Builder {
-    std::vector<Prim> prim;
+    RawVec<Prim> prim;
 
     static constexpr int kBins = 32;
     static constexpr float kTrav = 1.0f, kIsect = 1.0f;
@@ -115,7 +116,7 @@ struct Builder {
     // returned index is the subtree's root.  The tree depends only on the
     // range's contents, not on which thread or vector builds it.
     int build(int b, int e, std::vector<Node2>& nodes) {
-        Box4 box4, cb4;
+        Box4 box4 = Box4::empty(), cb4 = Box4::empty();
         for (int i = b; i < e; ++i) {
             box4.grow(prim[i].box);
             cb4.grow_point(_mm_loadu_ps(prim[i].c));  // lane 3 reads id: unused
@@ -137,6 +138,8 @@ struct Builder {
             kk[ax] = act[ax] ? (float)kBins * (1.f - 1e-6f) / ext : 0.f;
         }
         Box4 bb[3][kBins];
+        for (auto& row : bb)
+            for (Box4& x : row) x = Box4::empty();
         int bc[3][kBins] = {};
         uint32_t used[3] = {0u, 0u, 0u};  // bit i: bin i of the axis is non-empty
         // bin indices of the three axes at once: per lane the same rounded
@@ -169,7 +172,7 @@ struct Builder {
                 ra[j] = acc.area(); rc[j] = cnt;
             }
             ra[nb - 1] = bb[ax][ne[nb - 1]].area(); rc[nb - 1] = bc[ax][ne[nb - 1]];
-            acc = Box4(); cnt = 0;
+            acc = Box4::empty(); cnt = 0;
             for (int j = 0; j < nb - 1; ++j) {
                 acc.grow(bb[ax][ne[j]]); cnt += bc[ax][ne[j]];
                 const float c = acc.area() * cnt + ra[j + 1] * rc[j + 1];
@@ -329,23 +332,29 @@ void parallel_for(int64_t n, int threads, int64_t grain, F fn) {
 bool build_bvh(const float* xyz, int64_t nf, HostBvh& out, std::string& err, int max_leaf, int threads) {
     if (nf <= 0) { err = "mesh has no faces"; return false; }
     if (nf > (int64_t)(1 << 28)) { err = "too many faces (limit 2^28)"; return false; }
-    for (int64_t i = 0; i < nf * 9; ++i)
-        if (!std::isfinite(xyz[i])) { err = "vertex coordinates must be finite"; return false; }
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    std::atomic<bool> finite{true};
+    parallel_for(nf, threads, 65536, [&](int64_t lo, int64_t hi) {
+        for (int64_t i = 9 * lo; i < 9 * hi; ++i)
+            if (!std::isfinite(xyz[i])) { finite = false; return; }
+    });
+    if (!finite) { err = "vertex coordinates must be finite"; return false; }
 
     if (max_leaf < 1 || max_leaf > kMaxLeafTris) { err = "leaf size must be in [1, 4]"; return false; }
     Builder B;
     B.max_leaf = max_leaf;
-    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
     B.spare = threads - 1;
-    B.prim.resize(nf);
-    for (int64_t f = 0; f < nf; ++f) {
-        Prim& p = B.prim[f];
-        Box b; b.grow(xyz + 9 * f); b.grow(xyz + 9 * f + 3); b.grow(xyz + 9 * f + 6);
-        p.box.lo = _mm_setr_ps(b.lo[0], b.lo[1], b.lo[2], 0.f);
-        p.box.hi = _mm_setr_ps(b.hi[0], b.hi[1], b.hi[2], 0.f);
-        for (int k = 0; k < 3; ++k) p.c[k] = 0.5f * (b.lo[k] + b.hi[k]);
-        p.id = (int)f;
-    }
+    B.prim.resize(nf);  // uninitialised: filled (first touched) in parallel
+    parallel_for(nf, threads, 65536, [&](int64_t lo, int64_t hi) {
+        for (int64_t f = lo; f < hi; ++f) {
+            Prim& p = B.prim[f];
+            Box b; b.grow(xyz + 9 * f); b.grow(xyz + 9 * f + 3); b.grow(xyz + 9 * f + 6);
+            p.box.lo = _mm_setr_ps(b.lo[0], b.lo[1], b.lo[2], 0.f);
+            p.box.hi = _mm_setr_ps(b.hi[0], b.hi[1], b.hi[2], 0.f);
+            for (int k = 0; k < 3; ++k) p.c[k] = 0.5f * (b.lo[k] + b.hi[k]);
+            p.id = (int)f;
+        }
+    });
     std::vector<Node2> nodes;
     nodes.reserve(2 * nf);
     const int root = B.build(0, (int)nf, nodes);

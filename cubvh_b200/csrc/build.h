@@ -1,16 +1,31 @@
 // Host-side BVH construction and the reference's state_dict format.
 #pragma once
 #include <cstdint>
+#include <memory>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "layout.h"
 
 namespace cubvh {
 
+// std::allocator whose resize leaves trivially constructible elements
+// uninitialised, so the threads that fill a large array are the first to
+// touch its pages (first touch of fresh memory costs more than the writes)
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+    NoInitAlloc() = default;
+    template <class U> NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
+    template <class U> struct rebind { using other = NoInitAlloc<U>; };
+    template <class U> void construct(U* p) noexcept { ::new ((void*)p) U; }
+    template <class U, class... A> void construct(U* p, A&&... a) { ::new ((void*)p) U(std::forward<A>(a)...); }
+};
+template <class T> using RawVec = std::vector<T, NoInitAlloc<T>>;
+
 struct HostBvh {
-    std::vector<CNode> nodes;      // node 0 is the root
-    std::vector<CTri> tris;        // leaf-ordered soup
+    RawVec<CNode> nodes;           // node 0 is the root
+    RawVec<CTri> tris;             // leaf-ordered soup
     int depth = 0;                 // internal levels (root = 1)
     // nodes are stored breadth first: level l (root = 0) is the index range
     // [level_start[l], level_start[l + 1])
