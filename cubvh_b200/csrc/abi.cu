@@ -3,12 +3,17 @@
 // turns them into a status code plus a per-thread message.
 #include <cuda_runtime.h>
 
+#include <atomic>
+#include <climits>
+#include <cstdint>
 #include <cstring>
 #include <exception>
 #include <deque>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/cubvh_b200.h"
@@ -52,8 +57,8 @@ struct DevCopy {
 
 struct cubvh_bvh {
     HostBvh host;
-    std::vector<float> xyz;       // [F, 9] a, b, c of each face, face order
-    std::vector<int64_t> ids;     // face id of each face (position for meshes)
+    RawVec<float> xyz;            // [F, 9] a, b, c of each face, face order
+    RawVec<int64_t> ids;          // face id of each face (position for meshes)
     std::mutex mu;
     std::deque<DevCopy> dev;      // stable addresses across push_back
 };
@@ -82,6 +87,7 @@ int fail(int code, const std::string& msg) {
 int cuda_fail(cudaError_t e, const char* what) {
     return fail(CUBVH_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
+int host_threads() { return (int)std::max(1u, std::thread::hardware_concurrency()); }
 
 
 // Device copy of the BVH on the current device (uploaded on first use).
@@ -186,11 +192,16 @@ int finish_build(cubvh_bvh* h) {
     std::string err;
     if (!build_bvh(h->xyz.data(), (int64_t)h->ids.size(), h->host, err)) return fail(CUBVH_ERR_INVALID, err);
     // triangle ids: stored face ids (int32 in the node layout)
-    for (auto& t : h->host.tris) {
-        const int64_t id = h->ids[(size_t)t.id];
-        if (id < INT32_MIN || id > INT32_MAX) return fail(CUBVH_ERR_INVALID, "face id does not fit in int32");
-        t.id = (int32_t)id;
-    }
+    std::atomic<bool> fits{true};
+    parallel_for((int64_t)h->host.tris.size(), host_threads(), 65536, [&](int64_t lo, int64_t hi) {
+        for (int64_t s = lo; s < hi; ++s) {
+            CTri& t = h->host.tris[(size_t)s];
+            const int64_t id = h->ids[(size_t)t.id];
+            if (id < INT32_MIN || id > INT32_MAX) { fits = false; return; }
+            t.id = (int32_t)id;
+        }
+    });
+    if (!fits) return fail(CUBVH_ERR_INVALID, "face id does not fit in int32");
     return CUBVH_OK;
 }
 
@@ -230,27 +241,42 @@ int cubvh_bvh_create(const float* vertices, int64_t n_vertices, const int64_t* f
     *out = nullptr;
     if (!vertices || !faces) return fail(CUBVH_ERR_INVALID, "vertices/faces is null");
     if (n_vertices <= 0 || n_faces <= 0) return fail(CUBVH_ERR_INVALID, "empty mesh");
-    auto* h = new cubvh_bvh();
-    h->xyz.resize((size_t)n_faces * 9);
+    std::unique_ptr<cubvh_bvh> h(new cubvh_bvh());
+    h->xyz.resize((size_t)n_faces * 9);  // uninitialised: filled in parallel
     h->ids.resize((size_t)n_faces);
     h->host.faces.resize((size_t)n_faces * 3);
     h->host.n_vertices = n_vertices;
-    for (int64_t f = 0; f < n_faces; ++f) {
-        for (int k = 0; k < 3; ++k) {
-            const int64_t v = faces[3 * f + k];
-            if (v < 0 || v >= n_vertices) {
-                delete h;
-                return fail(CUBVH_ERR_INVALID, "face " + std::to_string(f) + " has vertex index " +
-                                                   std::to_string(v) + " outside [0, " + std::to_string(n_vertices) + ")");
+    // faces in parallel; a range stops at its first bad face, so the lowest
+    // of those is the first bad face of the mesh, the one reported
+    std::atomic<int64_t> first_bad{INT64_MAX};
+    parallel_for(n_faces, host_threads(), 65536, [&](int64_t lo, int64_t hi) {
+        for (int64_t f = lo; f < hi; ++f) {
+            for (int k = 0; k < 3; ++k) {
+                const int64_t v = faces[3 * f + k];
+                if (v < 0 || v >= n_vertices) {
+                    int64_t cur = first_bad.load();
+                    while (f < cur && !first_bad.compare_exchange_weak(cur, f)) {}
+                    return;
+                }
+                std::memcpy(&h->xyz[(size_t)f * 9 + 3 * k], vertices + 3 * v, 3 * sizeof(float));
+                h->host.faces[(size_t)f * 3 + k] = (int32_t)v;
             }
-            std::memcpy(&h->xyz[(size_t)f * 9 + 3 * k], vertices + 3 * v, 3 * sizeof(float));
-            h->host.faces[(size_t)f * 3 + k] = (int32_t)v;
+            h->ids[(size_t)f] = f;
         }
-        h->ids[(size_t)f] = f;
+    });
+    if (first_bad.load() != INT64_MAX) {
+        const int64_t f = first_bad.load();
+        int64_t v = 0;
+        for (int k = 0; k < 3; ++k) {
+            v = faces[3 * f + k];
+            if (v < 0 || v >= n_vertices) break;
+        }
+        return fail(CUBVH_ERR_INVALID, "face " + std::to_string(f) + " has vertex index " + std::to_string(v) +
+                                           " outside [0, " + std::to_string(n_vertices) + ")");
     }
-    const int rc = finish_build(h);
-    if (rc != CUBVH_OK) { delete h; return rc; }
-    *out = h;
+    const int rc = finish_build(h.get());
+    if (rc != CUBVH_OK) return rc;
+    *out = h.release();
     return CUBVH_OK;
     CUBVH_GUARD_END
 }

@@ -304,29 +304,6 @@ Box tri_box(const CTri& t) {
     return b;
 }
 
-// fn(lo, hi) over [0, n) split into contiguous ranges of at least `grain`
-// items on up to `threads` threads (the caller's thread takes the first
-// range; a range whose thread cannot be started runs on the caller's thread).
-// fn must not throw.
-template <class F>
-void parallel_for(int64_t n, int threads, int64_t grain, F fn) {
-    const int64_t parts = std::max<int64_t>(1, std::min<int64_t>(threads, (n + grain - 1) / grain));
-    if (parts <= 1) { fn(0, n); return; }
-    std::vector<std::thread> pool;
-    std::vector<int64_t> inline_parts;
-    for (int64_t i = 1; i < parts; ++i) {
-        const int64_t lo = n * i / parts, hi = n * (i + 1) / parts;
-        try {
-            pool.emplace_back([=, &fn] { fn(lo, hi); });
-        } catch (const std::system_error&) {
-            inline_parts.push_back(i);
-        }
-    }
-    fn(0, n / parts);
-    for (int64_t i : inline_parts) fn(n * i / parts, n * (i + 1) / parts);
-    for (auto& t : pool) t.join();
-}
-
 }  // namespace
 
 bool build_bvh(const float* xyz, int64_t nf, HostBvh& out, std::string& err, int max_leaf, int threads) {

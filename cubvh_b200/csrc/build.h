@@ -1,8 +1,11 @@
 // Host-side BVH construction and the reference's state_dict format.
 #pragma once
+#include <algorithm>
 #include <cstdint>
 #include <memory>
 #include <string>
+#include <system_error>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -23,6 +26,29 @@ struct NoInitAlloc : std::allocator<T> {
 };
 template <class T> using RawVec = std::vector<T, NoInitAlloc<T>>;
 
+// fn(lo, hi) over [0, n) split into contiguous ranges of at least `grain`
+// items on up to `threads` threads (the caller's thread takes the first
+// range; a range whose thread cannot be started runs on the caller's thread).
+// fn must not throw.
+template <class F>
+void parallel_for(int64_t n, int threads, int64_t grain, F fn) {
+    const int64_t parts = std::max<int64_t>(1, std::min<int64_t>(threads, (n + grain - 1) / grain));
+    if (parts <= 1) { fn(0, n); return; }
+    std::vector<std::thread> pool;
+    std::vector<int64_t> inline_parts;
+    for (int64_t i = 1; i < parts; ++i) {
+        const int64_t lo = n * i / parts, hi = n * (i + 1) / parts;
+        try {
+            pool.emplace_back([=, &fn] { fn(lo, hi); });
+        } catch (const std::system_error&) {
+            inline_parts.push_back(i);
+        }
+    }
+    fn(0, n / parts);
+    for (int64_t i : inline_parts) fn(n * i / parts, n * (i + 1) / parts);
+    for (auto& t : pool) t.join();
+}
+
 struct HostBvh {
     RawVec<CNode> nodes;           // node 0 is the root
     RawVec<CTri> tris;             // leaf-ordered soup
@@ -34,7 +60,7 @@ struct HostBvh {
     float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};  // scene bounds
     // face -> vertex indices, for refit / vertex gradients (empty when the
     // BVH was created from triangle records)
-    std::vector<int32_t> faces;    // [F, 3], original face order
+    RawVec<int32_t> faces;         // [F, 3], original face order
     int64_t n_vertices = 0;
 };
 
