@@ -245,3 +245,70 @@ def test_host_build_is_deterministic(mesh):
     for _ in range(2):
         nodes, tris, _ = layout(cubvh.cuBVH(v, f))
         assert hashlib.sha256(nodes.tobytes() + tris.tobytes()).hexdigest() == LAYOUT_SHA256[mesh]
+
+
+def test_c_abi_rejects_bad_arguments_before_any_device_work():
+    """Every entry point checks its arguments before it touches CUDA: on a
+    host without a GPU, bad arguments come back as status 1 with a message,
+    and empty work as status 0."""
+    L = _lib.lib()
+    P = ctypes.c_void_p
+    out = P()
+    v, f = W.icosphere(1)
+    bvh = cubvh.cuBVH(v, f)
+    h = bvh.impl.raw
+    V = np.ascontiguousarray(v, np.float32)
+
+    def bad(rc, needle=None):
+        assert rc == 1
+        msg = L.cubvh_last_error()
+        assert msg
+        if needle:
+            assert needle.encode() in msg, msg
+
+    bad(L.cubvh_bvh_create_device(None, 3, None, 1, 4, None, ctypes.byref(out)), "null")
+    bad(L.cubvh_bvh_create_device(V.ctypes.data, 0, V.ctypes.data, 1, 4, None, ctypes.byref(out)), "empty")
+    bad(L.cubvh_bvh_create_from_records(None, 5, ctypes.byref(out)), "null")
+    bad(L.cubvh_bvh_create_from_records(V.ctypes.data, 0, ctypes.byref(out)), "no triangle records")
+    bad(L.cubvh_bvh_info(None, None, None, None), "null")
+    bad(L.cubvh_bvh_state_dict(h, None, None), "null")
+    bad(L.cubvh_bvh_layout(h, None, None), "null")
+    bad(L.cubvh_bvh_upload(None), "null")
+    bad(L.cubvh_unsigned_distance(None, None, 5, None, None, None, None), "null")
+    bad(L.cubvh_ray_trace(h, None, None, -1, None, None, None, None), "negative")
+    assert L.cubvh_ray_trace(h, None, None, 0, None, None, None, None) == 0
+    bad(L.cubvh_ray_trace(h, None, None, 4, None, None, None, None), "null")
+    bad(L.cubvh_ray_trace_host(h, None, None, 4, None, None, None, None), "null")
+    bad(L.cubvh_signed_distance_host(h, None, 4, 5, None, None, None, None), "mode")
+    bad(L.cubvh_bvh_refit(h, None, len(V), None), "null")
+    bad(L.cubvh_bvh_refit(h, V.ctypes.data, len(V) + 1, None), "vertex count")
+    bad(L.cubvh_distance_backward(h, None, -2, None, None, None, None, None, None, None), "negative")
+    assert L.cubvh_distance_backward(h, None, 0, None, None, None, None, None, None, None) == 0
+    bad(L.cubvh_distance_backward(h, None, 3, None, None, None, None, None, None, None), "null")
+    bad(L.cubvh_floodfill_check(None, 1, 4, 4, 4, None), "null")
+    bad(L.cubvh_udf_to_sdf(None, 1, 4, 4, 4, 0.01, None, None, 0, None), "null")
+    assert L.cubvh_udf_to_sdf(None, 0, 4, 4, 4, 0.01, None, None, 0, None) == 0
+    bad(L.cubvh_floodfill_noalloc(None, 1, 4, 4, 4, None, None), "null")
+    bad(L.cubvh_floodfill(None, -1, 4, 4, 4, None, None, 0, None), "negative")
+
+    # arena: built on the host; its query calls refuse to run before a layout
+    F = np.ascontiguousarray(f, np.int64)
+    vp = (ctypes.c_void_p * 1)(V.ctypes.data)
+    fp = (ctypes.c_void_p * 1)(F.ctypes.data)
+    nv = (ctypes.c_int64 * 1)(len(V))
+    nf = (ctypes.c_int64 * 1)(len(F))
+    bad(L.cubvh_arena_create_device(0, vp, nv, fp, nf, None, None, ctypes.byref(out)), "at least one mesh")
+    a = P()
+    assert L.cubvh_arena_create(1, vp, nv, fp, nf, None, ctypes.byref(a)) == 0
+    try:
+        bad(L.cubvh_arena_distance(a, None, None, None, None, None), "set_queries")
+        bad(L.cubvh_arena_backward(a, None, None, None, None, None, None), "set_queries")
+        bad(L.cubvh_arena_set_queries(a, None, None), "null")
+        off = np.array([1, 5], np.int64)
+        md = np.array([0], np.uint32)
+        bad(L.cubvh_arena_set_queries(a, off.ctypes.data, md.ctypes.data), "query_offsets[0]")
+        off = np.array([0, 5], np.int64)
+        md = np.array([3], np.uint32)
+        bad(L.cubvh_arena_set_queries(a, off.ctypes.data, md.ctypes.data), "mode")
+    finally:
+        assert L.cubvh_arena_destroy(a) == 0
