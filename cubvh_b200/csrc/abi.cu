@@ -87,7 +87,7 @@ int fail(int code, const std::string& msg) {
 int cuda_fail(cudaError_t e, const char* what) {
     return fail(CUBVH_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
-int host_threads() { return (int)std::max(1u, std::thread::hardware_concurrency()); }
+int host_threads() { return host_build_threads(); }
 
 
 // Device copy of the BVH on the current device (uploaded on first use).
@@ -190,7 +190,8 @@ int near_lists(cubvh_bvh* h, DevCopy* d, cudaStream_t s, NearLists* out) {
 
 int finish_build(cubvh_bvh* h) {
     std::string err;
-    if (!build_bvh(h->xyz.data(), (int64_t)h->ids.size(), h->host, err)) return fail(CUBVH_ERR_INVALID, err);
+    if (!build_bvh(h->xyz.data(), (int64_t)h->ids.size(), h->host, err, kMaxLeafTris, host_threads()))
+        return fail(CUBVH_ERR_INVALID, err);
     // triangle ids: stored face ids (int32 in the node layout)
     std::atomic<bool> fits{true};
     parallel_for((int64_t)h->host.tris.size(), host_threads(), 65536, [&](int64_t lo, int64_t hi) {

@@ -156,7 +156,7 @@ int cubvh_arena_create(int32_t n_meshes, const float* const* vertices, const int
     std::vector<HostBvh> hb(M);
     std::vector<std::string> index_err(M), build_err(M);
     std::atomic<bool> any_index_err{false};
-    const int nthr = std::max(1, std::min<int>(M, (int)std::thread::hardware_concurrency()));
+    const int nthr = std::max(1, std::min<int>(M, host_build_threads()));
     std::vector<int> order(M);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return n_faces[a] > n_faces[b]; });

@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <immintrin.h>
 #include <functional>
@@ -306,10 +307,23 @@ Box tri_box(const CTri& t) {
 
 }  // namespace
 
+int host_build_threads() {
+    static const int n = [] {
+        const char* v = std::getenv("CUBVH_B200_BUILD_THREADS");
+        if (v) {
+            char* end = nullptr;
+            const long x = std::strtol(v, &end, 10);
+            if (end != v && *end == '\0' && x > 0) return (int)std::min<long>(x, 1 << 16);
+        }
+        return (int)std::max(1u, std::thread::hardware_concurrency());
+    }();
+    return n;
+}
+
 bool build_bvh(const float* xyz, int64_t nf, HostBvh& out, std::string& err, int max_leaf, int threads) {
     if (nf <= 0) { err = "mesh has no faces"; return false; }
     if (nf > (int64_t)(1 << 28)) { err = "too many faces (limit 2^28)"; return false; }
-    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    if (threads <= 0) threads = host_build_threads();
     std::atomic<bool> finite{true};
     parallel_for(nf, threads, 65536, [&](int64_t lo, int64_t hi) {
         for (int64_t i = 9 * lo; i < 9 * hi; ++i)

@@ -64,10 +64,14 @@ struct HostBvh {
     int64_t n_vertices = 0;
 };
 
+// Host threads a build may use: CUBVH_B200_BUILD_THREADS when set to a
+// positive integer (read once), otherwise every hardware thread.
+int host_build_threads();
+
 // Builds the wide BVH over triangles (a, b, c per face, original face index
 // = position).  tri_xyz: [F, 9] floats.  Returns false and sets err on bad input.
-// threads: host threads the build may use (0 = all cores); the tree is the
-// same for any count.
+// threads: host threads the build may use (0 = host_build_threads()); the
+// tree is the same for any count.
 bool build_bvh(const float* tri_xyz, int64_t n_faces, HostBvh& out, std::string& err,
                int max_leaf = kMaxLeafTris, int threads = 0);
 

@@ -312,3 +312,22 @@ def test_c_abi_rejects_bad_arguments_before_any_device_work():
         bad(L.cubvh_arena_set_queries(a, off.ctypes.data, md.ctypes.data), "mode")
     finally:
         assert L.cubvh_arena_destroy(a) == 0
+
+
+def test_build_threads_env_same_tree():
+    """CUBVH_B200_BUILD_THREADS caps the host build's threads (read once per
+    process); the tree is the same for any count."""
+    import subprocess
+    import sys
+    code = ("import sys, hashlib; sys.path.insert(0, 'tests')\n"
+            "import cubvh_b200 as cubvh\n"
+            "from cubvh_b200 import workloads as W\n"
+            "from test_host import layout\n"
+            "n, t, _ = layout(cubvh.cuBVH(*W.displaced_icosphere(6, 1)))\n"
+            "print(hashlib.sha256(n.tobytes() + t.tobytes()).hexdigest())\n")
+    for threads in ("1", "2"):
+        env = dict(os.environ, CUBVH_B200_BUILD_THREADS=threads)
+        r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env=env, capture_output=True, text=True,
+                           timeout=300)
+        assert r.returncode == 0, r.stderr
+        assert r.stdout.strip().splitlines()[-1] == LAYOUT_SHA256["ico6"]
