@@ -212,3 +212,31 @@ def test_fetch_on_another_stream(dev):
     finally:
         check(lib().cubvh_sparse_mc_free(res), "sparse_mc_free")
     assert torch.equal(got_v, want_v) and torch.equal(got_t, want_t)
+
+
+def _quantised_field(seed, n, levels):
+    rng = np.random.default_rng(seed)
+    field = rng.choice(levels, size=(n + 1, n + 1, n + 1)).astype(np.float32)
+    g = np.stack(np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij"), -1).reshape(-1, 3)
+    cp = g[:, None, :] + M.OFF[None]
+    return g.astype(np.int32), field[cp[..., 0], cp[..., 1], cp[..., 2]]
+
+
+@pytest.mark.parametrize("levels,iso", [((-1.0, 0.0, 1.0), 0.0), ((-1.0, 0.0, 1.0), 0.5), ((-1.0, 1.0), 0.0),
+                                        ((0.0, 1.0, 2.0, 3.0), 1.5)])
+def test_model_closed_on_quantised_lattices(oracle, levels, iso):
+    """Fields with exact ties (corners equal to iso, flat saddles): still
+    closed and consistently oriented inside the block, no triangle repeats a
+    vertex."""
+    for seed in range(8):
+        coords, corners = _quantised_field(seed, 6, list(levels))
+        v = oracle.sparse_mc_vertices(coords, corners, iso)
+        t = _model_tris(oracle, coords, corners, iso)
+        if len(t) == 0:
+            continue
+        e, cnt, dcnt = _edges(t)
+        assert (cnt <= 2).all() and (dcnt == 1).all()
+        und, c2 = np.unique(np.sort(e, 1), axis=0, return_counts=True)
+        open_v = v[und[c2 == 1].reshape(-1)]
+        assert np.all(np.any((open_v == 0) | (open_v == 6), axis=1))
+        assert not np.any((t[:, 0] == t[:, 1]) | (t[:, 1] == t[:, 2]) | (t[:, 0] == t[:, 2]))
