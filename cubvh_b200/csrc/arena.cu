@@ -218,22 +218,22 @@ int cubvh_arena_create(int32_t n_meshes, const float* const* vertices, const int
     a->nodes.resize(nn); a->tris.resize(nt); a->gslot.resize(nt);
     next = 0;
     run_workers(nthr, [&] {
-            for (int i; (i = next.fetch_add(1)) < M;) {
-                const int m = order[i];
-                const int32_t no = (int32_t)node_off[m], to = (int32_t)tri_off[m];
-                CNode* dn = a->nodes.data() + node_off[m];
-                for (const CNode& src : hb[m].nodes) {
-                    CNode nd = src;
-                    nd.child_base += no; nd.tri_base += to;
-                    *dn++ = nd;
-                }
-                std::memcpy(a->tris.data() + tri_off[m], hb[m].tris.data(), hb[m].tris.size() * sizeof(CTri));
-                int32_t* gs = a->gslot.data() + a->face_off[m];
-                for (size_t s = 0; s < hb[m].tris.size(); ++s) gs[hb[m].tris[s].id] = to + (int32_t)s;
-                HostBvh().nodes.swap(hb[m].nodes);  // release the per-mesh copy early
-                HostBvh().tris.swap(hb[m].tris);
+        for (int i; (i = next.fetch_add(1)) < M;) {
+            const int m = order[i];
+            const int32_t no = (int32_t)node_off[m], to = (int32_t)tri_off[m];
+            CNode* dn = a->nodes.data() + node_off[m];
+            for (const CNode& src : hb[m].nodes) {
+                CNode nd = src;
+                nd.child_base += no; nd.tri_base += to;
+                *dn++ = nd;
             }
-        });
+            std::memcpy(a->tris.data() + tri_off[m], hb[m].tris.data(), hb[m].tris.size() * sizeof(CTri));
+            int32_t* gs = a->gslot.data() + a->face_off[m];
+            for (size_t s = 0; s < hb[m].tris.size(); ++s) gs[hb[m].tris[s].id] = to + (int32_t)s;
+            HostBvh().nodes.swap(hb[m].nodes);  // release the per-mesh copy early
+            HostBvh().tris.swap(hb[m].tris);
+        }
+    });
     a->n_nodes = (int64_t)a->nodes.size();
     a->n_tris = (int64_t)a->tris.size();
     *out = a.release();
