@@ -587,6 +587,9 @@ def run_ours(args):
             nb_, nt_ = counts[op]
             alg = n * (io_bytes_per_query(op) + 24.0 * nb_ + 36.0 * nt_)
         achieved = alg / (per_op_ms[dom] / 1e3) / 1e9
+        # CPU-baseline leg: the reference's algorithm restated in oracle/ is
+        # timed here (queries and its host BVH build) as a baseline beside
+        # ours; nothing measured above runs through it
         cpu_q, cpu_t, cpu_thr, cpu_desc = cpu_time_sample(wl, wl.get("cpu_sample", 16 << 20))
         ops_detail = {"bvh_build": {"faces": int(len(wl["faces"])), "host_sah_s": build_host_s,
                                     "device_lbvh_s": build_dev_s, "reference_cpu_s": build_time_reference(wl)}}
