@@ -401,10 +401,8 @@ int cubvh_bvh_info(const cubvh_bvh* h, int64_t* n_faces, int64_t* n_nodes, int32
 int cubvh_bvh_state_dict_sizes(const cubvh_bvh* h, int64_t* n_node_records, int64_t* n_tri_records) {
     CUBVH_GUARD_BEGIN
     if (!h || !n_node_records || !n_tri_records) return fail(CUBVH_ERR_INVALID, "null argument");
-    RefFormat rf;
-    export_reference_format(h->xyz.data(), h->ids.data(), (int64_t)h->ids.size(), rf);
-    *n_node_records = (int64_t)(rf.nodes.size() / 9);
-    *n_tri_records = (int64_t)(rf.tris.size() / 12);
+    *n_node_records = reference_format_nodes((int64_t)h->ids.size());  // no build needed for the sizes
+    *n_tri_records = (int64_t)h->ids.size();
     return CUBVH_OK;
     CUBVH_GUARD_END
 }
@@ -414,6 +412,8 @@ int cubvh_bvh_state_dict(const cubvh_bvh* h, int32_t* node_records, int32_t* tri
     if (!h || !node_records || !tri_records) return fail(CUBVH_ERR_INVALID, "null argument");
     RefFormat rf;
     export_reference_format(h->xyz.data(), h->ids.data(), (int64_t)h->ids.size(), rf);
+    if ((int64_t)rf.nodes.size() != 9 * reference_format_nodes((int64_t)h->ids.size()))
+        return fail(CUBVH_ERR_INVALID, "internal: reference-format node count mismatch");
     std::memcpy(node_records, rf.nodes.data(), rf.nodes.size() * sizeof(int32_t));
     std::memcpy(tri_records, rf.tris.data(), rf.tris.size() * sizeof(int32_t));
     return CUBVH_OK;

@@ -491,23 +491,48 @@ void refit_host(HostBvh& bvh) {
 // ---------------------------------------------------------------------------
 // reference record format (state_dict)
 // ---------------------------------------------------------------------------
+int64_t reference_format_nodes(int64_t nf) {
+    if (nf <= 8) return 1;
+    int64_t count = 1;
+    std::vector<int64_t> ranges{nf};
+    while (!ranges.empty()) {
+        const int64_t n = ranges.back();
+        ranges.pop_back();
+        for (int c = 0; c < 4; ++c) {
+            const int64_t m = n * (c + 1) / 4 - n * c / 4;
+            ++count;
+            if (m > 8) ranges.push_back(m);
+        }
+    }
+    return count;
+}
+
 void export_reference_format(const float* xyz, const int64_t* ids, int64_t nf, RefFormat& out) {
     struct RNode { float lo[3], hi[3]; int32_t left, right, escape; };
     static_assert(sizeof(RNode) == 36, "reference node record is 36 bytes");
-    std::vector<int> order(nf);
-    std::iota(order.begin(), order.end(), 0);
-    std::vector<float> cen(3 * nf);
-    for (int64_t f = 0; f < nf; ++f)
-        for (int k = 0; k < 3; ++k)
-            cen[3 * f + k] = (xyz[9 * f + k] + xyz[9 * f + 3 + k] + xyz[9 * f + 6 + k]) / 3.0f;
+    // per-triangle centroid and vertex bounds, kept in the current order of
+    // the ranges so every pass reads sequentially.  A range's box from the
+    // per-triangle bounds has the bits a vertex-by-vertex scan gives:
+    // std::min / std::max keep the first of equal values either way.
+    struct TriRec { float c[3], lo[3], hi[3]; int f; };
+    std::vector<TriRec> rec((size_t)nf), rec2;
+    for (int64_t f = 0; f < nf; ++f) {
+        TriRec& r = rec[(size_t)f];
+        const float* p = xyz + 9 * f;
+        for (int k = 0; k < 3; ++k) {
+            r.c[k] = (p[k] + p[3 + k] + p[6 + k]) / 3.0f;
+            r.lo[k] = std::min(std::min(p[k], p[3 + k]), p[6 + k]);
+            r.hi[k] = std::max(std::max(p[k], p[3 + k]), p[6 + k]);
+        }
+        r.f = (int)f;
+    }
     auto box_of = [&](int b, int e, RNode& n) {
         for (int k = 0; k < 3; ++k) { n.lo[k] = INFINITY; n.hi[k] = -INFINITY; }
         for (int i = b; i < e; ++i)
-            for (int v = 0; v < 3; ++v)
-                for (int k = 0; k < 3; ++k) {
-                    const float c = xyz[9 * (int64_t)order[i] + 3 * v + k];
-                    n.lo[k] = std::min(n.lo[k], c); n.hi[k] = std::max(n.hi[k], c);
-                }
+            for (int k = 0; k < 3; ++k) {
+                n.lo[k] = std::min(n.lo[k], rec[(size_t)i].lo[k]);
+                n.hi[k] = std::max(n.hi[k], rec[(size_t)i].hi[k]);
+            }
     };
     // 4-ary tree, exactly four children per inner node (the reference's
     // traversal always reads four), leaves of at most 8 triangles: each inner
@@ -517,6 +542,7 @@ void export_reference_format(const float* xyz, const int64_t* ids, int64_t nf, R
     nodes[0].left = nodes[0].right = nodes[0].escape = -1;
     struct W { int node, b, e; };
     std::vector<W> stack;
+    std::vector<uint64_t> keys;
     if (nf > 8) stack.push_back({0, 0, (int)nf});
     else { nodes[0].left = -1; nodes[0].right = -(int)nf - 1; }
     while (!stack.empty()) {
@@ -524,13 +550,28 @@ void export_reference_format(const float* xyz, const int64_t* ids, int64_t nf, R
         float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
         for (int i = w.b; i < w.e; ++i)
             for (int k = 0; k < 3; ++k) {
-                lo[k] = std::min(lo[k], cen[3 * order[i] + k]); hi[k] = std::max(hi[k], cen[3 * order[i] + k]);
+                lo[k] = std::min(lo[k], rec[(size_t)i].c[k]); hi[k] = std::max(hi[k], rec[(size_t)i].c[k]);
             }
         int ax = 0;
         for (int k = 1; k < 3; ++k) if (hi[k] - lo[k] > hi[ax] - lo[ax]) ax = k;
-        std::stable_sort(order.begin() + w.b, order.begin() + w.e,
-                         [&](int a, int b) { return cen[3 * a + ax] < cen[3 * b + ax]; });
         const int n = w.e - w.b;
+        // stable order of the range along ax, as std::stable_sort by the
+        // centroid coordinate gives it: sort 64-bit keys of (coordinate as an
+        // order-preserving integer, current position); -0.0 is made +0.0
+        // first, since < treats them as equal and equal coordinates keep
+        // their current order
+        keys.resize((size_t)n);
+        for (int i = 0; i < n; ++i) {
+            const float c = rec[(size_t)(w.b + i)].c[ax] + 0.0f;
+            uint32_t u;
+            std::memcpy(&u, &c, sizeof(u));
+            u = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+            keys[(size_t)i] = ((uint64_t)u << 32) | (uint32_t)i;
+        }
+        std::sort(keys.begin(), keys.end());
+        rec2.resize((size_t)n);
+        for (int i = 0; i < n; ++i) rec2[(size_t)i] = rec[(size_t)(w.b + (int)(uint32_t)keys[(size_t)i])];
+        std::copy(rec2.begin(), rec2.end(), rec.begin() + w.b);
         const int first = (int)nodes.size();
         nodes[w.node].left = first; nodes[w.node].right = first + 4;
         for (int c = 0; c < 4; ++c) {
@@ -553,7 +594,7 @@ void export_reference_format(const float* xyz, const int64_t* ids, int64_t nf, R
     std::memcpy(out.nodes.data(), nodes.data(), nodes.size() * sizeof(RNode));
     out.tris.assign(nf * 12, 0);
     for (int64_t i = 0; i < nf; ++i) {
-        const int f = order[i];
+        const int f = rec[(size_t)i].f;
         float* dst = reinterpret_cast<float*>(&out.tris[12 * i]);
         std::memcpy(dst, xyz + 9 * (int64_t)f, 9 * sizeof(float));
         const int64_t id = ids ? ids[f] : (int64_t)f;

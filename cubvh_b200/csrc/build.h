@@ -90,5 +90,8 @@ struct RefFormat {
 };
 // ids: face id of each triangle of tri_xyz (NULL = its position).
 void export_reference_format(const float* tri_xyz, const int64_t* ids, int64_t n_faces, RefFormat& out);
+// Node records export_reference_format writes for n_faces triangles: the
+// tree's shape depends on the count only (ranges cut in four by count).
+int64_t reference_format_nodes(int64_t n_faces);
 
 }  // namespace cubvh
