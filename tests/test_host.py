@@ -331,3 +331,32 @@ def test_build_threads_env_same_tree():
                            timeout=300)
         assert r.returncode == 0, r.stderr
         assert r.stdout.strip().splitlines()[-1] == LAYOUT_SHA256["ico6"]
+
+
+def _signed_zero_sheet():
+    """A flat 60 x 60 sheet in z = 0 with -0.0 mixed into the coordinates
+    (ties and signed zeros in the reference-format sort and boxes)."""
+    g = np.stack(np.meshgrid(np.arange(60), np.arange(60), indexing="ij"), -1).reshape(-1, 2)
+    v = np.concatenate([g * 0.01, np.zeros((len(g), 1))], 1).astype(np.float32)
+    v[::3, 2] = -0.0
+    v[::7, 0] = -0.0 * v[::7, 0]
+    i = np.nonzero((g[:, 0] < 59) & (g[:, 1] < 59))[0]
+    return v, np.concatenate([np.stack([i, i + 60, i + 1], 1), np.stack([i + 1, i + 60, i + 61], 1)])
+
+
+STATE_DICT_SHA256 = {
+    # sha256 of the nodes and triangles records state_dict returns
+    "ico6": "60355373642b7a6c1964f247f63c7df14eb87baa134b8625e270e2bd91bdb85a",
+    "tori": "191a1577694b8e22e03c9870f59680df762bb0d98f3e3e4420fb39c708bb9f80",
+    "sheet": "e31e048f37e6b6a818f1075d2e32f6e4f63d9cbf09ac8a78693e50c1c29c8189",
+}
+
+
+@pytest.mark.parametrize("mesh", sorted(STATE_DICT_SHA256))
+def test_state_dict_records_pinned(mesh):
+    import hashlib
+    v, f = {"ico6": lambda: W.displaced_icosphere(6, 1), "tori": lambda: W.random_tori(2),
+            "sheet": _signed_zero_sheet}[mesh]()
+    sd = cubvh.cuBVH(v, f).state_dict()
+    digest = hashlib.sha256(sd["nodes"].numpy().tobytes() + sd["triangles"].numpy().tobytes()).hexdigest()
+    assert digest == STATE_DICT_SHA256[mesh]
