@@ -360,3 +360,22 @@ def test_state_dict_records_pinned(mesh):
     sd = cubvh.cuBVH(v, f).state_dict()
     digest = hashlib.sha256(sd["nodes"].numpy().tobytes() + sd["triangles"].numpy().tobytes()).hexdigest()
     assert digest == STATE_DICT_SHA256[mesh]
+
+
+def test_state_dict_sizes_for_many_face_counts():
+    """The node-record count state_dict reports (computed from the face count
+    alone) is the one its records have, for small and uneven counts."""
+    rng = np.random.default_rng(7)
+    for nf in list(range(9, 80)) + [255, 256, 257, 1023, 4097, 30011]:
+        v = rng.random((nf * 3, 3)).astype(np.float32)
+        f = np.arange(nf * 3, dtype=np.int64).reshape(-1, 3)
+        sd = cubvh.cuBVH(v, f).state_dict()
+        nodes, tris = sd["nodes"], sd["triangles"]
+        assert tris.shape == (nf, 12) and nodes.shape[1] == 9
+        # every node's child links point inside the array; leaves cover all faces once
+        recs = nodes.numpy().view(REFNODE).reshape(-1)
+        inner = recs["left"] >= 0
+        assert np.all(recs["right"][inner] <= len(recs))
+        leaf_ranges = sorted((-l - 1, -r - 1) for l, r in zip(recs["left"][~inner], recs["right"][~inner]))
+        assert leaf_ranges[0][0] == 0 and leaf_ranges[-1][1] == nf
+        assert all(a[1] == b[0] for a, b in zip(leaf_ranges, leaf_ranges[1:]))
