@@ -354,3 +354,147 @@ class RefBVH:
         c = np.zeros(2, np.int64) if count else None
         lib().orc_ref_sdf(self._h, _p(pts), I64(n), ctypes.c_int(mode), _p(d), _p(fid), _p(uvw), _p(c))
         return (d, fid, uvw, c) if count else (d, fid, uvw)
+
+
+# ------------------------------------------- the reference's own BVH (oracle/_ref)
+_REF_BVH_PATH = os.path.join(_HERE, "_ref", "libref_bvh.so")
+_ref_bvh = None
+
+
+def ref_bvh_available() -> bool:
+    """True when the reference's own BVH code (src/bvh.cu, compiled unchanged
+    against the Eigen stand-in) is in oracle/_ref (oracle/Makefile target
+    `ref`)."""
+    return os.path.exists(_REF_BVH_PATH)
+
+
+def _ref_bvh_lib():
+    global _ref_bvh
+    if _ref_bvh is None:
+        if not ref_bvh_available():
+            raise FileNotFoundError(_REF_BVH_PATH + " not built (make -C oracle ref REF=<reference checkout>)")
+        L = ctypes.CDLL(_REF_BVH_PATH)
+        vp, i64, i32 = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int
+        L.ref_bvh_create.restype = vp
+        L.ref_bvh_create.argtypes = [vp, i64, vp, i64]
+        L.ref_bvh_destroy.argtypes = [vp]
+        L.ref_bvh_num_nodes.restype = i64
+        L.ref_bvh_num_nodes.argtypes = [vp]
+        L.ref_bvh_export.argtypes = [vp, vp, vp]
+        L.ref_bvh_last_error.restype = ctypes.c_char_p
+        L.ref_bvh_unsigned_distance_gpu.argtypes = [vp, vp, i64, vp, vp, vp, vp]
+        L.ref_bvh_signed_distance_gpu.argtypes = [vp, vp, i64, i32, vp, vp, vp, vp]
+        L.ref_bvh_ray_trace_gpu.argtypes = [vp, vp, vp, i64, vp, vp, vp, vp]
+        L.ref_stab_directions_gpu.argtypes = [i64, i64, vp, vp]
+        L.ref_stab_directions_host.argtypes = [i64, i64, vp]
+        L.ref_bvh_unsigned_distance_host.argtypes = [vp, vp, i64, i64, vp, vp, vp, i32]
+        L.ref_bvh_signed_distance_host.argtypes = [vp, vp, i64, i64, i32, i64, vp, vp, vp, i32]
+        L.ref_bvh_ray_trace_host.argtypes = [vp, vp, vp, i64, i64, vp, vp, vp, i32]
+        for fn in ("unsigned_distance_gpu", "signed_distance_gpu", "ray_trace_gpu", "unsigned_distance_host",
+                   "signed_distance_host", "ray_trace_host"):
+            getattr(L, "ref_bvh_" + fn).restype = i32
+        L.ref_stab_directions_gpu.restype = i32
+        _ref_bvh = L
+    return _ref_bvh
+
+
+def ref_stab_dirs_host(n, i0=0):
+    """Stab directions [n, 32, 3] of queries i0 .. i0+n-1 from the reference's
+    own code built for the host (host sincosf)."""
+    out = np.empty((n, 32, 3), np.float32)
+    _ref_bvh_lib().ref_stab_directions_host(I64(i0), I64(n), _p(out))
+    return out
+
+
+def ref_stab_dirs_gpu_ptr(first, n, out_ptr, stream_ptr=0):
+    """Stab directions [n, 32, 3] float32 written to device memory out_ptr, as
+    the reference's raystab kernel computes them for its threads first ..
+    first+n-1 (CUDA sincosf).  Asynchronous on stream_ptr."""
+    L = _ref_bvh_lib()
+    if L.ref_stab_directions_gpu(I64(first), I64(n), ctypes.c_void_p(out_ptr), ctypes.c_void_p(stream_ptr)) != 0:
+        raise RuntimeError("reference stab directions: " + L.ref_bvh_last_error().decode())
+
+
+class ReferenceBVH:
+    """The reference's own BVH4 (src/bvh.cu), built from vertices / faces as
+    cuBVHImpl does (src/api_gpu.cu:21-40, leaf size 8).
+
+    Host methods run the reference's __host__ traversals per query on the
+    host cores (OpenMP) and return numpy arrays; `stride` takes every
+    stride-th query.  *_gpu methods run the reference's CUDA launchers on
+    device pointers (ints, e.g. torch's data_ptr()) on the given stream."""
+
+    def __init__(self, V, F):
+        V, F = _f32(V), _i64(F)
+        if F.size and (F.min() < 0 or F.max() >= len(V)):
+            raise ValueError("face index out of range")
+        L = _ref_bvh_lib()
+        h = L.ref_bvh_create(_p(V), I64(len(V)), _p(F), I64(len(F)))
+        if not h:
+            raise RuntimeError("reference BVH build: " + L.ref_bvh_last_error().decode())
+        self._h = ctypes.c_void_p(h)
+        self.n_faces = len(F)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _ref_bvh is not None:
+            _ref_bvh.ref_bvh_destroy(h)
+            self._h = None
+
+    @property
+    def n_nodes(self):
+        return int(_ref_bvh_lib().ref_bvh_num_nodes(self._h))
+
+    def state_dict_arrays(self):
+        nodes = np.empty((self.n_nodes, 9), np.int32)
+        tris = np.empty((self.n_faces, 12), np.int32)
+        _ref_bvh_lib().ref_bvh_export(self._h, _p(nodes), _p(tris))
+        return nodes, tris
+
+    # ---- host traversals
+    def unsigned_distance(self, pts, return_uvw=False, stride=1, threads=0):
+        pts = _f32(pts)
+        m = (len(pts) + stride - 1) // stride
+        d = np.empty(m, np.float32); fid = np.empty(m, np.int64)
+        uvw = np.empty((m, 3), np.float32) if return_uvw else None
+        _ref_bvh_lib().ref_bvh_unsigned_distance_host(self._h, _p(pts), I64(len(pts)), I64(stride), _p(d), _p(fid),
+                                                      _p(uvw), ctypes.c_int(threads))
+        return d, fid, uvw
+
+    def signed_distance(self, pts, mode=0, return_uvw=False, first_index=0, stride=1, threads=0):
+        pts = _f32(pts)
+        m = (len(pts) + stride - 1) // stride
+        d = np.empty(m, np.float32); fid = np.empty(m, np.int64)
+        uvw = np.empty((m, 3), np.float32) if return_uvw else None
+        _ref_bvh_lib().ref_bvh_signed_distance_host(self._h, _p(pts), I64(len(pts)), I64(stride), ctypes.c_int(mode),
+                                                    I64(first_index), _p(d), _p(fid), _p(uvw), ctypes.c_int(threads))
+        return d, fid, uvw
+
+    def ray_trace(self, ro, rd, stride=1, threads=0):
+        ro, rd = _f32(ro), _f32(rd)
+        m = (len(ro) + stride - 1) // stride
+        pos = np.empty((m, 3), np.float32); fid = np.empty(m, np.int64); dep = np.empty(m, np.float32)
+        _ref_bvh_lib().ref_bvh_ray_trace_host(self._h, _p(ro), _p(rd), I64(len(ro)), I64(stride), _p(pos), _p(fid),
+                                              _p(dep), ctypes.c_int(threads))
+        return pos, fid, dep
+
+    # ---- the reference's CUDA launchers (device pointers)
+    def _check(self, rc, what):
+        if rc != 0:
+            raise RuntimeError("reference %s: %s" % (what, _ref_bvh_lib().ref_bvh_last_error().decode()))
+
+    def unsigned_distance_gpu(self, pts, n, dist, fid, uvw=0, stream=0):
+        vp = ctypes.c_void_p
+        self._check(_ref_bvh_lib().ref_bvh_unsigned_distance_gpu(self._h, vp(pts), I64(n), vp(dist), vp(fid),
+                                                                  vp(uvw), vp(stream)), "unsigned_distance")
+
+    def signed_distance_gpu(self, pts, n, mode, dist, fid, uvw=0, stream=0):
+        vp = ctypes.c_void_p
+        self._check(_ref_bvh_lib().ref_bvh_signed_distance_gpu(self._h, vp(pts), I64(n), ctypes.c_int(mode),
+                                                                vp(dist), vp(fid), vp(uvw), vp(stream)),
+                    "signed_distance")
+
+    def ray_trace_gpu(self, ro, rd, n, pos, fid, depth, stream=0):
+        vp = ctypes.c_void_p
+        self._check(_ref_bvh_lib().ref_bvh_ray_trace_gpu(self._h, vp(ro), vp(rd), I64(n), vp(pos), vp(fid),
+                                                         vp(depth), vp(stream)), "ray_trace")
