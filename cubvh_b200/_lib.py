@@ -26,6 +26,7 @@ c_int = ctypes.c_int
 _SIGS = {
     "cubvh_bvh_create": [c_vp, c_i64, c_vp, c_i64, ctypes.POINTER(c_vp)],
     "cubvh_bvh_create_from_records": [c_vp, c_i64, ctypes.POINTER(c_vp)],
+    "cubvh_bvh_create_from_state_dict": [c_vp, c_i64, c_vp, c_i64, ctypes.POINTER(c_vp)],
     "cubvh_bvh_create_device": [c_vp, c_i64, c_vp, c_i64, c_i32, c_vp, ctypes.POINTER(c_vp)],
     "cubvh_bvh_destroy": [c_vp],
     "cubvh_bvh_info": [c_vp, ctypes.POINTER(c_i64), ctypes.POINTER(c_i64), ctypes.POINTER(c_i32)],

@@ -113,6 +113,11 @@ class _DistanceFn(torch.autograd.Function):
         return gp, gv, None, None, None
 
 
+# Record format of cuBVH.state_dict(): 1 = the reference's int32 [n, 9] node
+# and [F, 12] triangle records, which unversioned reference dicts also hold.
+STATE_DICT_VERSION = 1
+
+
 class cuBVH:
     def __init__(self, vertices, triangles, device_build: bool = False):
         # vertices: np.ndarray / torch.Tensor [N, 3]; triangles: [M, 3]
@@ -146,18 +151,32 @@ class cuBVH:
 
     # ----------------------------------------------------------- state dict
     def state_dict(self):
-        """{'nodes': int32 [n, 9], 'triangles': int32 [F, 12]} in the
-        reference's record format (CPU tensors)."""
+        """{'nodes': int32 [n, 9], 'triangles': int32 [F, 12], 'version':
+        int32 [1]} (CPU tensors).  nodes and triangles are the reference's
+        records (include/gpu/bvh.cuh:84-109, src/api_gpu.cu:110-121), so the
+        reference's from_state_dict loads the dict (it reads those two keys
+        only); 'version' tags the record format (STATE_DICT_VERSION)."""
         nn, nt = ctypes.c_int64(), ctypes.c_int64()
         check(lib().cubvh_bvh_state_dict_sizes(self.impl.raw, ctypes.byref(nn), ctypes.byref(nt)),
               "state_dict")
         nodes = torch.empty(int(nn.value), 9, dtype=torch.int32)
         tris = torch.empty(int(nt.value), 12, dtype=torch.int32)
         check(lib().cubvh_bvh_state_dict(self.impl.raw, _ptr(nodes), _ptr(tris)), "state_dict")
-        return {"nodes": nodes, "triangles": tris}
+        return {"nodes": nodes, "triangles": tris,
+                "version": torch.tensor([STATE_DICT_VERSION], dtype=torch.int32)}
 
     @staticmethod
     def from_state_dict(state_dict):
+        """Mirror of cubvh/api.py:26-36.  Accepts dicts of this library
+        (version 1) and of the reference (no 'version' key, same records);
+        any other version raises RuntimeError."""
+        if "version" in state_dict:
+            ver = state_dict["version"]
+            ver = int(ver.reshape(-1)[0]) if torch.is_tensor(ver) and ver.numel() == 1 else ver
+            if not isinstance(ver, int) or ver != STATE_DICT_VERSION:
+                raise RuntimeError(f"state_dict format version {ver!r} is not supported "
+                                   f"(this library reads version {STATE_DICT_VERSION} and unversioned "
+                                   f"reference dicts)")
         if "triangles" not in state_dict:
             raise RuntimeError("state_dict missing 'triangles' tensor")
         if "nodes" not in state_dict:
@@ -168,9 +187,16 @@ class cuBVH:
         tris = tris.contiguous()
         if tris.dtype != torch.int32 or tris.dim() != 2 or tris.shape[1] != 12:
             raise RuntimeError("triangles must be an int32 [F, 12] tensor of triangle records")
+        nodes = state_dict["nodes"]
+        if not torch.is_tensor(nodes) or nodes.device.type != "cpu":
+            raise RuntimeError("nodes must be on CPU")
+        nodes = nodes.contiguous()
+        if nodes.dtype != torch.int32 or nodes.dim() != 2 or nodes.shape[1] != 9 or nodes.shape[0] == 0:
+            raise RuntimeError("nodes must be an int32 [n, 9] tensor of node records")
         raw = ctypes.c_void_p()
-        check(lib().cubvh_bvh_create_from_records(_ptr(tris), tris.shape[0], ctypes.byref(raw)),
-              "from_state_dict")
+        # the loaded records are kept: state_dict() returns them unchanged
+        check(lib().cubvh_bvh_create_from_state_dict(_ptr(nodes), nodes.shape[0], _ptr(tris), tris.shape[0],
+                                                     ctypes.byref(raw)), "from_state_dict")
         obj = cuBVH.__new__(cuBVH)
         obj.impl = _Handle(raw)
         return obj
@@ -336,10 +362,14 @@ class cuBVH:
         return self._query(positions, return_uvw, m, vertices)
 
 
-def floodfill(grid, check_bounds: bool = False):
+def floodfill(grid, check_bounds: bool = True):
     # grid: torch.Tensor, bool, [B, H, W, D] or [H, W, D]
     # return: torch.Tensor, int32, same shape: -1 for occupied voxels, else the
     # smallest linear index of the voxel's free component (not remapped)
+    # check_bounds (default): wait for the result and raise RuntimeError if the
+    # union-find hit its device-side step bound (the reference's floodfill
+    # also returns only when done); False keeps the call asynchronous on the
+    # current stream and skips the check.
     grid = grid.contiguous()
     if not grid.is_cuda: grid = grid.cuda()
     squeeze = grid.dim() == 3
@@ -400,7 +430,7 @@ def sparse_marching_cubes(coords, corners, iso, ensure_consistency=False):
     return verts, tris
 
 
-def udf_to_sdf(udf, eps: float = None, check_bounds: bool = False):
+def udf_to_sdf(udf, eps: float = None, check_bounds: bool = True):
     """Signed distance grid from an unsigned distance grid, in one fused
     floodfill pass: the occupancy -> SDF step of the reference's watertight
     recipe (test/benchmark_watertight.py:89-143, readme.md:95-102), which the
@@ -414,7 +444,8 @@ def udf_to_sdf(udf, eps: float = None, check_bounds: bool = False):
     eps: occupancy threshold; default 2 / resolution, resolution = the last
     dimension (the reference's 2-voxel tolerance for a res^3 grid).
     Returns float32 of the same shape.  Results equal the composition above
-    bit for bit (voxel labels as ``floodfill``)."""
+    bit for bit (voxel labels as ``floodfill``).  check_bounds as for
+    ``floodfill``."""
     udf = udf.float().contiguous()
     if not udf.is_cuda: udf = udf.cuda()
     squeeze = udf.dim() == 3

@@ -59,6 +59,9 @@ struct cubvh_bvh {
     HostBvh host;
     RawVec<float> xyz;            // [F, 9] a, b, c of each face, face order
     RawVec<int64_t> ids;          // face id of each face (position for meshes)
+    // state_dict records this BVH was loaded from (cubvh_bvh_create_from_state_dict),
+    // returned unchanged by cubvh_bvh_state_dict as the reference does
+    std::vector<int32_t> sd_nodes, sd_tris;
     std::mutex mu;
     std::deque<DevCopy> dev;      // stable addresses across push_back
 };
@@ -357,6 +360,22 @@ int cubvh_bvh_create_from_records(const int32_t* rec, int64_t n_faces, cubvh_bvh
     CUBVH_GUARD_END
 }
 
+int cubvh_bvh_create_from_state_dict(const int32_t* node_records, int64_t n_node_records, const int32_t* rec,
+                                     int64_t n_faces, cubvh_bvh** out) {
+    CUBVH_GUARD_BEGIN
+    if (!out) return fail(CUBVH_ERR_INVALID, "out is null");
+    *out = nullptr;
+    if (!node_records || n_node_records <= 0) return fail(CUBVH_ERR_INVALID, "no node records");
+    cubvh_bvh* h = nullptr;
+    const int rc = cubvh_bvh_create_from_records(rec, n_faces, &h);
+    if (rc != CUBVH_OK) return rc;
+    h->sd_nodes.assign(node_records, node_records + 9 * n_node_records);
+    h->sd_tris.assign(rec, rec + 12 * n_faces);
+    *out = h;
+    return CUBVH_OK;
+    CUBVH_GUARD_END
+}
+
 int cubvh_bvh_destroy(cubvh_bvh* h) {
     CUBVH_GUARD_BEGIN
     if (!h) return CUBVH_OK;
@@ -401,7 +420,9 @@ int cubvh_bvh_info(const cubvh_bvh* h, int64_t* n_faces, int64_t* n_nodes, int32
 int cubvh_bvh_state_dict_sizes(const cubvh_bvh* h, int64_t* n_node_records, int64_t* n_tri_records) {
     CUBVH_GUARD_BEGIN
     if (!h || !n_node_records || !n_tri_records) return fail(CUBVH_ERR_INVALID, "null argument");
-    *n_node_records = reference_format_nodes((int64_t)h->ids.size());  // no build needed for the sizes
+    // no build needed for the sizes
+    *n_node_records = h->sd_nodes.empty() ? reference_format_nodes((int64_t)h->ids.size())
+                                          : (int64_t)h->sd_nodes.size() / 9;
     *n_tri_records = (int64_t)h->ids.size();
     return CUBVH_OK;
     CUBVH_GUARD_END
@@ -410,6 +431,11 @@ int cubvh_bvh_state_dict_sizes(const cubvh_bvh* h, int64_t* n_node_records, int6
 int cubvh_bvh_state_dict(const cubvh_bvh* h, int32_t* node_records, int32_t* tri_records) {
     CUBVH_GUARD_BEGIN
     if (!h || !node_records || !tri_records) return fail(CUBVH_ERR_INVALID, "null argument");
+    if (!h->sd_nodes.empty()) {
+        std::memcpy(node_records, h->sd_nodes.data(), h->sd_nodes.size() * sizeof(int32_t));
+        std::memcpy(tri_records, h->sd_tris.data(), h->sd_tris.size() * sizeof(int32_t));
+        return CUBVH_OK;
+    }
     RefFormat rf;
     export_reference_format(h->xyz.data(), h->ids.data(), (int64_t)h->ids.size(), rf);
     if ((int64_t)rf.nodes.size() != 9 * reference_format_nodes((int64_t)h->ids.size()))
@@ -863,9 +889,17 @@ int cubvh_udf_to_sdf(const float* udf, int B, int H, int W, int D, float eps, fl
 
 int cubvh_floodfill_check(const void* workspace, int B, int H, int W, int D, void* stream) {
     CUBVH_GUARD_BEGIN
-    if (!workspace) return fail(CUBVH_ERR_INVALID, "workspace is null");
-    const int rc = check_grid_dims(B, H, W, D);
+    int rc = check_grid_dims(B, H, W, D);
     if (rc != CUBVH_OK) return rc;
+    if (!workspace) {
+        // the fixed array of cubvh_floodfill_noalloc
+        std::string err;
+        void* ws = nullptr;
+        if ((rc = floodfill_noalloc_fits(B, H, W, D, err)) != CUBVH_OK ||
+            (rc = floodfill_noalloc_scratch(&ws, err)) != CUBVH_OK)
+            return fail(rc, err);
+        workspace = ws;
+    }
     int status = 0;
     const char* p = static_cast<const char*>(workspace) + floodfill_status_offset(B, H, W, D);
     cudaError_t e = cudaMemcpyAsync(&status, p, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream);

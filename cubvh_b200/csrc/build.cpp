@@ -3,8 +3,8 @@
 //
 // The reference builds a BVH4 by centroid median splits on the host
 // (src/bvh.cu:515-620) and stores 36-byte nodes; this builder targets the
-// 80-byte compressed node instead.  export_reference_format() writes the
-// reference's own record format for state_dict compatibility.
+// 80-byte compressed node instead.  export_reference_format() writes, for
+// state_dict, the records of the reference's own build of the same mesh.
 //
 // The binary tree is built by recursion over triangle ranges; large ranges
 // hand their left half to another thread, and the breadth-first collapse
@@ -492,14 +492,16 @@ void refit_host(HostBvh& bvh) {
 // reference record format (state_dict)
 // ---------------------------------------------------------------------------
 int64_t reference_format_nodes(int64_t nf) {
-    if (nf <= 8) return 1;
+    if (nf < 4) return 1;
     int64_t count = 1;
     std::vector<int64_t> ranges{nf};
     while (!ranges.empty()) {
         const int64_t n = ranges.back();
         ranges.pop_back();
-        for (int c = 0; c < 4; ++c) {
-            const int64_t m = n * (c + 1) / 4 - n * c / 4;
+        // halves of halves: n/2 / 2, n/2 - n/2 / 2, (n - n/2) / 2, ...
+        const int64_t h0 = n / 2, h1 = n - h0;
+        const int64_t parts[4] = {h0 / 2, h0 - h0 / 2, h1 / 2, h1 - h1 / 2};
+        for (int64_t m : parts) {
             ++count;
             if (m > 8) ranges.push_back(m);
         }
@@ -507,98 +509,119 @@ int64_t reference_format_nodes(int64_t nf) {
     return count;
 }
 
+// The reference's BVH4 build (src/bvh.cu:515-620), restated so that the
+// records are the ones the reference's own build writes for the same mesh:
+//  - a range is cut in two at its middle (std::nth_element, count / 2) along
+//    the axis of largest centroid variance, the mean and variance summed in
+//    float in the range's current order (first largest axis on ties); the
+//    two halves are cut the same way, the second half first, giving four
+//    children per inner node;
+//  - children of at most 8 triangles become leaves; larger ones are pushed on
+//    a stack and split when popped (last pushed first), which numbers nodes
+//    in the reference's order;
+//  - node boxes scan the range's vertices (a, b, c per triangle) from the
+//    first vertex with std::min / std::max;
+//  - escape links in pre-order: the next sibling, else the parent's escape.
+// std::nth_element's permutation depends only on the comparison results, so
+// sorting 16-byte (centroid, face) records gives the reference's order of
+// its 48-byte triangles.  Meshes of fewer than 4 triangles (which the
+// reference cannot build) give one leaf.
 void export_reference_format(const float* xyz, const int64_t* ids, int64_t nf, RefFormat& out) {
     struct RNode { float lo[3], hi[3]; int32_t left, right, escape; };
     static_assert(sizeof(RNode) == 36, "reference node record is 36 bytes");
-    // per-triangle centroid and vertex bounds, kept in the current order of
-    // the ranges so every pass reads sequentially.  A range's box from the
-    // per-triangle bounds has the bits a vertex-by-vertex scan gives:
-    // std::min / std::max keep the first of equal values either way.
-    struct TriRec { float c[3], lo[3], hi[3]; int f; };
-    std::vector<TriRec> rec((size_t)nf), rec2;
+    struct Rec { float c[3]; int32_t f; };
+    std::vector<Rec> rec((size_t)nf);
     for (int64_t f = 0; f < nf; ++f) {
-        TriRec& r = rec[(size_t)f];
         const float* p = xyz + 9 * f;
-        for (int k = 0; k < 3; ++k) {
-            r.c[k] = (p[k] + p[3 + k] + p[6 + k]) / 3.0f;
-            r.lo[k] = std::min(std::min(p[k], p[3 + k]), p[6 + k]);
-            r.hi[k] = std::max(std::max(p[k], p[3 + k]), p[6 + k]);
-        }
-        r.f = (int)f;
+        // Triangle::centroid(): (a + b + c) / 3 per component, left to right
+        for (int k = 0; k < 3; ++k) rec[(size_t)f].c[k] = (p[k] + p[3 + k] + p[6 + k]) / 3.0f;
+        rec[(size_t)f].f = (int32_t)f;
     }
-    auto box_of = [&](int b, int e, RNode& n) {
-        for (int k = 0; k < 3; ++k) { n.lo[k] = INFINITY; n.hi[k] = -INFINITY; }
-        for (int i = b; i < e; ++i)
-            for (int k = 0; k < 3; ++k) {
-                n.lo[k] = std::min(n.lo[k], rec[(size_t)i].lo[k]);
-                n.hi[k] = std::max(n.hi[k], rec[(size_t)i].hi[k]);
-            }
+    auto box_of = [&](int64_t b, int64_t e, RNode& n) {
+        const float* p0 = xyz + 9 * (int64_t)rec[(size_t)b].f;
+        for (int k = 0; k < 3; ++k) n.lo[k] = n.hi[k] = p0[k];
+        for (int64_t i = b; i < e; ++i) {
+            const float* p = xyz + 9 * (int64_t)rec[(size_t)i].f;
+            for (int v = 0; v < 3; ++v)
+                for (int k = 0; k < 3; ++k) {
+                    n.lo[k] = std::min(n.lo[k], p[3 * v + k]);
+                    n.hi[k] = std::max(n.hi[k], p[3 * v + k]);
+                }
+        }
     };
-    // 4-ary tree, exactly four children per inner node (the reference's
-    // traversal always reads four), leaves of at most 8 triangles: each inner
-    // range is ordered along its widest centroid axis and cut in four.
     std::vector<RNode> nodes(1);
-    box_of(0, (int)nf, nodes[0]);
-    nodes[0].left = nodes[0].right = nodes[0].escape = -1;
-    struct W { int node, b, e; };
-    std::vector<W> stack;
-    std::vector<uint64_t> keys;
-    if (nf > 8) stack.push_back({0, 0, (int)nf});
-    else { nodes[0].left = -1; nodes[0].right = -(int)nf - 1; }
-    while (!stack.empty()) {
-        const W w = stack.back(); stack.pop_back();
-        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-        for (int i = w.b; i < w.e; ++i)
-            for (int k = 0; k < 3; ++k) {
-                lo[k] = std::min(lo[k], rec[(size_t)i].c[k]); hi[k] = std::max(hi[k], rec[(size_t)i].c[k]);
+    box_of(0, nf, nodes[0]);
+    nodes[0].escape = -1;
+    if (nf < 4) {
+        nodes[0].left = -1;
+        nodes[0].right = -(int32_t)nf - 1;
+    } else {
+        struct Range { int32_t node; int64_t b, e; };
+        std::vector<Range> stack{{0, 0, nf}};
+        while (!stack.empty()) {
+            const Range r = stack.back();
+            stack.pop_back();
+            int64_t cb[4] = {r.b}, ce[4] = {r.e};
+            for (int nc = 1; nc < 4; nc *= 2) {
+                for (int i = nc - 1; i >= 0; --i) {
+                    const int64_t b = cb[i], e = ce[i];
+                    const float cnt = (float)(e - b);
+                    float mean[3] = {0.f, 0.f, 0.f}, var[3] = {0.f, 0.f, 0.f};
+                    for (int64_t j = b; j < e; ++j)
+                        for (int k = 0; k < 3; ++k) mean[k] = mean[k] + rec[(size_t)j].c[k];
+                    for (int k = 0; k < 3; ++k) mean[k] = mean[k] / cnt;
+                    for (int64_t j = b; j < e; ++j)
+                        for (int k = 0; k < 3; ++k) {
+                            const float d = rec[(size_t)j].c[k] - mean[k];
+                            var[k] = var[k] + d * d;
+                        }
+                    for (int k = 0; k < 3; ++k) var[k] = var[k] / cnt;
+                    int ax = 0;
+                    for (int k = 1; k < 3; ++k)
+                        if (var[k] > var[ax]) ax = k;
+                    const int64_t m = b + (e - b) / 2;
+                    std::nth_element(rec.begin() + b, rec.begin() + m, rec.begin() + e,
+                                     [ax](const Rec& x, const Rec& y) { return x.c[ax] < y.c[ax]; });
+                    cb[2 * i] = b;
+                    ce[2 * i + 1] = e;
+                    ce[2 * i] = cb[2 * i + 1] = m;
+                }
             }
-        int ax = 0;
-        for (int k = 1; k < 3; ++k) if (hi[k] - lo[k] > hi[ax] - lo[ax]) ax = k;
-        const int n = w.e - w.b;
-        // stable order of the range along ax, as std::stable_sort by the
-        // centroid coordinate gives it: sort 64-bit keys of (coordinate as an
-        // order-preserving integer, current position); -0.0 is made +0.0
-        // first, since < treats them as equal and equal coordinates keep
-        // their current order
-        keys.resize((size_t)n);
-        for (int i = 0; i < n; ++i) {
-            const float c = rec[(size_t)(w.b + i)].c[ax] + 0.0f;
-            uint32_t u;
-            std::memcpy(&u, &c, sizeof(u));
-            u = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-            keys[(size_t)i] = ((uint64_t)u << 32) | (uint32_t)i;
-        }
-        std::sort(keys.begin(), keys.end());
-        rec2.resize((size_t)n);
-        for (int i = 0; i < n; ++i) rec2[(size_t)i] = rec[(size_t)(w.b + (int)(uint32_t)keys[(size_t)i])];
-        std::copy(rec2.begin(), rec2.end(), rec.begin() + w.b);
-        const int first = (int)nodes.size();
-        nodes[w.node].left = first; nodes[w.node].right = first + 4;
-        for (int c = 0; c < 4; ++c) {
-            const int cb = w.b + (int)((int64_t)n * c / 4), ce = w.b + (int)((int64_t)n * (c + 1) / 4);
-            RNode rn; box_of(cb, ce, rn); rn.escape = -1;
-            if (ce - cb <= 8) { rn.left = -cb - 1; rn.right = -ce - 1; nodes.push_back(rn); }
-            else { rn.left = rn.right = 0; nodes.push_back(rn); stack.push_back({first + c, cb, ce}); }
+            const int32_t first = (int32_t)nodes.size();
+            nodes[(size_t)r.node].left = first;
+            for (int c = 0; c < 4; ++c) {
+                RNode n;
+                box_of(cb[c], ce[c], n);
+                n.escape = -1;
+                if (ce[c] - cb[c] <= 8) {
+                    n.left = -(int32_t)cb[c] - 1;
+                    n.right = -(int32_t)ce[c] - 1;
+                } else {
+                    n.left = n.right = 0;
+                    stack.push_back({first + c, cb[c], ce[c]});
+                }
+                nodes.push_back(n);
+            }
+            nodes[(size_t)r.node].right = first + 4;
         }
     }
-    // pre-order escape links: the next sibling, else the parent's escape
-    std::vector<std::pair<int, int>> work{{0, -1}};
+    std::vector<std::pair<int32_t, int32_t>> work{{0, -1}};
     while (!work.empty()) {
-        const auto [ni, esc] = work.back(); work.pop_back();
-        nodes[ni].escape = esc;
-        if (nodes[ni].left < 0) continue;  // leaf
-        const int f0 = nodes[ni].left, f1 = nodes[ni].right;
-        for (int c = f1 - 1; c >= f0; --c) work.push_back({c, c + 1 < f1 ? c + 1 : esc});
+        const auto [ni, esc] = work.back();
+        work.pop_back();
+        nodes[(size_t)ni].escape = esc;
+        if (nodes[(size_t)ni].left < 0) continue;  // leaf
+        const int32_t f0 = nodes[(size_t)ni].left, f1 = nodes[(size_t)ni].right;
+        for (int32_t c = f1 - 1; c >= f0; --c) work.push_back({c, c + 1 < f1 ? c + 1 : esc});
     }
     out.nodes.resize(nodes.size() * 9);
     std::memcpy(out.nodes.data(), nodes.data(), nodes.size() * sizeof(RNode));
-    out.tris.assign(nf * 12, 0);
+    out.tris.assign((size_t)nf * 12, 0);
     for (int64_t i = 0; i < nf; ++i) {
-        const int f = rec[(size_t)i].f;
-        float* dst = reinterpret_cast<float*>(&out.tris[12 * i]);
-        std::memcpy(dst, xyz + 9 * (int64_t)f, 9 * sizeof(float));
-        const int64_t id = ids ? ids[f] : (int64_t)f;
-        std::memcpy(&out.tris[12 * i + 10], &id, sizeof(int64_t));
+        const int64_t f = rec[(size_t)i].f;
+        std::memcpy(&out.tris[12 * (size_t)i], xyz + 9 * f, 9 * sizeof(float));
+        const int64_t id = ids ? ids[f] : f;
+        std::memcpy(&out.tris[12 * (size_t)i + 10], &id, sizeof(int64_t));
     }
 }
 

@@ -36,6 +36,10 @@ void parallel_for(int64_t n, int threads, int64_t grain, F fn) {
     if (parts <= 1) { fn(0, n); return; }
     std::vector<std::thread> pool;
     std::vector<int64_t> inline_parts;
+    // both vectors sized up front: growing them inside the loop could throw
+    // with threads already running, which would terminate the process
+    pool.reserve((size_t)parts - 1);
+    inline_parts.reserve((size_t)parts - 1);
     for (int64_t i = 1; i < parts; ++i) {
         const int64_t lo = n * i / parts, hi = n * (i + 1) / parts;
         try {
@@ -80,7 +84,8 @@ bool build_bvh(const float* tri_xyz, int64_t n_faces, HostBvh& out, std::string&
 void refit_host(HostBvh& bvh);
 
 // The reference's on-disk format (include/gpu/bvh.cuh:84-109,
-// src/api_gpu.cu:110-121): a BVH4 built by median splits (src/bvh.cu:515-620)
+// src/api_gpu.cu:110-121): the BVH4 the reference's own median-split build
+// (src/bvh.cu:515-620) makes, record for record,
 // as int32 [n_nodes, 9] records (box min, box max, left, right, escape) and
 // the triangle soup in that BVH's order as int32 [F, 12] records (a, b, c,
 // 4 pad bytes, int64 original index).
@@ -91,7 +96,8 @@ struct RefFormat {
 // ids: face id of each triangle of tri_xyz (NULL = its position).
 void export_reference_format(const float* tri_xyz, const int64_t* ids, int64_t n_faces, RefFormat& out);
 // Node records export_reference_format writes for n_faces triangles: the
-// tree's shape depends on the count only (ranges cut in four by count).
+// tree's shape depends on the count only (each range halved, then each half
+// halved, down to leaves of at most 8).
 int64_t reference_format_nodes(int64_t n_faces);
 
 }  // namespace cubvh

@@ -98,6 +98,11 @@ size_t floodfill_status_offset(int B, int H, int W, int D);
 // Floodfill with the library's fixed scratch array (floodfill_noalloc.cu).
 int floodfill_noalloc(const uint8_t* grid, int B, int H, int W, int D, int32_t* labels, cudaStream_t stream,
                       std::string& err);
+// CUBVH_OK when a [B, H, W, D] floodfill fits that array, else
+// CUBVH_ERR_INVALID with a message.
+int floodfill_noalloc_fits(int B, int H, int W, int D, std::string& err);
+// Device address of that array on the current device.
+int floodfill_noalloc_scratch(void** ws, std::string& err);
 
 // Sparse marching cubes (sparse_mc.cu): device coords int32 [n, 3] and
 // corners float32 [n, 8]; the merged vertices float32 [n_verts, 3] and

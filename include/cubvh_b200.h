@@ -73,6 +73,14 @@ int cubvh_bvh_create_device(const float* vertices, int64_t n_vertices, const int
  * BVH is rebuilt).  Replaces cuBVHImpl(state_dict) (src/api_gpu.cu:47-68)
  * behind from_state_dict (src/bindings.cpp:24). */
 int cubvh_bvh_create_from_records(const int32_t* tri_records, int64_t n_faces, cubvh_bvh** out);
+/* As cubvh_bvh_create_from_records, and the BVH keeps the node records
+ * (int32 [n_node_records, 9], host) and triangle records it was loaded from:
+ * cubvh_bvh_state_dict then returns exactly those records, as the reference's
+ * state_dict does after load_state_dict (include/gpu/bvh.cuh:84-109,
+ * src/api_gpu.cu:47-68, 110-121).  The node records are stored, not checked;
+ * queries use the BVH rebuilt from the triangles. */
+int cubvh_bvh_create_from_state_dict(const int32_t* node_records, int64_t n_node_records,
+                                     const int32_t* tri_records, int64_t n_faces, cubvh_bvh** out);
 
 /* Release the BVH and its device copies.  Replaces the pybind-owned
  * delete of cuBVH (src/bindings.cpp:17-21). */
@@ -83,8 +91,10 @@ int cubvh_bvh_info(const cubvh_bvh* bvh, int64_t* n_faces, int64_t* n_nodes, int
 
 /* Reference-format state_dict: number of node records (int32 x 9 each) and
  * triangle records (int32 x 12 each), then the records themselves written to
- * host buffers of those sizes.  Replaces cuBVH::state_dict
- * (src/api_gpu.cu:110-121, include/gpu/bvh.cuh:84-94). */
+ * host buffers of those sizes: the records of the reference's own BVH4
+ * build (src/bvh.cu:515-620) of this mesh, record for record, or the loaded
+ * records for a BVH from cubvh_bvh_create_from_state_dict.  Replaces
+ * cuBVH::state_dict (src/api_gpu.cu:110-121, include/gpu/bvh.cuh:84-94). */
 int cubvh_bvh_state_dict_sizes(const cubvh_bvh* bvh, int64_t* n_node_records, int64_t* n_tri_records);
 int cubvh_bvh_state_dict(const cubvh_bvh* bvh, int32_t* node_records, int32_t* tri_records);
 
@@ -243,7 +253,9 @@ int cubvh_floodfill_workspace_size(int B, int H, int W, int D, size_t* bytes);
 int cubvh_floodfill(const uint8_t* grid, int B, int H, int W, int D, int32_t* labels, void* workspace,
                     size_t workspace_bytes, void* stream);
 /* Synchronises `stream` and returns CUBVH_ERR_DEVICE_BOUND if the floodfill
- * that last used `workspace` (same B, H, W, D) hit a device-side bound. */
+ * that last used `workspace` (same B, H, W, D) hit a device-side bound.
+ * workspace NULL: the fixed array of cubvh_floodfill_noalloc, i.e. the last
+ * no-allocation floodfill (same B, H, W, D). */
 int cubvh_floodfill_check(const void* workspace, int B, int H, int W, int D, void* stream);
 
 /* Signed distance grid from an unsigned one, fused into the floodfill (the
@@ -273,7 +285,10 @@ int cubvh_udf_to_sdf(const float* udf, int B, int H, int W, int D, float eps, fl
  * the one array: calls that overlap on the GPU (different streams, or
  * different host threads without ordering) race and corrupt each other's
  * results, so order them.  The call clears everything it reads, so no state
- * carries over between calls. */
+ * carries over between calls.  cubvh_floodfill_check(NULL, B, H, W, D,
+ * stream) reports a device-side bound hit of the last call.  The array's
+ * address is looked up once per device, so calls must not span a
+ * cudaDeviceReset of that device. */
 int cubvh_floodfill_noalloc(const uint8_t* grid, int B, int H, int W, int D, int32_t* labels, void* stream);
 
 #ifdef __cplusplus

@@ -131,6 +131,24 @@ def test_state_dict_reference_format():
     assert torch.equal(sd2["nodes"], nodes) and torch.equal(sd2["triangles"], tris)
 
 
+def test_state_dict_version():
+    v, f = W.icosphere(2)
+    sd = cubvh.cuBVH(v, f).state_dict()
+    assert sd["version"].dtype == torch.int32 and sd["version"].tolist() == [1]
+    # the reloaded BVH returns the loaded records unchanged (as the reference's)
+    back = cubvh.cuBVH.from_state_dict(sd).state_dict()
+    assert all(torch.equal(back[k], sd[k]) for k in ("nodes", "triangles", "version"))
+    # reference dicts carry no version and load the same
+    ref = cubvh.cuBVH.from_state_dict({"nodes": sd["nodes"], "triangles": sd["triangles"]})
+    assert torch.equal(ref.state_dict()["triangles"], sd["triangles"])
+    assert cubvh.cuBVH.from_state_dict(dict(sd, version=1)).num_faces == len(f)
+    for bad in (torch.tensor([2], dtype=torch.int32), 0, "1"):
+        with pytest.raises(RuntimeError, match="version"):
+            cubvh.cuBVH.from_state_dict(dict(sd, version=bad))
+    with pytest.raises(RuntimeError, match="nodes"):
+        cubvh.cuBVH.from_state_dict(dict(sd, nodes=sd["nodes"].float()))
+
+
 def test_from_state_dict_ids_survive():
     v, f = W.icosphere(1)
     sd = cubvh.cuBVH(v, f).state_dict()
@@ -285,7 +303,9 @@ def test_c_abi_rejects_bad_arguments_before_any_device_work():
     bad(L.cubvh_distance_backward(h, None, -2, None, None, None, None, None, None, None), "negative")
     assert L.cubvh_distance_backward(h, None, 0, None, None, None, None, None, None, None) == 0
     bad(L.cubvh_distance_backward(h, None, 3, None, None, None, None, None, None, None), "null")
-    bad(L.cubvh_floodfill_check(None, 1, 4, 4, 4, None), "null")
+    # NULL workspace = the no-allocation floodfill's array, which a 256^3 grid exceeds
+    bad(L.cubvh_floodfill_check(None, 1, 256, 256, 256, None), "scratch")
+    bad(L.cubvh_floodfill_check(None, -1, 4, 4, 4, None), "negative")
     bad(L.cubvh_udf_to_sdf(None, 1, 4, 4, 4, 0.01, None, None, 0, None), "null")
     assert L.cubvh_udf_to_sdf(None, 0, 4, 4, 4, 0.01, None, None, 0, None) == 0
     bad(L.cubvh_floodfill_noalloc(None, 1, 4, 4, 4, None, None), "null")
@@ -345,10 +365,12 @@ def _signed_zero_sheet():
 
 
 STATE_DICT_SHA256 = {
-    # sha256 of the nodes and triangles records state_dict returns
-    "ico6": "60355373642b7a6c1964f247f63c7df14eb87baa134b8625e270e2bd91bdb85a",
-    "tori": "191a1577694b8e22e03c9870f59680df762bb0d98f3e3e4420fb39c708bb9f80",
-    "sheet": "e31e048f37e6b6a818f1075d2e32f6e4f63d9cbf09ac8a78693e50c1c29c8189",
+    # sha256 of the nodes and triangles records state_dict returns: the
+    # records of the reference's own build of the mesh (tests/test_ref_bvh.py
+    # compares them with that build when it is compiled)
+    "ico6": "c5b808b0440a125cba10bf420ef95edcb34b5ccfe1e361174777a008a3f07370",
+    "tori": "5398185421d1f1c871f012593428baa9b6517f7c4a139f5b3aea837bbe4ef8d3",
+    "sheet": "8661958b7122c397f8412af019b4dd713296a0da201c97afcabcced720c3fa61",
 }
 
 

@@ -7,7 +7,9 @@ library, so the call needs no workspace and allocates nothing.
 Checked through the C ABI against the regular cubvh_floodfill (which takes a
 caller workspace) on two calls in a row, so that anything the first call left
 in the shared scratch would show up in the second; labels must match bit for
-bit.  This file runs last so that a failure here does not hide the rest.
+bit, and the bound status of each call (read with cubvh_floodfill_check and
+a NULL workspace) must be clear.  This file runs last so that a failure here
+does not hide the rest.
 """
 
 import ctypes
@@ -54,6 +56,8 @@ def test_floodfill_noalloc_matches_regular_twice():
         got = torch.full(grid.shape, -7, dtype=torch.int32, device=dev)
         rc = fn(grid.data_ptr(), B, H, W, D, got.data_ptr(), stream)
         assert rc == 0, L.cubvh_last_error()
+        # the bound status of this call, read from the built-in array
+        assert L.cubvh_floodfill_check(None, B, H, W, D, stream) == 0, L.cubvh_last_error()
         want = _regular(L, grid, stream)
         torch.cuda.synchronize()
         assert torch.equal(got, want)
