@@ -232,10 +232,12 @@ def build_time_device(cubvh, wl, dev, reps=3):
 
 def build_time_reference(wl):
     """Seconds for the reference's own host build (its BVH4 median-split
-    build, restated in the oracle's FP32 mirror)."""
+    build: src/bvh.cu compiled into oracle/_ref, else the oracle's FP32
+    restatement of it)."""
     from oracle import oracle as O
+    cls = O.ReferenceBVH if O.ref_bvh_available() else O.RefBVH
     t0 = time.perf_counter()
-    O.RefBVH(wl["vertices"], wl["faces"])
+    cls(wl["vertices"], wl["faces"])
     return time.perf_counter() - t0
 
 
@@ -276,13 +278,18 @@ def traversal_counts(wl, sample_stride=64):
 
 # -------------------------------------------------------------- CPU arms
 def cpu_time_sample(wl, max_queries, threads=None):
-    """Time the reference's algorithm (oracle FP32 mirror) on a strided
-    sample of at most ~max_queries queries spread over every op; returns
-    (queries, seconds, threads, description)."""
+    """Time the reference's CPU path on a strided sample of at most
+    ~max_queries queries spread over every op: its own __host__ traversals
+    (src/bvh.cu compiled into oracle/_ref, kind "reference") on all OpenMP
+    threads, or, where that library is not built, the oracle's FP32
+    restatement of them (kind "port", the same bits: tests/test_ref_bvh.py).
+    Returns (queries, seconds, threads, description, kind)."""
     from oracle import oracle as O
     if threads:
         O.set_threads(threads)
-    ref = O.RefBVH(wl["vertices"], wl["faces"])
+    kind = "reference" if O.ref_bvh_available() else "port"
+    ref = O.ReferenceBVH(wl["vertices"], wl["faces"]) if kind == "reference" else O.RefBVH(wl["vertices"], wl["faces"])
+    nthr = threads or O.threads()
     total = sum(len(a[0]) for op, a in wl["ops"] if op not in GRID_OPS)
     stride = max(1, -(-total // int(max_queries)))
     q, t, parts = 0, 0.0, []
@@ -291,20 +298,28 @@ def cpu_time_sample(wl, max_queries, threads=None):
             continue
         if op == "ray":
             ro, rd = np.ascontiguousarray(args[0][::stride]), np.ascontiguousarray(args[1][::stride])
-            t0 = time.perf_counter(); ref.ray_trace(ro, rd); dt = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            ref.ray_trace(ro, rd, threads=nthr) if kind == "reference" else ref.ray_trace(ro, rd)
+            dt = time.perf_counter() - t0
             n = len(ro)
         else:
             p = np.ascontiguousarray(args[0][::stride])
+            kw = {"threads": nthr} if kind == "reference" else {}
             t0 = time.perf_counter()
             if op in ("sdf_watertight", "sdf_raystab"):
-                ref.signed_distance(p, mode=0 if op == "sdf_watertight" else 1)
+                if kind == "reference":  # raystab seeds each query's stab rays with its index in the call
+                    ref.signed_distance(args[0], mode=0 if op == "sdf_watertight" else 1, stride=stride, **kw)
+                else:
+                    ref.signed_distance(p, mode=0 if op == "sdf_watertight" else 1)
             else:
-                ref.unsigned_distance(p, return_uvw=(op == "udf_uvw"))
+                ref.unsigned_distance(p, return_uvw=(op == "udf_uvw"), **kw)
             dt = time.perf_counter() - t0
             n = len(p)
         q += n; t += dt
         parts.append(f"{op}: {n} of {len(args[0])}")
-    return q, t, O.threads(), "every %d-th query (%s)" % (stride, "; ".join(parts))
+    src = ("the reference's own host traversals (src/bvh.cu, oracle/_ref)" if kind == "reference"
+           else "the oracle's FP32 restatement of the reference's traversals")
+    return q, t, nthr, "every %d-th query (%s); %s" % (stride, "; ".join(parts), src), kind
 
 
 def reference_cuda_floodfill(wl, steps, warmup):
@@ -340,20 +355,117 @@ def reference_cuda_floodfill(wl, steps, warmup):
             "occupancy_udf": f"oracle FP32 mirror of the reference traversal, {t_udf:.1f} s on the host cores"}
 
 
+def reference_cuda_queries(wl, steps, warmup, dev=None):
+    """The reference's own CUDA query kernels (src/bvh.cu's launchers,
+    compiled unchanged into oracle/_ref/libref_bvh.so) on the workload's
+    query ops: one thread per query, 128-thread blocks, on the current
+    stream.  value: device-resident inputs and outputs, CUDA events around
+    each op; e2e: the reference API's own flow from pinned host tensors
+    (whole-array upload, kernel, whole-array download), CUDA events.  Its
+    BVH build and its lazy first-query upload are outside both."""
+    import torch
+    from oracle import oracle as O
+    if not O.ref_bvh_available():
+        return {"unavailable": "oracle/_ref/libref_bvh.so not built (needs the reference checkout)"}
+    if not torch.cuda.is_available():
+        return {"unavailable": "no CUDA device"}
+    dev = dev or torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    t0 = time.perf_counter()
+    R = O.ReferenceBVH(wl["vertices"], wl["faces"])
+    build_s = time.perf_counter() - t0
+    ops = []
+    for op, a in wl["ops"]:
+        if op in GRID_OPS:
+            continue
+        if op == "ray":
+            hin = [torch.from_numpy(a[0]).pin_memory(), torch.from_numpy(a[1]).pin_memory()]
+            n = hin[0].shape[0]
+            outs = [torch.empty(n, 3, device=dev), torch.empty(n, dtype=torch.int64, device=dev),
+                    torch.empty(n, device=dev)]
+
+            def call(di, o=outs, n=n):
+                R.ray_trace_gpu(di[0].data_ptr(), di[1].data_ptr(), n, o[0].data_ptr(), o[1].data_ptr(),
+                                o[2].data_ptr(), sp)
+        else:
+            hin = [torch.from_numpy(a[0]).pin_memory()]
+            n = hin[0].shape[0]
+            outs = [torch.empty(n, device=dev), torch.empty(n, dtype=torch.int64, device=dev)]
+            if op == "udf_uvw":
+                outs.append(torch.empty(n, 3, device=dev))
+            mode = {"sdf_watertight": 0, "sdf_raystab": 1}.get(op)
+
+            def call(di, o=outs, n=n, mode=mode):
+                u = o[2].data_ptr() if len(o) > 2 else 0
+                if mode is None:
+                    R.unsigned_distance_gpu(di[0].data_ptr(), n, o[0].data_ptr(), o[1].data_ptr(), u, sp)
+                else:
+                    R.signed_distance_gpu(di[0].data_ptr(), n, mode, o[0].data_ptr(), o[1].data_ptr(), u, sp)
+        din = [t.to(dev) for t in hin]
+        hout = [torch.empty(o.shape, dtype=o.dtype, pin_memory=True) for o in outs]
+        ops.append((op, n, call, din, hin, outs, hout))
+    if not ops:
+        return {}
+    for _ in range(max(1, warmup)):
+        for _, _, call, din, *_ in ops:
+            call(din)
+    torch.cuda.synchronize()
+    res, q, tot, tot_e2e = {}, 0, 0.0, 0.0
+    for op, n, call, din, hin, outs, hout in ops:
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ev[0].record(stream)
+        for _ in range(steps):
+            call(din)
+        ev[1].record(stream)
+        # the reference API's flow with host tensors: .cuda() of the inputs,
+        # the kernel, .cpu() of the outputs
+        ev[2].record(stream)
+        for _ in range(steps):
+            dd = [h.to(dev, non_blocking=True) for h in hin]
+            call(dd)
+            for o, h in zip(outs, hout):
+                h.copy_(o, non_blocking=True)
+        ev[3].record(stream)
+        torch.cuda.synchronize()
+        ms, ms_e2e = ev[0].elapsed_time(ev[1]) / steps, ev[2].elapsed_time(ev[3]) / steps
+        res[op] = {"queries": n, "ms_per_launch": ms, "queries_per_s": n / (ms / 1e3), "e2e_ms": ms_e2e}
+        q += n; tot += ms; tot_e2e += ms_e2e
+    return {"value": q / (tot / 1e3), "unit": "queries/s", "ms_per_step": tot,
+            "e2e": {"value": q / (tot_e2e / 1e3), "ms_per_step": tot_e2e,
+                    "host_buffers": "pinned, whole-array copies around each call"},
+            "steps": steps, "ops": res, "reference_build_s": build_s,
+            "kernels": "src/bvh.cu unsigned_distance_kernel / signed_distance_*_kernel / raytrace_kernel "
+                       "(1 thread per query, 128-thread blocks)"}
+
+
+def workload_config(wl, world):
+    """The `config` object both arms print (the same for the same workload)."""
+    q = sum(len(a[0]) for op, a in wl["ops"] if op not in GRID_OPS)
+    return {"workload": wl["name"], "description": wl["desc"], "queries_per_step": q,
+            "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"}
+
+
 def run_reference(args):
     rank, world, _ = _rank_info()
     if rank != 0:
         return
     wl = build_workload(args.workload, args.res, args.sdf_points, args.grid)
     ref_cuda = {}
+    try:
+        import torch
+        if torch.cuda.is_available():
+            ref_cuda = reference_cuda_queries(wl, max(3, min(args.steps, 5)), args.warmup)
+    except Exception as e:  # the CPU arm stands on its own
+        ref_cuda = {"unavailable": f"{type(e).__name__}: {e}"}
     if any(op == "floodfill" for op, _ in wl["ops"]):
         ref_cuda["floodfill"] = reference_cuda_floodfill(wl, args.steps, args.warmup)
-    per_step = 4 << 20        # bounded sample of the workload per step
-    for _ in range(args.warmup):
+    per_step = wl.get("cpu_sample", 16 << 20)   # the same bounded sample as the GPU arm's cpu_baseline
+    for _ in range(min(args.warmup, 1)):
         cpu_time_sample(wl, per_step)
     qs, ts = 0, 0.0
     for _ in range(args.steps):
-        q, t, thr, desc = cpu_time_sample(wl, per_step)
+        q, t, thr, desc, kind = cpu_time_sample(wl, per_step)
         qs += q; ts += t
     val = qs / ts
     line = {
@@ -361,8 +473,8 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * ts / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded meshes and queries)",
-        "config": {"workload": wl["name"], "description": wl["desc"], "sample": desc},
-        "cpu_baseline": {"value": val, "unit": "queries/s", "cores": thr, "kind": "port", "sample": desc},
+        "config": workload_config(wl, world),
+        "cpu_baseline": {"value": val, "unit": "queries/s", "cores": thr, "kind": kind, "sample": desc},
         "e2e": {"value": val, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     if ref_cuda:
@@ -590,7 +702,7 @@ def run_ours(args):
         # CPU-baseline leg: the reference's algorithm restated in oracle/ is
         # timed here (queries and its host BVH build) as a baseline beside
         # ours; nothing measured above runs through it
-        cpu_q, cpu_t, cpu_thr, cpu_desc = cpu_time_sample(wl, wl.get("cpu_sample", 16 << 20))
+        cpu_q, cpu_t, cpu_thr, cpu_desc, cpu_kind = cpu_time_sample(wl, wl.get("cpu_sample", 16 << 20))
         ops_detail = {"bvh_build": {"faces": int(len(wl["faces"])), "host_sah_s": build_host_s,
                                     "device_lbvh_s": build_dev_s, "reference_cpu_s": build_time_reference(wl)}}
         for i, (o, nq, _, kn) in enumerate(dev_ops):
@@ -609,15 +721,14 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded meshes and queries)",
-            "config": {"workload": wl["name"], "description": wl["desc"], "queries_per_step": q_per_step,
-                       "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
+            "config": workload_config(wl, world),
             "e2e": {"value": e2e_val, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "steps": e2e_steps},
             "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": _profile_traffic(op, wl["name"], n),
                          "algorithmic_bytes_per_launch": alg},
-            "cpu_baseline": {"value": cpu_q / cpu_t, "unit": "queries/s", "cores": cpu_thr, "kind": "port",
+            "cpu_baseline": {"value": cpu_q / cpu_t, "unit": "queries/s", "cores": cpu_thr, "kind": cpu_kind,
                              "sample": cpu_desc},
             "gpu_launches": gpu_launches,
             "clocks": clk.summary(),
@@ -813,8 +924,8 @@ def run_ours_fwd_bwd(args):
         }
         if args.workload == "grad_displaced":
             wl = build_workload("grad_displaced")
-            cq, ct, cthr, cdesc = cpu_time_sample(wl, 4 << 20)
-            line["cpu_baseline"] = {"value": cq / ct, "unit": "queries/s", "cores": cthr, "kind": "port",
+            cq, ct, cthr, cdesc, ckind = cpu_time_sample(wl, 4 << 20)
+            line["cpu_baseline"] = {"value": cq / ct, "unit": "queries/s", "cores": cthr, "kind": ckind,
                                     "sample": cdesc + " (forward only: the reference has no backward)"}
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -39,6 +39,7 @@ _SIGS = {
     "cubvh_ray_trace": [c_vp, c_vp, c_vp, c_i64, c_vp, c_vp, c_vp, c_vp],
     "cubvh_ray_trace_host": [c_vp, c_vp, c_vp, c_i64, c_vp, c_vp, c_vp, c_vp],
     "cubvh_signed_distance_host": [c_vp, c_vp, c_i64, c_u32, c_vp, c_vp, c_vp, c_vp],
+    "cubvh_stab_directions": [c_i64, c_i64, c_vp, c_vp],
     "cubvh_floodfill_workspace_size": [c_int, c_int, c_int, c_int, ctypes.POINTER(c_sz)],
     "cubvh_floodfill": [c_vp, c_int, c_int, c_int, c_int, c_vp, c_vp, c_sz, c_vp],
     "cubvh_floodfill_check": [c_vp, c_int, c_int, c_int, c_int, c_vp],

@@ -962,6 +962,22 @@ int cubvh_distance_backward(cubvh_bvh* h, const float* points, int64_t n, const 
     CUBVH_GUARD_END
 }
 
+int cubvh_stab_directions(int64_t first, int64_t n, float* dirs, void* stream) {
+    CUBVH_GUARD_BEGIN
+    if (n < 0 || first < 0) return fail(CUBVH_ERR_INVALID, "negative query index or count");
+    if (n == 0) return CUBVH_OK;
+    if (!dirs) return fail(CUBVH_ERR_INVALID, "dirs is null");
+    if (first + n > ((int64_t)1 << 32)) return fail(CUBVH_ERR_INVALID, "query indices beyond 2^32");
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    if ((e = ensure_constants(device)) != cudaSuccess) return cuda_fail(e, "constant upload");
+    if ((e = launch_stab_dirs(first, n, dirs, (cudaStream_t)stream)) != cudaSuccess)
+        return cuda_fail(e, "stab directions launch");
+    return CUBVH_OK;
+    CUBVH_GUARD_END
+}
+
 // Floodfill that allocates nothing: see include/cubvh_b200.h.
 int cubvh_floodfill_noalloc(const uint8_t* grid, int B, int H, int W, int D, int32_t* labels, void* stream) {
     CUBVH_GUARD_BEGIN

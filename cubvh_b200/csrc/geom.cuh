@@ -221,24 +221,10 @@ __device__ __forceinline__ float qf(uint32_t word, int byte) {
 __device__ __forceinline__ float exp2i(int e) { return __int_as_float((e + 127) << 23); }
 
 // ------------------------------------------------------------ stab directions
-// Coefficients (-1)^k/(2k+1)! and (-1)^k/(2k)! by a fixed IEEE division
-// sequence (filled from the host by upload_constants(); this header is
-// compiled into one translation unit only).
-static __constant__ double c_sin_coef[14];
-static __constant__ double c_cos_coef[14];
 // Lattice terms of direction k: (k + 1.33) / (31 + 2 * 1.33) at [k] and
 // k / golden ratio at [32 + k], float IEEE divisions done by the host (the
 // same values as computing them here); read per lane through L1.
 static __device__ float g_lattice[64];
-
-__device__ __forceinline__ void det_sincos(float phi, float* s, float* c) {
-    const double x = (double)phi, x2 = dM(x, x);
-    double ps = c_sin_coef[13], pc = c_cos_coef[13];
-#pragma unroll
-    for (int k = 12; k >= 0; --k) { ps = dA(dM(ps, x2), c_sin_coef[k]); pc = dA(dM(pc, x2), c_cos_coef[k]); }
-    *s = __double2float_rn(dM(ps, x));
-    *c = __double2float_rn(pc);
-}
 
 // pcg32 with the default state and stream, advanced by 2*i; two next_float
 // draws give the query's lattice offset.
@@ -265,17 +251,22 @@ __device__ __forceinline__ float2 stab_offset(uint32_t i) {
     return make_float2(__uint_as_float((u0 >> 9) | 0x3f800000u) - 1.0f,
                        __uint_as_float((u1 >> 9) | 0x3f800000u) - 1.0f);
 }
-// Direction k of the 32-ray Fibonacci lattice (epsilon 1.33) with offset.
+// Direction k of the 32-ray Fibonacci lattice (epsilon 1.33) with offset:
+// the reference's device arithmetic (include/gpu/common.h:63-96 compiled by
+// nvcc with its default contraction): cos(theta) = 1 - 2a, phi = 2 pi (b -
+// 0.5), sin(theta) = sqrt(max(fma(-cos, cos, 1), 0)), CUDA's sincosf for
+// phi, each product rounded on its own.  The directions equal the
+// reference's CUDA build bit for bit (tested against it).
 __device__ __forceinline__ float3 stab_dir(uint32_t k, float2 off) {
     float a = __fadd_rn(__ldg(&g_lattice[k]), off.x);
     a = __fsub_rn(a, floorf(a));
     float b = __fadd_rn(__ldg(&g_lattice[32 + k]), off.y);
     b = __fsub_rn(b, floorf(b));
-    const float cos_t = __fadd_rn(__fmul_rn(-2.0f, a), 1.0f);
+    const float cos_t = __fmaf_rn(-2.0f, a, 1.0f);  // -2a is exact: the same as a product and a sum
     const float phi = __fmul_rn(__fmul_rn(2.0f, 3.14159265358979323846f), __fsub_rn(b, 0.5f));
-    const float sin_t = __fsqrt_rn(fmaxf(__fsub_rn(1.0f, __fmul_rn(cos_t, cos_t)), 0.0f));
+    const float sin_t = __fsqrt_rn(fmaxf(__fmaf_rn(-cos_t, cos_t, 1.0f), 0.0f));
     float sp, cp;
-    det_sincos(phi, &sp, &cp);
+    sincosf(phi, &sp, &cp);
     return make_float3(__fmul_rn(sin_t, cp), __fmul_rn(sin_t, sp), cos_t);
 }
 

@@ -13,6 +13,8 @@ cudaError_t upload_constants();
 // upload_constants() once per device (the current one must be `device`):
 // every entry point that launches query kernels on a device calls it first.
 cudaError_t ensure_constants(int device);
+// Raystab stab directions of queries first .. first+n-1 into float [n, 32, 3].
+cudaError_t launch_stab_dirs(int64_t first, int64_t n, float* dirs, cudaStream_t stream);
 
 // Arena work descriptors (query.cu): a packet is up to 32 consecutive
 // positions of the (sorted) query order, all on one mesh.

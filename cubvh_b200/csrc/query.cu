@@ -1534,13 +1534,28 @@ cudaError_t launch_arena_distance(const ArenaLaunch& a, const float* pts, float*
 
 int cell_bits_for(int64_t n) { return cell_bits(n); }
 
-cudaError_t upload_constants() {
-    double s[14], c[14];
-    s[0] = 1.0; c[0] = 1.0;
-    for (int k = 1; k < 14; ++k) {
-        s[k] = -s[k - 1] / (double)((2 * k) * (2 * k + 1));
-        c[k] = -c[k - 1] / (double)((2 * k - 1) * (2 * k));
+// The raystab stab directions of queries first .. first+n-1 (inspection):
+// dirs[(i * 32 + k) * 3 + c], the same stab_dir values the sign pass uses.
+__global__ void k_stab_dirs(int64_t n, uint32_t first, float* __restrict__ dirs) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float2 off = stab_offset(first + (uint32_t)i);
+    float* o = dirs + i * 96;
+    for (uint32_t k = 0; k < 32; ++k) {
+        const float3 d = stab_dir(k, off);
+        o[3 * k] = d.x;
+        o[3 * k + 1] = d.y;
+        o[3 * k + 2] = d.z;
     }
+}
+
+cudaError_t launch_stab_dirs(int64_t first, int64_t n, float* dirs, cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    k_stab_dirs<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(n, (uint32_t)first, dirs); count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t upload_constants() {
     float lat[64];
     const volatile float eps = 1.33f, phi = 1.6180339887498948482045868343656f;
     const float den = 31.0f + 2.0f * eps;
@@ -1548,10 +1563,7 @@ cudaError_t upload_constants() {
         lat[k] = ((float)k + eps) / den;
         lat[32 + k] = (float)k / phi;
     }
-    cudaError_t e = cudaMemcpyToSymbol(c_sin_coef, s, sizeof(s));
-    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_cos_coef, c, sizeof(c));
-    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_lattice, lat, sizeof(lat));
-    return e;
+    return cudaMemcpyToSymbol(g_lattice, lat, sizeof(lat));
 }
 
 }  // namespace cubvh

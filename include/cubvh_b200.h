@@ -238,6 +238,15 @@ int cubvh_arena_distance(cubvh_arena* arena, const float* points, float* distanc
 int cubvh_arena_backward(cubvh_arena* arena, const float* points, const int64_t* face_id,
                          const float* grad_distances, const float* distances, float* grad_points, void* stream);
 
+/* Stab directions of the raystab sign (inspection; no entry point of the
+ * reference exposes them): for queries first .. first+n-1 of a call, float32
+ * [n, 32, 3] unit vectors d_k written to device memory `dirs` on `stream`;
+ * query i casts -d_k and +d_k for k = 0..31.  They are the reference's
+ * device directions bit for bit: pcg32 advanced by 2i, two next_float draws
+ * as the lattice offset, fibonacci_dir<32> with CUDA's sincosf
+ * (src/bvh.cu:408-427, 658-685; include/gpu/common.h:63-96). */
+int cubvh_stab_directions(int64_t first, int64_t n, float* dirs, void* stream);
+
 /* Floodfill of a batch of boolean grids: grid uint8/bool [B, H, W, D]
  * (nonzero = occupied), labels int32 [B, H, W, D]: -1 for occupied voxels,
  * else the smallest global linear index of the voxel's 6-connected free

@@ -387,34 +387,12 @@ void orc_stab_offsets(int64_t n, int64_t i0, float* out2) {
     }
 }
 
-// Deterministic sin/cos: Taylor series in double, Horner in x^2, fixed
-// operation order.  |x| <= pi.  Used so that the stab directions are a pure
-// function of the inputs (the CUDA kernels evaluate the identical sequence).
-// Coefficients by a fixed sequence of IEEE divisions (identical on every
-// IEEE-754 machine): s_k = (-1)^k / (2k+1)!, c_k = (-1)^k / (2k)!.
-struct SinCosCoef {
-    double s[14], c[14];
-    SinCosCoef() {
-        s[0] = 1.0; c[0] = 1.0;
-        for (int k = 1; k < 14; ++k) {
-            s[k] = -s[k - 1] / (double)((2 * k) * (2 * k + 1));
-            c[k] = -c[k - 1] / (double)((2 * k - 1) * (2 * k));
-        }
-    }
-};
-static const SinCosCoef SC;
-static inline void det_sincos(float phi, float* s, float* c) {
-    const double x = (double)phi, x2 = x * x;
-    double ps = SC.s[13], pc = SC.c[13];
-    for (int k = 12; k >= 0; --k) { ps = ps * x2 + SC.s[k]; pc = pc * x2 + SC.c[k]; }
-    *s = (float)(ps * x);
-    *c = (float)pc;
-}
-
 // fibonacci_dir<32> (include/gpu/common.h:63-96) in the reference's float
-// operation order; use_libm selects the host sincosf (reference CPU mirror)
-// instead of det_sincos (FP64 oracle, matches the CUDA kernels bit for bit).
-static inline void stab_dir(uint32_t i, float ox, float oy, bool use_libm, float out[3]) {
+// operation order with the host's sin / cos (what the reference's own host
+// build computes; its CUDA build calls the device sincosf and contracts
+// 1 - cos^2 into a fused multiply-add, so its directions can differ in the
+// last bit: the GPU tests pass those directions in as a table).
+static inline void stab_dir(uint32_t i, float ox, float oy, float out[3]) {
     const float eps = 1.33f;
     const float den = (float)31u + 2.0f * eps;
     float a = ((float)i + eps) / den + ox;
@@ -426,25 +404,24 @@ static inline void stab_dir(uint32_t i, float ox, float oy, bool use_libm, float
     const float cos_theta = -2.0f * a + 1.0f;
     const float phi = (2.0f * PI) * (b - 0.5f);
     const float sin_theta = std::sqrt(std::max(1.0f - cos_theta * cos_theta, 0.0f));
-    float sp, cp;
-    if (use_libm) { sp = std::sin(phi); cp = std::cos(phi); }
-    else det_sincos(phi, &sp, &cp);
+    const float sp = std::sin(phi), cp = std::cos(phi);
     out[0] = sin_theta * cp; out[1] = sin_theta * sp; out[2] = cos_theta;
 }
-void orc_stab_dirs(int64_t n, int64_t i0, int use_libm, float* out) {
+void orc_stab_dirs(int64_t n, int64_t i0, float* out) {
     for (int64_t k = 0; k < n; ++k) {
         float off[2];
         orc_stab_offsets(1, i0 + k, off);
         for (uint32_t r = 0; r < 32; ++r)
-            stab_dir(r, off[0], off[1], use_libm != 0, out + 3 * (32 * k + r));
+            stab_dir(r, off[0], off[1], out + 3 * (32 * k + r));
     }
 }
 
-// Raystab sign rule (src/bvh.cu:408-427) in double with the stab directions
-// above: negative iff all 64 rays (-d_k then +d_k, k = 0..31) hit within
-// [0, 1000).  i0 = index of the first point within its call.
+// Raystab sign rule (src/bvh.cu:408-427) in double: negative iff all 64 rays
+// (-d_k then +d_k, k = 0..31) hit within [0, 1000).  i0 = index of the
+// first point within its call.  dirs: float [n, 32, 3] stab directions of
+// the n points, or NULL for the host rule above (stab_dir).
 void orc_sdf_raystab64(const float* V, const int64_t* F, int64_t nf, const float* pts, int64_t n,
-                       int64_t i0, double eps_b, double eps_g,
+                       int64_t i0, double eps_b, double eps_g, const float* dirs,
                        double* sdist, int64_t* fid_out, int32_t* flags) {
     std::vector<double> dist(n);
     std::vector<int64_t> fid(n);
@@ -457,7 +434,8 @@ void orc_sdf_raystab64(const float* V, const int64_t* F, int64_t nf, const float
         bool inside = true, amb = false;
         for (uint32_t k = 0; k < 32 && inside; ++k) {
             float dir[3];
-            stab_dir(k, off[0], off[1], false, dir);
+            if (dirs) for (int c = 0; c < 3; ++c) dir[c] = dirs[(32 * i + k) * 3 + c];
+            else stab_dir(k, off[0], off[1], dir);
             const float ndir[3] = {-dir[0], -dir[1], -dir[2]};
             if (!any_hit64(V, F, nf, p, d3(ndir), 1000.0, eps_b, eps_g, &amb)) { inside = false; break; }
             if (!any_hit64(V, F, nf, p, d3(dir), 1000.0, eps_b, eps_g, &amb)) { inside = false; break; }
@@ -950,7 +928,7 @@ void orc_ref_sdf(void* h, const float* pts, int64_t n, int mode, float* dist, in
             bool inside = true;
             for (uint32_t k = 0; k < 32 && inside; ++k) {
                 float dir[3];
-                stab_dir(k, off[0], off[1], true, dir);
+                stab_dir(k, off[0], off[1], dir);
                 const F3 d{dir[0], dir[1], dir[2]}, nd{-dir[0], -dir[1], -dir[2]};
                 if (ref_ray(B, p, nd, cp_).first < 0 || ref_ray(B, p, d, cp_).first < 0) inside = false;
             }

@@ -116,12 +116,19 @@ def sdf_watertight64(V, F, pts):
     return sd, fid, fl
 
 
-def sdf_raystab64(V, F, pts, i0=0, eps_b=1e-9, eps_g=1e-9):
+def sdf_raystab64(V, F, pts, i0=0, eps_b=1e-9, eps_g=1e-9, dirs=None):
+    """Raystab signed distance in double.  dirs: float32 [n, 32, 3] stab
+    directions of the n points (e.g. the reference's CUDA directions from
+    ref_stab_dirs_gpu_ptr), or None for the host rule (stab_dirs)."""
     V, F, pts = _f32(V), _i64(F), _f32(pts)
     n = len(pts)
+    if dirs is not None:
+        dirs = _f32(dirs)
+        if dirs.shape != (n, 32, 3):
+            raise ValueError("dirs must be [n, 32, 3]")
     sd = np.empty(n, np.float64); fid = np.empty(n, np.int64); fl = np.empty(n, np.int32)
     lib().orc_sdf_raystab64(_p(V), _p(F), I64(len(F)), _p(pts), I64(n), I64(i0), F64(eps_b),
-                            F64(eps_g), _p(sd), _p(fid), _p(fl))
+                            F64(eps_g), _p(dirs), _p(sd), _p(fid), _p(fl))
     return sd, fid, fl
 
 
@@ -137,9 +144,11 @@ def stab_offsets(n, i0=0):
     return out
 
 
-def stab_dirs(n, i0=0, use_libm=False):
+def stab_dirs(n, i0=0):
+    """Stab directions [n, 32, 3] of points i0 .. i0+n-1 with the host's
+    sin / cos (the reference's host build gives the same bits)."""
     out = np.empty((n, 32, 3), np.float32)
-    lib().orc_stab_dirs(I64(n), I64(i0), ctypes.c_int(1 if use_libm else 0), _p(out))
+    lib().orc_stab_dirs(I64(n), I64(i0), _p(out))
     return out
 
 

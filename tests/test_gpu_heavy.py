@@ -41,14 +41,14 @@ def test_heavy_udf_uvw(oracle, dev):
 
 
 @pytest.mark.parametrize("mode", ["watertight", "raystab"])
-def test_heavy_signed(oracle, dev, mode):
+def test_heavy_signed(oracle, dev, stab_dirs, mode):
     v, f = W.displaced_icosphere(3, 1)
     pts = np.concatenate([_centre_points(2500, 0.1, 2), W.uniform_points(4000, 3)])
     d, fid, _ = cubvh.cuBVH(v, f).signed_distance(torch.from_numpy(pts).to(dev), mode=mode)
     if mode == "watertight":
         sd, ofid, _ = oracle.sdf_watertight64(v, f, pts)
     else:
-        sd, ofid, _ = oracle.sdf_raystab64(v, f, pts)
+        sd, ofid, _ = oracle.sdf_raystab64(v, f, pts, dirs=stab_dirs(len(pts)))
     assert np.array_equal(_np(fid), ofid)
     assert np.array_equal(_np(d), sd.astype(np.float32))
     assert (_np(d)[:2500] < 0).all()
@@ -63,7 +63,7 @@ def test_heavy_many(oracle, dev):
     _check_udf(oracle, v, f, pts[sub], (d[sub], fid[sub], uvw[sub]))
 
 
-def test_heavy_in_arena(oracle, dev):
+def test_heavy_in_arena(oracle, dev, stab_dirs):
     meshes = [W.icosphere(4, 0.8), W.torus(0.5, 0.2, 48, 16), W.displaced_icosphere(3, 5)]
     meshes = [(np.asarray(v, np.float32), np.asarray(f, np.int64)) for v, f in meshes]
     qs = [_centre_points(2000, 0.05, 6), W.uniform_points(5000, 7), _centre_points(1500, 0.1, 8)]
@@ -75,7 +75,7 @@ def test_heavy_in_arena(oracle, dev):
     for m, ((v, f), q) in enumerate(zip(meshes, qs)):
         sl = slice(off[m], off[m + 1])
         if m == 2:
-            sd, ofid, _ = oracle.sdf_raystab64(v, f, q)
+            sd, ofid, _ = oracle.sdf_raystab64(v, f, q, dirs=stab_dirs(len(q)))
             want = sd.astype(np.float32)
         else:
             od, ofid, _, _, _ = oracle.udf64(v, f, q)

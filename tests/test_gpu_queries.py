@@ -221,7 +221,7 @@ def test_sdf_watertight(oracle, dev):
 
 
 @pytest.mark.parametrize("mesh", ["sphere", "tori"])
-def test_sdf_raystab(oracle, dev, mesh):
+def test_sdf_raystab(oracle, dev, stab_dirs, mesh):
     if mesh == "sphere":
         v, f = W.displaced_icosphere(3, 1)
     else:
@@ -231,7 +231,7 @@ def test_sdf_raystab(oracle, dev, mesh):
     pts = np.concatenate([rng.uniform(-1, 1, (1500, 3)).astype(np.float32),
                           W.surface_points(v, f, 1500, 0.02, rng)])
     got = bvh.signed_distance(torch.from_numpy(pts).to(dev), mode="raystab")
-    sd, fid, fl = oracle.sdf_raystab64(v, f, pts)
+    sd, fid, fl = oracle.sdf_raystab64(v, f, pts, dirs=stab_dirs(len(pts)))
     check_sdf(got, sd, fid, "raystab")
     assert got[2] is None
 

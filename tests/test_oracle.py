@@ -48,12 +48,20 @@ def test_stab_directions(oracle):
     assert d.shape == (64, 32, 3)
     n = np.linalg.norm(d.astype(np.float64), axis=-1)
     assert np.abs(n - 1).max() < 1e-6
-    # the deterministic sine/cosine agrees with the C library to float rounding
-    dl = oracle.stab_dirs(64, 0, use_libm=True)
-    assert np.abs(d - dl).max() < 4e-7
+    # the Fibonacci lattice: cos(theta) = 1 - 2 * frac((k + 1.33) / 33.66 + offset.x)
+    off = oracle.stab_offsets(64)
+    k = np.arange(32, dtype=np.float32)
+    a = (k + np.float32(1.33)) / (np.float32(31) + np.float32(2) * np.float32(1.33)) + off[:, :1]
+    a = a - np.floor(a)
+    assert np.array_equal(d[..., 2], np.float32(-2) * a + np.float32(1))
+    # a direction table given to the raystab oracle replaces the host rule
+    v, f = cube_mesh()
+    pts = np.array([[0.1, 0.2, 0.3], [3.0, 0.0, 0.0]], np.float32)
+    s0, _, _ = oracle.sdf_raystab64(v, f, pts)
+    s1, _, _ = oracle.sdf_raystab64(v, f, pts, dirs=oracle.stab_dirs(2, 0))
+    assert np.array_equal(s0, s1) and s0[0] < 0 < s0[1]
     # per-query offsets differ (jump-ahead by 2 per query)
-    off = oracle.stab_offsets(4)
-    assert len(np.unique(off[:, 0])) == 4
+    assert len(np.unique(off[:4, 0])) == 4
 
 
 def test_udf64_cube_analytic(oracle):

@@ -104,7 +104,7 @@ def test_stride_sampling_matches_dense():
 
 def test_host_stab_directions_equal_oracle_libm():
     ref = O.ref_stab_dirs_host(2000, 12345)
-    assert np.array_equal(ref, O.stab_dirs(2000, 12345, use_libm=True))
+    assert np.array_equal(ref, O.stab_dirs(2000, 12345))
 
 
 def test_reference_build_accepts_torch_style_inputs():
