@@ -43,6 +43,9 @@ sys.path.insert(0, ROOT)
 METRIC = "mesh queries/s (ray_trace + signed_distance watertight), 1 B200"
 # ops over a voxel grid (no query count, no traversal)
 GRID_OPS = ("floodfill", "udf_to_sdf")
+# queries per step of the CPU legs (the reference's host traversals): both
+# arms time the same strided sample of the workload, about 4 s of CPU work
+CPU_SAMPLE = 4 << 20
 
 
 def _launches() -> int:
@@ -339,7 +342,19 @@ def reference_cuda_floodfill(wl, steps, warmup):
     res = next(a[0] for op, a in wl["ops"] if op == "floodfill")
     pts = next(a[0] for op, a in wl["ops"] if op == "udf")
     t0 = time.perf_counter()
-    udf = O.RefBVH(wl["vertices"], wl["faces"]).unsigned_distance(pts)[0]
+    if O.ref_bvh_available():   # the reference's own CUDA unsigned distance
+        R = O.ReferenceBVH(wl["vertices"], wl["faces"])
+        P = torch.from_numpy(pts).cuda()
+        d = torch.empty(len(pts), device=P.device)
+        fid = torch.empty(len(pts), dtype=torch.int64, device=P.device)
+        R.unsigned_distance_gpu(P.data_ptr(), len(pts), d.data_ptr(), fid.data_ptr(), 0,
+                                torch.cuda.current_stream().cuda_stream)
+        udf = d.cpu().numpy()
+        del P, d, fid
+        udf_src = "the reference's CUDA unsigned distance (oracle/_ref)"
+    else:
+        udf = O.RefBVH(wl["vertices"], wl["faces"]).unsigned_distance(pts)[0]
+        udf_src = "the oracle's FP32 restatement of the reference traversal on the host cores"
     t_udf = time.perf_counter() - t0
     grid = np.ascontiguousarray(udf.reshape(res, res, res) < np.float32(2.0 / res))
     for _ in range(max(1, warmup)):
@@ -352,7 +367,7 @@ def reference_cuda_floodfill(wl, steps, warmup):
     return {"e2e_ms": 1e3 * statistics.median(times), "steps": steps,
             "grid": f"{res}^3 occupancy udf < 2/{res}, blocked fraction {grid.mean():.4f}",
             "host_buffers": "pageable numpy arrays",
-            "occupancy_udf": f"oracle FP32 mirror of the reference traversal, {t_udf:.1f} s on the host cores"}
+            "occupancy_udf": f"{udf_src}, {t_udf:.1f} s"}
 
 
 def reference_cuda_queries(wl, steps, warmup, dev=None):
@@ -460,7 +475,7 @@ def run_reference(args):
         ref_cuda = {"unavailable": f"{type(e).__name__}: {e}"}
     if any(op == "floodfill" for op, _ in wl["ops"]):
         ref_cuda["floodfill"] = reference_cuda_floodfill(wl, args.steps, args.warmup)
-    per_step = wl.get("cpu_sample", 16 << 20)   # the same bounded sample as the GPU arm's cpu_baseline
+    per_step = wl.get("cpu_sample", CPU_SAMPLE)   # the same bounded sample as the GPU arm's cpu_baseline
     for _ in range(min(args.warmup, 1)):
         cpu_time_sample(wl, per_step)
     qs, ts = 0, 0.0
@@ -480,6 +495,91 @@ def run_reference(args):
     if ref_cuda:
         line["reference_cuda"] = ref_cuda
     print(json.dumps(line), flush=True)
+
+
+def parity_sample(wl, op_outs, per_op=4096):
+    """Outside the timed region: the last step's outputs of each query op on
+    a strided sample of per_op queries against the FP64 brute-force oracle
+    (distances / depths within 1e-6 relative + 1e-7 absolute, face ids equal,
+    signs equal)."""
+    from oracle import oracle as O
+    rec = {}
+    v, f = wl["vertices"], wl["faces"]
+    for op, a in wl["ops"]:
+        if op not in op_outs:
+            continue
+        n = len(a[0])
+        stride = max(1, n // per_op)
+        if stride % 2 == 0:
+            stride += 1      # odd strides cross image rows and grid lines
+        idx = np.arange(0, n, stride)
+        outs = [t[idx.tolist()].cpu().numpy() if t is not None else None for t in op_outs[op]]
+        if op == "ray":
+            t64, f64, _ = O.ray64(v, f, a[0][idx], a[1][idx])
+            got_d, got_f = outs[2].astype(np.float64), outs[1]
+            want_d, hit = t64, f64 >= 0
+            sign_ok = True
+        else:
+            if op == "sdf_watertight":
+                want, f64, _ = O.sdf_watertight64(v, f, a[0][idx])
+            elif op == "sdf_raystab":
+                want, f64, _ = O.sdf_raystab64(v, f, a[0][idx], i0=0, dirs=_stab_dirs_sample(idx))
+            else:
+                want, f64, _, _, _ = O.udf64(v, f, a[0][idx])
+            got_d, got_f = outs[0].astype(np.float64), outs[1]
+            sign_ok = bool(np.array_equal(np.signbit(outs[0]), np.signbit(want.astype(np.float32))))
+            want_d, hit = np.abs(want), np.ones(len(idx), bool)
+            got_d = np.abs(got_d)
+        err = np.abs(got_d - want_d)[hit]
+        rel = err / np.maximum(want_d[hit], 1e-300)
+        within = bool((err <= 1e-7 + 1e-6 * want_d[hit]).all())
+        rec[op] = {"sample": int(len(idx)), "stride": int(stride), "max_abs_err": float(err.max()) if err.size else 0.0,
+                   "max_rel_err": float(rel.max()) if rel.size else 0.0, "within_tolerance": within,
+                   "face_id_equal": bool(np.array_equal(got_f, f64)), "signs_equal": sign_ok}
+    return rec
+
+
+def _stab_dirs_sample(idx):
+    """Stab directions of queries idx (the reference's device directions
+    where oracle/_ref is built, else this library's, equal to them)."""
+    import torch
+    from oracle import oracle as O
+    from cubvh_b200._lib import lib
+    out = np.empty((len(idx), 32, 3), np.float32)
+    buf = torch.empty(1, 32, 3, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    for k, i in enumerate(idx):
+        if O.ref_bvh_available():
+            O.ref_stab_dirs_gpu_ptr(int(i), 1, buf.data_ptr(), s)
+        else:
+            lib().cubvh_stab_directions(int(i), 1, ctypes.c_void_p(buf.data_ptr()), ctypes.c_void_p(s))
+        out[k] = buf[0].cpu().numpy()
+    return out
+
+
+# the other configurations, each in a process of its own after the headline
+CONFIG_RUNS = [("C0", ["--workload", "udf_icosphere"]), ("C2", ["--workload", "dense_tori"]),
+               ("C3", ["--workload", "grad_displaced", "--adam-steps", "50"]), ("C4", ["--workload", "batch_256"])]
+
+
+def run_config_records(args):
+    """Runs bench.py once per other configuration (C0, C2, C3, C4) with this
+    run's --steps / --warmup and returns their JSON lines, keyed by config."""
+    out = {}
+    for key, extra in CONFIG_RUNS:
+        cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--steps", str(args.steps), "--warmup",
+               str(args.warmup), "--no-configs"] + extra
+        t0 = time.perf_counter()
+        try:
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+            lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+            rec = json.loads(lines[-1]) if r.returncode == 0 and lines else {
+                "failed": f"exit {r.returncode}", "stderr_tail": r.stderr[-2000:]}
+        except subprocess.TimeoutExpired:
+            rec = {"failed": "timeout after 900 s"}
+        rec["wall_s"] = time.perf_counter() - t0
+        out[key] = rec
+    return out
 
 
 # -------------------------------------------------------------- GPU arm
@@ -509,6 +609,7 @@ def run_ours(args):
 
     # device-resident inputs / outputs
     dev_ops = []
+    op_outs = {}
     for op, a in wl["ops"]:
         if op == "ray":
             ro = torch.from_numpy(a[0]).to(dev); rd = torch.from_numpy(a[1]).to(dev)
@@ -518,6 +619,7 @@ def run_ours(args):
             fn = (lambda ro=ro, rd=rd, n=n, o=outs: check(
                 L.cubvh_ray_trace(h, P(ro), P(rd), n, P(o[0]), P(o[1]), P(o[2]), sp), "ray_trace"))
             dev_ops.append((op, n, fn, "ray: k_ray"))
+            op_outs[op] = outs
         elif op in ("sdf_watertight", "sdf_raystab", "udf", "udf_uvw"):
             p = torch.from_numpy(a[0]).to(dev)
             n = p.shape[0]
@@ -537,6 +639,7 @@ def run_ours(args):
                     L.cubvh_unsigned_distance(h, P(p), n, P(d), P(fid), u, sp), "udf"))
                 kname = "%s: Morton bucketing + k_udf<%d,0>" % (op, 1 if uvw is not None else 0)
             dev_ops.append((op, n, fn, kname))
+            op_outs[op] = (d, fid, uvw)
             if args.workload == "dense_tori":
                 occ_src = d
         elif op == "udf_to_sdf":
@@ -702,7 +805,7 @@ def run_ours(args):
         # CPU-baseline leg: the reference's algorithm restated in oracle/ is
         # timed here (queries and its host BVH build) as a baseline beside
         # ours; nothing measured above runs through it
-        cpu_q, cpu_t, cpu_thr, cpu_desc, cpu_kind = cpu_time_sample(wl, wl.get("cpu_sample", 16 << 20))
+        cpu_q, cpu_t, cpu_thr, cpu_desc, cpu_kind = cpu_time_sample(wl, wl.get("cpu_sample", CPU_SAMPLE))
         ops_detail = {"bvh_build": {"faces": int(len(wl["faces"])), "host_sah_s": build_host_s,
                                     "device_lbvh_s": build_dev_s, "reference_cpu_s": build_time_reference(wl)}}
         for i, (o, nq, _, kn) in enumerate(dev_ops):
@@ -716,6 +819,16 @@ def run_ours(args):
             if o == "floodfill" and ff_host_ms is not None:
                 d["e2e_host_pageable_ms"] = ff_host_ms
             ops_detail[o] = d
+        parity = parity_sample(wl, op_outs)
+        ref_cuda = None
+        if world == 1:
+            ref_cuda = reference_cuda_queries(wl, max(3, min(args.steps, 5)), 1, dev)
+            for o, r in (ref_cuda.get("ops") or {}).items():
+                if o in ops_detail:
+                    ops_detail[o]["reference_cuda_ms_per_launch"] = r["ms_per_launch"]
+                    ops_detail[o]["speedup_vs_reference_cuda"] = r["ms_per_launch"] / ops_detail[o]["ms_per_launch"]
+            if any(op == "floodfill" for op, _ in wl["ops"]):
+                ref_cuda["floodfill"] = reference_cuda_floodfill(wl, 3, 1)
         line = {
             "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -733,7 +846,12 @@ def run_ours(args):
             "gpu_launches": gpu_launches,
             "clocks": clk.summary(),
             "ops": ops_detail,
+            "parity": parity,
         }
+        if ref_cuda is not None:
+            line["reference_cuda"] = ref_cuda
+        if world == 1 and args.configs and args.workload == "rays_displaced":
+            line["configs"] = run_config_records(args)
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.barrier()
@@ -849,11 +967,37 @@ def run_ours_fwd_bwd(args):
                 d.sum().backward()
 
         per_call()
-        pc_ms = _timed(per_call, 1, stream)
+        pc_ms = _timed(per_call, 3, stream)
+        # the reference's own CUDA kernels, one call per mesh (forward only:
+        # the reference has no backward), inputs already on the device
+        ref_pc = None
+        from oracle import oracle as O
+        if O.ref_bvh_available() and world == 1:
+            rbvhs = [O.ReferenceBVH(v, f) for v, f in meshes]
+            rout = [(torch.empty(len(q_), device=dev), torch.empty(len(q_), dtype=torch.int64, device=dev))
+                    for q_ in views]
+            sp_ = stream.cuda_stream
+
+            def ref_per_call():
+                for rb, q_, mode, (rd_, rf_) in zip(rbvhs, views, modes, rout):
+                    if mode == "unsigned":
+                        rb.unsigned_distance_gpu(q_.data_ptr(), q_.shape[0], rd_.data_ptr(), rf_.data_ptr(), 0, sp_)
+                    else:
+                        rb.signed_distance_gpu(q_.data_ptr(), q_.shape[0], 1, rd_.data_ptr(), rf_.data_ptr(), 0, sp_)
+
+            ref_per_call()
+            ref_pc = _timed(ref_per_call, 3, stream)
+            del rbvhs, rout
         desc = (f"{len(ms)} meshes (displaced icospheres L2-7 / tori, {sum(len(f) for _, f in meshes):,} faces), "
                 f"{nq:,} queries (10k-2M per mesh, log-uniform), even meshes unsigned, odd raystab; fwd + bwd")
         kname = "batched fwd_bwd: arena bucketing + k_udf + k_sign_raystab + k_arena_backward_points"
-        extra["per_call"] = {"ms_per_step": pc_ms, "queries_per_s": nq / (pc_ms / 1e3)}
+        extra["per_call"] = {"ms_per_step": pc_ms, "queries_per_s": nq / (pc_ms / 1e3), "steps": 3,
+                             "what": "one cuBVH per mesh, one forward call and its backward each"}
+        if ref_pc is not None:
+            extra["per_call_reference_cuda"] = {
+                "ms_per_step": ref_pc, "queries_per_s": nq / (ref_pc / 1e3), "steps": 3,
+                "what": "the reference's own CUDA kernels (src/bvh.cu), one call per mesh, forward only "
+                        "(it has no backward)"}
         extra["autotune"] = {str(k): v for k, v in report.items()}
         # the same step on the arena built on the GPU (linear BVHs)
         arena_dev.set_queries(counts, modes, device=dev)
@@ -879,6 +1023,8 @@ def run_ours_fwd_bwd(args):
     value = world * nq / (ms_step / 1e3)
     if args.workload == "batch_256":
         extra["speedup_vs_per_call"] = extra["per_call"]["ms_per_step"] / ms_step
+        if "per_call_reference_cuda" in extra:
+            extra["speedup_vs_reference_per_call"] = extra["per_call_reference_cuda"]["ms_per_step"] / ms_step
     # e2e: host points in, gradients and distances back
     hp = pts.detach().cpu().pin_memory()
     hd = torch.empty(nq, pin_memory=True)
@@ -1036,6 +1182,9 @@ def main():
     ap.add_argument("--res", type=int, default=2048, help="camera resolution (rays_displaced)")
     ap.add_argument("--sdf-points", type=int, default=8 << 20, help="SDF queries (rays_displaced)")
     ap.add_argument("--grid", type=int, default=512, help="grid resolution (dense_tori)")
+    ap.add_argument("--no-configs", dest="configs", action="store_false",
+                    help="headline workload only (by default a 1-GPU run of the default workload also runs "
+                         "C0, C2, C3 and C4 and adds their lines under 'configs')")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -107,8 +107,8 @@ def test_stab_directions_equal_reference(dev):
         torch.cuda.synchronize()
         assert torch.equal(ours.view(torch.int32), ref.view(torch.int32)), f"first {first}"
     # the host build of the same code (host sincosf, no FMA) differs in the last bits
-    host = O.ref_stab_dirs_host(4096, 0)
-    _report("stab_directions", dict(queries=3 << 18, equal=True,
+    host = O.ref_stab_dirs_host(4096, first)
+    _report("stab_directions", dict(queries=3 << 18, equal=True, host_build_components_compared=host.size,
                                     host_build_components_differing=int((host != _np(ref[:4096])).sum())))
 
 
@@ -261,3 +261,37 @@ def test_c2_udf_and_floodfill_vs_reference(dev):
         assert np.array_equal(_np(labels), O.ref_floodfill(g))
         rec.update(floodfill_512_equal=True, blocked=int(g.sum()))
     _report("C2 udf 512^3 grid of 12 tori + floodfill", rec)
+
+
+# ------------------------------------------------ recorded reference outputs
+FIX = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_bvh.npz"))
+
+
+@pytest.mark.parametrize("name", ["dodeca", "ico3", "disp4", "tori3"])
+def test_ours_vs_recorded_reference(dev, stab_dirs, name):
+    """Our kernels on the fixture inputs against the reference's recorded CUDA
+    outputs (tests/golden/ref_bvh.npz): face ids equal except at FP64 ties,
+    signs equal except where FP64 sides with ours, hits equal except where
+    FP64 sides with ours."""
+    g = lambda k: FIX[f"{name}_{k}"]
+    v, f, pts = g("v"), g("f"), g("pts")
+    bvh = cubvh.cuBVH(v, f)
+    P = torch.from_numpy(pts).to(dev)
+    d, fid, uvw = map(_np, bvh.unsigned_distance(P, return_uvw=True))
+    rec = dict(udf=_face_mismatches(v, f, pts, fid, g("gpu_udf_fid")))
+    assert rec["udf"].get("ours_farther", 0) == 0
+    dirs = g("gpu_stab_dirs") if f"{name}_gpu_stab_dirs" in FIX.files else stab_dirs(len(pts))
+    for tag, mode in (("sdfw", "watertight"), ("sdfr", "raystab")):
+        sd, sfid, _ = map(lambda t: _np(t) if t is not None else None, bvh.signed_distance(P, mode=mode))
+        rec[tag] = _sign_disagreements(v, f, pts, sd, g(f"gpu_{tag}_d"), mode, dirs=dirs)
+        rec[tag].update(_face_mismatches(v, f, pts, sfid, g(f"gpu_{tag}_fid")))
+        assert rec[tag].get("ours_farther", 0) == 0
+    _, rfid, rdep = map(_np, bvh.ray_trace(torch.from_numpy(g("ro")).to(dev), torch.from_numpy(g("rd")).to(dev)))
+    mm = np.nonzero(rfid != g("gpu_ray_fid"))[0]
+    rec["ray"] = dict(face_mismatch=int(len(mm)))
+    if len(mm):
+        t64, f64, fl = O.ray64(v, f, g("ro")[mm], g("rd")[mm])
+        assert ((rfid[mm] == f64) | ((fl & 1) != 0)).all()
+        rec["ray"].update(ours_equal_fp64=int((rfid[mm] == f64).sum()),
+                          ref_equal_fp64=int((g("gpu_ray_fid")[mm] == f64).sum()))
+    _report(f"recorded reference outputs: {name}", rec)

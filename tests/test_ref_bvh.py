@@ -13,6 +13,8 @@ reference's CUDA kernels are in test_gpu_ref_bvh.py).
   host build's.
 """
 
+import os
+
 import numpy as np
 import pytest
 import torch
@@ -113,3 +115,62 @@ def test_reference_build_accepts_torch_style_inputs():
     assert R.n_nodes > 0
     with pytest.raises(ValueError):
         O.ReferenceBVH(v, f + len(v))
+
+
+# ------------------------------------------------ recorded reference outputs
+# tests/golden/ref_bvh.npz: the reference's CUDA kernels and host build on four
+# cases (make_ref_bvh.py beside it), including its test's own dodecahedron.
+FIX = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_bvh.npz"))
+FIX_CASES = ["dodeca", "ico3", "disp4", "tori3"]
+
+
+@pytest.mark.parametrize("name", FIX_CASES)
+def test_reference_host_build_reproduces_fixture(name):
+    """The live host build of the reference (this checkout's oracle/_ref) gives
+    the recorded host outputs bit for bit."""
+    g = lambda k: FIX[f"{name}_{k}"]
+    R = O.ReferenceBVH(g("v"), g("f"))
+    for tag, mode in (("udf", None), ("sdfw", 0), ("sdfr", 1)):
+        d, fid, uvw = (R.unsigned_distance(g("pts"), return_uvw=True) if mode is None
+                       else R.signed_distance(g("pts"), mode, return_uvw=True))
+        assert np.array_equal(d, g(f"host_{tag}_d")) and np.array_equal(fid, g(f"host_{tag}_fid"))
+        assert np.array_equal(uvw, g(f"host_{tag}_uvw"))
+    pos, fid, dep = R.ray_trace(g("ro"), g("rd"))
+    assert np.array_equal(fid, g("host_ray_fid")) and np.array_equal(dep, g("host_ray_depth"))
+
+
+@pytest.mark.parametrize("name", FIX_CASES)
+def test_oracle_agrees_with_recorded_reference(oracle, name):
+    """The FP64 oracle against the reference's recorded CUDA outputs: face ids
+    differ only at ties (FP64 distances within 1e-7), distances and depths
+    within the reference's FP32 error, signs equal except on points within
+    1e-6 of the surface (where FP32 cannot decide)."""
+    g = lambda k: FIX[f"{name}_{k}"]
+    v, f, pts = g("v"), g("f"), g("pts")
+    od, ofid, _, _, _ = oracle.udf64(v, f, pts)
+    rfid = g("gpu_udf_fid")
+    mm = ofid != rfid
+    if mm.any():
+        a, _ = oracle.face_dist64(v, f, pts[mm], rfid[mm])
+        assert np.abs(a - od[mm]).max() <= 1e-7
+    assert np.abs(g("gpu_udf_d").astype(np.float64) - od).max() < 1e-6
+    sw, _, _ = oracle.sdf_watertight64(v, f, pts)
+    far = np.abs(sw) > 1e-6
+    assert np.array_equal(np.signbit(g("gpu_sdfw_d"))[far], (sw < 0)[far])
+    t, rf, _ = oracle.ray64(v, f, g("ro"), g("rd"))
+    hit = rf >= 0
+    assert np.array_equal(hit, g("gpu_ray_fid") >= 0)
+    assert np.abs(g("gpu_ray_depth")[hit].astype(np.float64) - t[hit]).max() < 1e-5
+    if f"{name}_gpu_stab_dirs" in FIX.files:
+        sr, _, _ = oracle.sdf_raystab64(v, f, pts, dirs=g("gpu_stab_dirs"))
+        far = np.abs(sr) > 1e-6
+        assert np.array_equal(np.signbit(g("gpu_sdfr_d"))[far], (sr < 0)[far])
+
+
+def test_fixture_dodecahedron_is_the_reference_tests():
+    """The dodecahedron case is the reference test's own solid: 20 vertices on
+    the unit sphere, 36 faces, every vertex used."""
+    v, f = FIX["dodeca_v"], FIX["dodeca_f"]
+    assert v.shape == (20, 3) and f.shape == (36, 3)
+    assert np.allclose(np.linalg.norm(v, axis=1), 1.0, atol=1e-6)
+    assert np.array_equal(np.unique(f), np.arange(20))
