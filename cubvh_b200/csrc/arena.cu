@@ -383,6 +383,8 @@ int cubvh_arena_set_queries(cubvh_arena* a, const int64_t* query_offsets, const 
     const size_t o_slots = off; off += al(sizeof(int32_t) * std::max<int64_t>(Q, 1));
     const int64_t hcap = heavy_cap_for(std::max<int64_t>(Q, 1));
     const size_t o_heavy = off; off += al(sizeof(uint2) * hcap);
+    const int64_t n_rs_q = (int64_t)rs.size() * 32;                // raystab candidates (second pass)
+    const size_t o_cand = off; off += al(sizeof(uint4) * std::max<int64_t>(n_rs_q, 1));
     std::lock_guard<std::mutex> lk(a->mu);
     if (a->d_layout) { cudaFree(a->d_layout); a->d_layout = nullptr; a->has_layout = false; }
     cudaError_t e = cudaMalloc(&a->d_layout, off);
@@ -415,6 +417,7 @@ int cubvh_arena_set_queries(cubvh_arena* a, const int64_t* query_offsets, const 
     L.slots = reinterpret_cast<int32_t*>(base + o_slots);
     L.heavy = reinterpret_cast<uint2*>(base + o_heavy);
     L.heavy_cap = hcap;
+    L.rs_cand = reinterpret_cast<uint4*>(base + o_cand);
     a->n_queries = Q;
     a->has_layout = true;
     return CUBVH_OK;

@@ -40,6 +40,7 @@ struct ArenaLaunch {
     unsigned long long* counters;      // 256 bytes
     uint32_t* order; uint32_t* hist; uint32_t* bsum; int32_t* slots;
     uint2* heavy; int64_t heavy_cap;   // heavy-query list (heavy_cap_for(n_queries) entries)
+    uint4* rs_cand;                    // raystab second-pass candidates (32 * n_rs_packets entries)
 };
 cudaError_t launch_arena_distance(const ArenaLaunch& a, const float* pts, float* dist, int64_t* fid, float* uvw,
                                   cudaStream_t stream);

@@ -25,6 +25,7 @@
 //    a local-memory stack with their lower-bound key, re-checked on pop.
 #include <climits>
 #include <cstdint>
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <math_constants.h>
 
@@ -1003,12 +1004,21 @@ __global__ void __launch_bounds__(kQBlock) k_sign_watertight_ovf(const uint32_t*
 // few, so lanes never wait for one another except at the end of a chunk.
 // The per-query setup (query index, stab stream offset, root) is computed by
 // the whole warp in lockstep when the chunk is taken.
+//
+// With max_rays < 64 this is the first of two passes: a query whose first
+// max_rays rays all hit is not finished here but appended to `cand` (query
+// index, stab offset, root: warp-aggregated atomic on cand_n), for
+// k_sign_raystab_lines.  Outside points mostly see their first rays miss
+// and end in this pass; the candidates are mostly inside points, which need
+// every ray.
 constexpr int kChunkMax = 2;  // packets per raystab chunk
 __global__ void __launch_bounds__(kQBlock) k_sign_raystab(Work w, const uint32_t* __restrict__ order,
                                                           const float* __restrict__ pts, float* __restrict__ dist,
                                                           const CNode* __restrict__ nodes,
                                                           const CTri* __restrict__ tris,
-                                                          unsigned long long* __restrict__ ctr, int64_t grab) {
+                                                          unsigned long long* __restrict__ ctr, int64_t grab,
+                                                          int max_rays, uint4* __restrict__ cand,
+                                                          unsigned long long* __restrict__ cand_n) {
     __shared__ int s_next[kQBlock / 32];
     __shared__ uint4 s_q[kQBlock / 32][kChunkMax * 32];  // query index, offset x/y bits, root (-1: none)
     const int wib = threadIdx.x >> 5;
@@ -1093,6 +1103,16 @@ __global__ void __launch_bounds__(kQBlock) k_sign_raystab(Work w, const uint32_t
                     idx = -1;
                     continue;
                 }
+                if ((int)r == max_rays) {  // first pass: the rest goes to k_sign_raystab_lines
+                    const cooperative_groups::coalesced_group g = cooperative_groups::coalesced_threads();
+                    unsigned long long b = 0;
+                    if (g.thread_rank() == 0) b = atomicAdd(cand_n, (unsigned long long)g.size());
+                    b = g.shfl(b, 0) + g.thread_rank();
+                    cand[b] = make_uint4((uint32_t)idx, __float_as_uint(off.x), __float_as_uint(off.y),
+                                         (uint32_t)root);
+                    idx = -1;
+                    continue;
+                }
                 if (r & 1) d = sd;
                 else { sd = stab_dir(r >> 1, off); d = make_float3(-sd.x, -sd.y, -sd.z); }
                 inv = ray_inv_approx(d);
@@ -1102,6 +1122,103 @@ __global__ void __launch_bounds__(kQBlock) k_sign_raystab(Work w, const uint32_t
                 st[sp++] = root;
             }
         }
+        __syncwarp();
+    }
+}
+
+// Second raystab pass: a warp per candidate query.  The query's rays
+// first_ray .. 63 (ray 2k = -d_k, ray 2k + 1 = +d_k, all from the query
+// point; the first pass traced the others) form a pool: lane l starts with
+// ray first_ray + l and, whenever its ray hits, takes the next ray of the
+// pool, so lanes stay busy until the pool is empty.  A ray that finds no hit
+// ends the query for the whole warp (__any_sync): the point is outside; when
+// the pool is empty and every lane's ray has hit, it is inside.  Each step
+// of a lane is one inner node or one triangle, so lanes at inner nodes and
+// lanes at leaves run steps of similar length side by side.  The rays of a
+// warp start at the same point, so the first levels of their walks read the
+// same nodes.  Warps take candidates from a counter in the order the first
+// pass appended them (near one another in space).
+__global__ void __launch_bounds__(kQBlock) k_sign_raystab_lines(const float* __restrict__ pts,
+                                                                float* __restrict__ dist,
+                                                                const CNode* __restrict__ nodes,
+                                                                const CTri* __restrict__ tris,
+                                                                const uint4* __restrict__ cand,
+                                                                const unsigned long long* __restrict__ cand_n,
+                                                                unsigned long long* __restrict__ next, int first_ray) {
+    __shared__ int s_pool[kQBlock / 32];
+    __shared__ float3 s_dir[kQBlock / 32][32];   // the query's stab directions d_0 .. d_31
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const unsigned long long n = *cand_n;
+    const float tmaxf = 1000.0f;
+    const float cull = cull_of(1000.0);
+    int st[kStack];
+    while (true) {
+        unsigned long long c = 0;
+        if (lane == 0) c = atomicAdd(next, 1ull);
+        c = __shfl_sync(kFull, c, 0);
+        if (c >= n) break;
+        const uint4 e = cand[c];
+        const int64_t idx = e.x;
+        const float2 off = make_float2(__uint_as_float(e.y), __uint_as_float(e.z));
+        const int root = (int)e.w;
+        const float3 p = load3(pts, idx);
+        if (lane == 0) s_pool[wib] = first_ray + 32;
+        s_dir[wib][lane] = stab_dir((uint32_t)lane, off);   // lane k: direction k
+        __syncwarp();
+        int ray = first_ray + lane;            // >= 64: this lane has no ray left
+        float3 d = make_float3(0.f, 0.f, 0.f), inv = d;
+        bool degen = false;
+        float dinf = 0.f;
+        int sp = 0, ls = 0, le = 0;            // stack; triangles [ls, le) of the current leaf
+        auto start_ray = [&]() {
+            const float3 sd = s_dir[wib][ray >> 1];
+            d = (ray & 1) ? sd : make_float3(-sd.x, -sd.y, -sd.z);
+            inv = ray_inv_approx(d);
+            degen = ray_degenerate(inv);
+            dinf = f3inf(d);
+            sp = 0;
+            st[sp++] = root;
+            ls = le = 0;
+        };
+        if (ray < 64) start_ray();
+        bool inside = false;
+        while (true) {
+            bool miss = false;
+            if (ray < 64) {
+                bool hit = false;
+                if (ls >= le) {
+                    if (sp == 0) {
+                        miss = true;
+                    } else {
+                        const int ref = st[--sp];
+                        if (ref >= 0) {
+                            const NodeView nd = load_node(nodes, ref);
+                            if (degen) push_ray_children<true>(nd, p, inv, cull, st, sp);
+                            else push_ray_children_affine(nd, p, inv, cull, st, sp);
+                        } else {
+                            leaf_range(ref, ls, le);
+                        }
+                    }
+                }
+                if (ls < le) {                 // one triangle of the current leaf
+                    const TriV t = load_tri(tris, ls++);
+                    float tt, terr;
+                    const int cl = ray_tri_f(p, d, dinf, t, tmaxf, &tt, &terr);
+                    if (cl == 1) hit = true;
+                    else if (cl < 0) {
+                        double t64;
+                        hit = ray_tri_d(to_d3(p), to_d3(d), to_d3(t.a), to_d3(t.b), to_d3(t.c), 1000.0, &t64);
+                    }
+                }
+                if (hit) {
+                    ray = atomicAdd(&s_pool[wib], 1);
+                    if (ray < 64) start_ray();
+                }
+            }
+            if (__any_sync(kFull, miss)) break;            // a stab ray left the mesh: outside
+            if (__all_sync(kFull, ray >= 64)) { inside = true; break; }
+        }
+        if (inside && lane == 0) dist[idx] = -dist[idx];
         __syncwarp();
     }
 }
@@ -1335,6 +1452,7 @@ size_t query_workspace_bytes(int mode, int64_t n) {
     if (mode > 0) b += al(sizeof(int32_t) * n);                   // winning slots
     if (mode == 1) b += al(sizeof(uint32_t) * n);                 // watertight overflow queue
     if (mode >= 0) b += al(sizeof(uint2) * heavy_cap_for(n));     // heavy-query list
+    if (mode == 2) b += al(sizeof(uint4) * n);                    // raystab candidates (second pass)
     return b;
 }
 
@@ -1354,6 +1472,25 @@ int64_t chunk_for(int64_t n, unsigned grid) {
     const int64_t packets = (n + 31) / 32;
     const int64_t warps = (int64_t)grid * (kQBlock / 32);
     return packets >= (int64_t)kChunkMax * warps ? kChunkMax : 1;
+}
+}  // namespace
+
+namespace {
+// Rays the first raystab pass traces per query before handing the query to
+// the second pass (a line of two rays per stab direction).
+constexpr int kRaystabFirstRays = 2;
+// The two raystab passes over the packets of `w` (n queries): counters ctr
+// (first pass), cand_n (candidates appended), lines_next (second-pass
+// queue); cand holds up to n candidates.
+void launch_raystab(const Work& w, int64_t n, const uint32_t* order, const float* pts, float* dist,
+                    const CNode* nodes, const CTri* tris, unsigned long long* ctr, uint4* cand,
+                    unsigned long long* cand_n, unsigned long long* lines_next, cudaStream_t stream) {
+    const unsigned g = persistent_grid(k_sign_raystab, n);
+    k_sign_raystab<<<g, kQBlock, 0, stream>>>(w, order, pts, dist, nodes, tris, ctr, chunk_for(n, g),
+                                              kRaystabFirstRays, cand, cand_n); count_launch();
+    const unsigned g2 = persistent_grid(k_sign_raystab_lines, n);
+    k_sign_raystab_lines<<<g2, kQBlock, 0, stream>>>(pts, dist, nodes, tris, cand, cand_n, lines_next,
+                                                     kRaystabFirstRays); count_launch();
 }
 }  // namespace
 
@@ -1388,6 +1525,7 @@ cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts
     if (mode == 1) w += al(sizeof(uint32_t) * n);
     uint2* heavy = reinterpret_cast<uint2*>(w);
     const int64_t hcap = heavy_cap_for(n);
+    w += al(sizeof(uint2) * hcap);
     const Work work{nullptr, nullptr, n, slot_face0, qbase};
 #define CUBVH_L(U, S) do { const unsigned g_ = persistent_grid(k_udf<U, S, false>, n); \
         const float ppw_ = packets_per_warp((n + 31) / 32, g_); \
@@ -1421,8 +1559,8 @@ cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts
                                                                 nullptr, nullptr, ctr + 1, grab_for(n, g)); count_launch();
         }
     } else if (mode == 2) {
-        const unsigned g = persistent_grid(k_sign_raystab, n);
-        k_sign_raystab<<<g, kQBlock, 0, stream>>>(work, order, pts, dist, nodes, tris, ctr + 1, chunk_for(n, g)); count_launch();
+        uint4* cand = reinterpret_cast<uint4*>(w);
+        launch_raystab(work, n, order, pts, dist, nodes, tris, ctr + 1, cand, ctr + 12, ctr + 13, stream);
     }
     return cudaGetLastError();
 }
@@ -1525,9 +1663,8 @@ cudaError_t launch_arena_distance(const ArenaLaunch& a, const float* pts, float*
     }
     if (a.n_rs_packets > 0) {
         const Work w{a.rs_packets, a.meshes, a.n_rs_packets, 0};
-        const unsigned gr = persistent_grid(k_sign_raystab, 32 * a.n_rs_packets);
-        k_sign_raystab<<<gr, kQBlock, 0, stream>>>(w, a.order, pts, dist, a.nodes, a.tris, a.counters + 2,
-                                                   chunk_for(32 * a.n_rs_packets, gr)); count_launch();
+        launch_raystab(w, 32 * a.n_rs_packets, a.order, pts, dist, a.nodes, a.tris, a.counters + 2, a.rs_cand,
+                       a.counters + 12, a.counters + 13, stream);
     }
     return cudaGetLastError();
 }
