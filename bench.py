@@ -100,6 +100,23 @@ def _profile_traffic(op: str, workload: str, n_queries: int = 0):
         return None
 
 
+def _profile_l2(op: str, workload: str):
+    """L2 figures of `op` from the committed ncu summary
+    profiles/l2_<workload>.json (a capture of a smaller case of the same
+    workload): L2 GB/s, L2 throughput as a fraction of its peak, and the
+    issue-active fraction of its kernels, time-weighted."""
+    path = os.path.join(ROOT, "profiles", f"l2_{workload}.json")
+    try:
+        with open(path) as fh:
+            e = json.load(fh)[op]
+        return {"gbs": e["l2_gbs"], "frac_of_l2_peak": e["lts_pct"] / 100.0,
+                "issue_active_frac": e["issue_active_pct"] / 100.0,
+                "kernels": sorted(e["kernels"]), "source": os.path.relpath(path, ROOT),
+                "case_queries": e["captured_queries"]}
+    except Exception:
+        return None
+
+
 class ClockSampler:
     """nvidia-smi sampling (every 100 ms) of SM clock and throttle reasons
     during a region.  The sampler is running before the region starts; a
@@ -829,6 +846,7 @@ def run_ours(args):
                     ops_detail[o]["speedup_vs_reference_cuda"] = r["ms_per_launch"] / ops_detail[o]["ms_per_launch"]
             if any(op == "floodfill" for op, _ in wl["ops"]):
                 ref_cuda["floodfill"] = reference_cuda_floodfill(wl, 3, 1)
+        l2 = _profile_l2(op, wl["name"])
         line = {
             "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -840,7 +858,11 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": _profile_traffic(op, wl["name"], n),
-                         "algorithmic_bytes_per_launch": alg},
+                         "algorithmic_bytes_per_launch": alg,
+                         "l2": l2, "l2_frac": l2["frac_of_l2_peak"] if l2 else None,
+                         "note": "achieved counts the reference traversal's bytes (query I/O + 24 B per box + "
+                                 "36 B per triangle test) against the HBM copy bandwidth; the BVH is L1/L2-"
+                                 "resident, so l2 (ncu) shows the kernels' own L2 load and issue figures"},
             "cpu_baseline": {"value": cpu_q / cpu_t, "unit": "queries/s", "cores": cpu_thr, "kind": cpu_kind,
                              "sample": cpu_desc},
             "gpu_launches": gpu_launches,
