@@ -393,17 +393,19 @@ def floodfill(grid, check_bounds: bool = True):
     return mask.squeeze(0) if squeeze else mask
 
 
-def sparse_marching_cubes(coords, corners, iso, ensure_consistency=False):
+def sparse_marching_cubes(coords, corners, iso, ensure_consistency=False, triangulation="reference"):
     # coords: torch.Tensor, int32, [N, 3] voxel coordinates
     # corners: torch.Tensor, float32, [N, 8] corner values, corner order
     #   (0,0,0), (1,0,0), (1,1,0), (0,1,0), (0,0,1), (1,0,1), (1,1,1), (0,1,1)
     # iso: float; ensure_consistency: average the values of shared corners first
+    # triangulation: "reference" (default): the reference's marching-cubes
+    #   case table, so vertices and triangles equal the reference's index for
+    #   index; "closed": this library's own triangulation, closed and
+    #   consistently oriented wherever the corner values agree (ambiguous
+    #   faces decided by their saddle)
     # return: vertices float32 [M, 3] (voxel units), triangles int32 [T, 3], on
-    # the GPU.  Same vertex array as the reference (one vertex per cut voxel
-    # edge, merged, sorted by edge); the triangulation is this library's own
-    # (closed and consistently oriented where the corner values agree; may
-    # split 4+-vertex polygons and ambiguous faces differently from the
-    # reference's table).  Mirrors cubvh/api.py:173-187.
+    # the GPU (one vertex per cut voxel edge, merged, sorted by edge).
+    # Mirrors cubvh/api.py:173-187.
     coords = coords.int().contiguous()
     corners = corners.float().contiguous()
     if not coords.is_cuda: coords = coords.cuda()
@@ -412,13 +414,15 @@ def sparse_marching_cubes(coords, corners, iso, ensure_consistency=False):
             or coords.shape[0] != corners.shape[0]:
         raise RuntimeError(f"sparse_marching_cubes expects coords [N, 3] and corners [N, 8], got "
                            f"{tuple(coords.shape)} and {tuple(corners.shape)}")
+    if triangulation not in ("reference", "closed"):
+        raise ValueError(f"triangulation must be 'reference' or 'closed', got {triangulation!r}")
+    flags = (1 if ensure_consistency else 0) | (2 if triangulation == "closed" else 0)
     N = coords.shape[0]
     dev = coords.device
     with torch.cuda.device(dev):
         res = ctypes.c_void_p()
         nv, nt = ctypes.c_int64(), ctypes.c_int64()
-        check(lib().cubvh_sparse_marching_cubes(_ptr(coords), _ptr(corners), N, float(iso),
-                                                1 if ensure_consistency else 0, _stream_ptr(dev),
+        check(lib().cubvh_sparse_marching_cubes(_ptr(coords), _ptr(corners), N, float(iso), flags, _stream_ptr(dev),
                                                 ctypes.byref(res), ctypes.byref(nv), ctypes.byref(nt)),
               "sparse_marching_cubes")
         try:

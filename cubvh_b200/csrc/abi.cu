@@ -750,7 +750,8 @@ int cubvh_sparse_marching_cubes(const int32_t* coords, const float* corners, int
     }
     cudaGetDevice(&m->device);
     std::string err;
-    const int rc = sparse_mc_run(coords, corners, n, iso, ensure_consistency != 0, (cudaStream_t)stream, m->r, err);
+    const int rc = sparse_mc_run(coords, corners, n, iso, (ensure_consistency & CUBVH_SMC_ENSURE_CONSISTENCY) != 0,
+                                 (ensure_consistency & CUBVH_SMC_CLOSED) != 0, (cudaStream_t)stream, m->r, err);
     if (rc != 0) {
         cudaStreamSynchronize((cudaStream_t)stream);  // kernels may still write the result buffers
         cubvh_sparse_mc_free(m);

@@ -118,8 +118,10 @@ struct SparseMCResult {
     int32_t* tris = nullptr;
     int64_t n_verts = 0, n_tris = 0;
 };
+// closed: this library's own closed triangulation instead of the reference's
+// case table (sparse_mc.cu).
 int sparse_mc_run(const int32_t* coords, const float* corners, int64_t n, float iso, bool ensure_consistency,
-                  cudaStream_t stream, SparseMCResult& out, std::string& err);
+                  bool closed, cudaStream_t stream, SparseMCResult& out, std::string& err);
 void sparse_mc_release(SparseMCResult& r);
 
 }  // namespace cubvh

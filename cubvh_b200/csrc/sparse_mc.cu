@@ -14,24 +14,33 @@
 // averaging replaces every corner value by the mean over the voxels sharing
 // that corner.
 //
-// Triangulation (this file's own, no lookup table): on each cube face, walk
-// its corners counter-clockwise as seen from outside the cube; a segment of
-// the surface joins an edge where the walk enters the inside region to the
-// next edge where it leaves it.  A face with four cut edges (inside corners on
-// a diagonal) is resolved by the sign of its bilinear saddle (Nielson and
-// Hamann's asymptotic decider): the two inside corners are joined through the
-// face when the saddle value is below iso.  Both cubes sharing a face take the
-// same decision, so the surface is closed wherever the corner values agree.
-// Every cut edge is entered on one of its faces and left on the other, so the
-// segments form closed loops.  Each loop, started at its lowest edge, is cut
-// into a triangle fan from the first vertex none of whose diagonals joins two
-// edges of one face that the loop crosses twice (such a diagonal would lie in
-// that face and be shared with the neighbouring cube's triangles); when no
-// vertex qualifies, ears whose closing diagonal avoids such faces are clipped
-// one by one.  Triangles face from the inside (values below iso) to
-// the outside.  A cube with one corner inside gives the same triangle as the
-// reference; cubes whose polygons have four or more vertices, or that have
-// ambiguous faces, may be triangulated differently.
+// Triangulation.  By default the reference's: each voxel's triangles come
+// from the marching-cubes case table of its corner configuration (mc_cases.h,
+// recovered from the reference's own outputs for the 256 configurations:
+// tests/golden/make_ref_mc_cases.py), table triangle (e0, e1, e2) written as
+// vertices (e0, e2, e1), voxel by voxel, so the triangle array equals the
+// reference's index for index.  The table is the public marching-cubes case
+// table; its configurations with faces cut four times (the ambiguous cases)
+// are triangulated without looking at the face's saddle, so neighbouring
+// cubes can disagree and leave holes there.
+//
+// Optionally (flag kSmcClosed) this file's own triangulation, no lookup
+// table: on each cube face, walk its corners counter-clockwise as seen from
+// outside the cube; a segment of the surface joins an edge where the walk
+// enters the inside region to the next edge where it leaves it.  A face with
+// four cut edges (inside corners on a diagonal) is resolved by the sign of
+// its bilinear saddle (Nielson and Hamann's asymptotic decider): the two
+// inside corners are joined through the face when the saddle value is below
+// iso.  Both cubes sharing a face take the same decision, so the surface is
+// closed wherever the corner values agree.  Every cut edge is entered on one
+// of its faces and left on the other, so the segments form closed loops.
+// Each loop, started at its lowest edge, is cut into a triangle fan from the
+// first vertex none of whose diagonals joins two edges of one face that the
+// loop crosses twice (such a diagonal would lie in that face and be shared
+// with the neighbouring cube's triangles); when no vertex qualifies, ears
+// whose closing diagonal avoids such faces are clipped one by one.
+// Triangles face from the inside (values below iso) to the outside.  A cube
+// with one corner inside gives the same triangle as the table.
 #include <cstddef>
 #include <cstdint>
 #include <cub/cub.cuh>
@@ -42,6 +51,7 @@
 
 #include "launches.h"
 #include "kernels.h"
+#include "mc_cases.h"
 #include "scan.cuh"
 
 namespace cubvh {
@@ -148,12 +158,19 @@ __device__ __forceinline__ int n_triangles(const Cube& c, float iso) {
     return __popc(c.cut) - 2 * loops;
 }
 
-__global__ void k_smc_count(int64_t n, const float* __restrict__ corners, float iso, uint32_t* __restrict__ nv,
-                            uint32_t* __restrict__ nt) {
+// triangles of a corner configuration in the case table
+__device__ __forceinline__ int n_table_triangles(uint32_t inside) {
+    int t = 0;
+    while (t < 5 && c_mc_tri[inside][3 * t] >= 0) ++t;
+    return t;
+}
+
+__global__ void k_smc_count(int64_t n, const float* __restrict__ corners, float iso, bool table,
+                            uint32_t* __restrict__ nv, uint32_t* __restrict__ nt) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const Cube c = load_cube(corners, i, iso);
         nv[i] = __popc(c.cut);
-        nt[i] = (uint32_t)n_triangles(c, iso);
+        nt[i] = (uint32_t)(table ? n_table_triangles(c.inside) : n_triangles(c, iso));
     }
 }
 
@@ -169,8 +186,9 @@ __device__ __forceinline__ uint64_t pack_point(int x, int y, int z, const KeyPac
 // Vertices (position, edge key) in edge order and triangles (indices into
 // this launch's vertex list, before merging) of every voxel.
 __global__ void k_smc_emit(int64_t n, const int32_t* __restrict__ coords, const float* __restrict__ corners,
-                           float iso, const uint32_t* __restrict__ vpre, const uint32_t* __restrict__ tpre, KeyPack kp,
-                           float* __restrict__ pos, uint64_t* __restrict__ key, int32_t* __restrict__ tri) {
+                           float iso, bool table, const uint32_t* __restrict__ vpre, const uint32_t* __restrict__ tpre,
+                           KeyPack kp, float* __restrict__ pos, uint64_t* __restrict__ key,
+                           int32_t* __restrict__ tri) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const Cube c = load_cube(corners, i, iso);
         if (!c.cut) continue;
@@ -198,10 +216,23 @@ __global__ void k_smc_emit(int64_t n, const int32_t* __restrict__ coords, const 
             key[k] = pack_point(min(ax, bx), min(ay, by), min(az, bz), kp) * 3u + (uint64_t)axis;
             ++k;
         }
-        int8_t nxt[12];
-        surface_links(c, iso, nxt);
         uint32_t t_out = tpre[i];
         const uint32_t t_end = tpre[i + 1];  // the count pass's triangles: never write past them
+        auto vid = [&](int e) { return (int32_t)(vb + __popc(c.cut & ((1u << e) - 1u))); };
+        if (table) {
+            // the case table's triangles, written (e0, e2, e1) as the reference does
+            for (int t = 0; t < 5 && t_out < t_end; ++t) {
+                const int e0 = c_mc_tri[c.inside][3 * t];
+                if (e0 < 0) break;
+                tri[3 * t_out] = vid(e0);
+                tri[3 * t_out + 1] = vid(c_mc_tri[c.inside][3 * t + 2]);
+                tri[3 * t_out + 2] = vid(c_mc_tri[c.inside][3 * t + 1]);
+                ++t_out;
+            }
+            continue;
+        }
+        int8_t nxt[12];
+        surface_links(c, iso, nxt);
         // loops, in order of their lowest edge
         int8_t loop_of[12];
         int8_t seq[12];
@@ -235,7 +266,6 @@ __global__ void k_smc_emit(int64_t n, const int32_t* __restrict__ coords, const 
                 mark[e0] |= 1u << f; mark[e1] |= 1u << f; mark[e2] |= 1u << f; mark[e3] |= 1u << f;
             }
         }
-        auto vid = [&](int e) { return (int32_t)(vb + __popc(c.cut & ((1u << e) - 1u))); };
         for (int l = 0; l < nl && t_out < t_end; ++l) {
             const int b0 = start[l], L = start[l + 1] - start[l];
             int8_t* q = seq + b0;
@@ -453,7 +483,7 @@ struct AsyncTemps {
 // results stay in `out` (owned by the caller through cubvh_sparse_mc_*,
 // which releases them on an error return as well).
 int sparse_mc_run(const int32_t* coords, const float* corners, int64_t n, float iso, bool ensure_consistency,
-                  cudaStream_t s, SparseMCResult& out, std::string& err) {
+                  bool closed, cudaStream_t s, SparseMCResult& out, std::string& err) {
     out = SparseMCResult{};
     if (n <= 0) return 0;
     if (n > (int64_t)INT32_MAX / 12) { err = "too many voxels (the vertex count must fit in int32)"; return 1; }
@@ -509,7 +539,7 @@ int sparse_mc_run(const int32_t* coords, const float* corners, int64_t n, float 
     if ((e = tmp.get(&nv, n + 1)) != cudaSuccess || (e = tmp.get(&nt, n + 1)) != cudaSuccess ||
         (e = tmp.get(&bs, nb)) != cudaSuccess)
         return fail(e, "pool allocation");
-    k_smc_count<<<g, 256, 0, s>>>(n, use, iso, nv, nt); count_launch();
+    k_smc_count<<<g, 256, 0, s>>>(n, use, iso, !closed, nv, nt); count_launch();
     scan::exclusive(nv, bs, n, s);   // nv[n] = total
     scan::exclusive(nt, bs, n, s);
     uint32_t tot[2];
@@ -531,7 +561,7 @@ int sparse_mc_run(const int32_t* coords, const float* corners, int64_t n, float 
             (e = tmp.get(&bs2, nb2)) != cudaSuccess ||
             (e = pool_get(pool, s, &out.tris, (size_t)(3 * t))) != cudaSuccess)
             return fail(e, "sparse marching cubes buffers");
-        k_smc_emit<<<g, 256, 0, s>>>(n, coords, use, iso, nv, nt, kp, pos, key, out.tris); count_launch();
+        k_smc_emit<<<g, 256, 0, s>>>(n, coords, use, iso, !closed, nv, nt, kp, pos, key, out.tris); count_launch();
         // emission index as the value: the stable sort keeps each key's lowest first
         k_smc_iota<<<grid_for(m), 256, 0, s>>>(m, ord); count_launch();
         size_t tb = 0;

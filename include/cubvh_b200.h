@@ -156,23 +156,29 @@ int cubvh_signed_distance_host(cubvh_bvh* bvh, const float* points, int64_t n, u
 /* Sparse marching cubes.  coords int32 [n, 3] voxel coordinates and
  * corners float32 [n, 8] corner values (corner order (0,0,0), (1,0,0),
  * (1,1,0), (0,1,0), (0,0,1), (1,0,1), (1,1,1), (0,1,1) from the voxel's
- * coordinate), both device memory; iso the level; ensure_consistency != 0
- * first replaces every corner value by its mean over the voxels sharing
- * the corner.  Runs on `stream` and waits for it (the output sizes depend on
- * the data); *out receives a result holding *n_verts vertices (float32
+ * coordinate), both device memory; iso the level; ensure_consistency holds
+ * flags: CUBVH_SMC_ENSURE_CONSISTENCY (1, the reference's boolean) first
+ * replaces every corner value by its mean over the voxels sharing the
+ * corner; CUBVH_SMC_CLOSED (2) triangulates with this library's own closed
+ * triangulation instead of the reference's case table.  Runs on `stream`
+ * and waits for it (the output sizes depend on the data); *out receives a result holding *n_verts vertices (float32
  * [n_verts, 3], voxel units) and *n_tris triangles (int32 [n_tris, 3]);
  * cubvh_sparse_mc_fetch copies them into device arrays of those sizes on
  * its own `stream` (any stream: the copies wait for the building stream's
  * last kernels), cubvh_sparse_mc_free releases the result (it waits for this
  * result's build and fetches first, not for other work on the device).  The
  * result's memory, and the call's temporaries, come from a stream-ordered
- * pool of the library's own that keeps up to 256 MiB between calls.  The vertex array equals the
- * reference's (one vertex per cut voxel edge, merged across voxels, sorted
- * by edge); the triangulation is this library's own (see sparse_mc.cu): a
- * closed, consistently oriented surface where the corner values agree.
+ * pool of the library's own that keeps up to 256 MiB between calls.  The
+ * vertex array equals the reference's (one vertex per cut voxel edge, merged
+ * across voxels, sorted by edge), and so does the triangle array, index for
+ * index (the reference's marching-cubes case table, voxel by voxel); with
+ * CUBVH_SMC_CLOSED the triangles are this library's own (see sparse_mc.cu):
+ * a closed, consistently oriented surface where the corner values agree.
  * Replaces sparse_marching_cubes (src/api_gpu.cu:154-215,
  * include/gpu/spcumc.cuh `_sparse_marching_cubes`). */
 typedef struct cubvh_smc cubvh_smc;
+#define CUBVH_SMC_ENSURE_CONSISTENCY 1
+#define CUBVH_SMC_CLOSED 2
 int cubvh_sparse_marching_cubes(const int32_t* coords, const float* corners, int64_t n, float iso,
                                 int ensure_consistency, void* stream, cubvh_smc** out, int64_t* n_verts,
                                 int64_t* n_tris);

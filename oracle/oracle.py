@@ -252,6 +252,33 @@ def sparse_mc_vertices(coords, corners, iso, return_ids=False):
     return pos[order[head]], vi, ei, ids
 
 
+def sparse_mc_triangles(coords, corners, iso, table):
+    """The reference's sparse-marching-cubes triangle array
+    (include/gpu/spcumc.cuh classifyVoxels / generateTriangles and the remap
+    to merged vertices): voxel by voxel, for its corner configuration c (bit
+    k: corner k below iso) the case table's triangles table[c] = (e0, e1,
+    e2, ...), -1 after the last, each written as the merged vertices of
+    edges (e0, e2, e1).  table: int [256, 16] (the reference's case table,
+    e.g. tests/golden/ref_mc_cases.npz `tri_edges`).  Returns int32 [T, 3]."""
+    coords = np.asarray(coords)
+    v = np.asarray(corners, np.float32)
+    table = np.asarray(table)
+    _, vi, ei, ids = sparse_mc_vertices(coords, v, iso, return_ids=True)
+    vid = {}
+    for a, e, i in zip(vi.tolist(), ei.tolist(), ids.tolist()):
+        vid[(a, e)] = i
+    cube = ((v < np.float32(iso)) * (1 << np.arange(8))).sum(1)
+    out = []
+    for n, c in enumerate(cube.tolist()):
+        row = table[c]
+        for t in range(5):
+            if row[3 * t] < 0:
+                break
+            e0, e1, e2 = int(row[3 * t]), int(row[3 * t + 1]), int(row[3 * t + 2])
+            out.append((vid[(n, e0)], vid[(n, e2)], vid[(n, e1)]))
+    return np.array(out, np.int32).reshape(-1, 3)
+
+
 _REF_SMC_PATH = os.path.join(_HERE, "_ref", "libref_sparse_mc.so")
 _ref_smc = None
 

@@ -3,12 +3,15 @@
 tests/golden/ref_sparse_mc.npz holds the vertex and triangle arrays that the
 reference's CUDA sparse marching cubes (include/gpu/spcumc.cuh, built from the
 reference tree into oracle/_ref) returned for three voxel sets
-(make_ref_sparse_mc.py beside it).  The vertex arrays must be equal bit for
-bit (the oracle's restatement on the CPU, the CUDA kernels on the GPU).  The
-triangulation is this library's own: a cube with one corner on its own side
-gives the reference's triangle; otherwise the tests check what holds for any
-correct triangulation: closed and consistently oriented where the corner
-values agree, no edge in more than two triangles, the same enclosed volume."""
+(make_ref_sparse_mc.py beside it); tests/golden/ref_mc_cases.npz its triangle
+list for each of the 256 corner configurations of one voxel (its case table,
+make_ref_mc_cases.py).  By default the vertex and triangle arrays must equal
+the reference's index for index (the oracle's restatement on the CPU, the
+CUDA kernels on the GPU).  The optional closed triangulation
+(triangulation="closed") is this library's own: the tests check what holds
+for any correct triangulation there: closed and consistently oriented where
+the corner values agree, no edge in more than two triangles, the same
+enclosed volume."""
 
 import os
 import sys
@@ -24,7 +27,10 @@ sys.path.insert(0, os.path.join(HERE, "golden"))
 import make_ref_sparse_mc as M  # noqa: E402
 
 R = np.load(os.path.join(HERE, "golden", "ref_sparse_mc.npz"))
+TABLE = np.load(os.path.join(HERE, "golden", "ref_mc_cases.npz"))["tri_edges"]
 CASES = M.cases()
+EDGE_CORNERS = np.array([[0, 1], [1, 2], [2, 3], [3, 0], [4, 5], [5, 6], [6, 7], [7, 4], [0, 4], [1, 5], [2, 6],
+                         [3, 7]])
 
 
 def _edges(t):
@@ -51,20 +57,42 @@ def test_oracle_vertices_match_reference(oracle, name):
     assert np.array_equal(oracle.sparse_mc_vertices(coords, corners, iso), R[name + "_verts"])
 
 
-def _run(name, dev, ensure=False):
+def test_case_table_cuts_only_cut_edges():
+    """Every triangle of the reference's case table joins three different
+    edges that the configuration cuts (one corner inside); empty and full
+    cubes have no triangle."""
+    for c in range(256):
+        inside = [(c >> k) & 1 for k in range(8)]
+        cut = {e for e, (a, b) in enumerate(EDGE_CORNERS) if inside[a] != inside[b]}
+        row = TABLE[c][TABLE[c] >= 0]
+        assert len(row) % 3 == 0 and set(row.tolist()) <= cut
+        assert all(len(set(row[i:i + 3].tolist())) == 3 for i in range(0, len(row), 3))
+        if not cut:
+            assert len(row) == 0
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_oracle_triangles_match_reference(oracle, name):
+    coords, corners, iso = CASES[name]
+    assert np.array_equal(oracle.sparse_mc_triangles(coords, corners, iso, TABLE), R[name + "_tris"])
+
+
+def _run(name, dev, ensure=False, triangulation="reference"):
     coords, corners, iso = CASES[name]
     v, t = cubvh.sparse_marching_cubes(torch.from_numpy(coords).to(dev), torch.from_numpy(corners).to(dev), iso,
-                                       ensure_consistency=ensure)
+                                       ensure_consistency=ensure, triangulation=triangulation)
     assert v.dtype == torch.float32 and t.dtype == torch.int32 and v.is_cuda and t.is_cuda
     return v.cpu().numpy(), t.cpu().numpy()
 
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_vertices_match_reference(dev, name):
+def test_vertices_and_triangles_match_reference(dev, name):
     v, t = _run(name, dev)
     assert np.array_equal(v, R[name + "_verts"])
-    assert t.min() >= 0 and t.max() < len(v)
+    assert np.array_equal(t, R[name + "_tris"])          # index for index
+    _, tc = _run(name, dev, triangulation="closed")
+    assert tc.min() >= 0 and tc.max() < len(v)
 
 
 @pytest.mark.gpu
@@ -78,7 +106,7 @@ def test_single_triangle_cubes_match_reference(oracle, dev, name):
     single = np.nonzero(ncut == 3)[0]
     assert len(single) > 50
     want = {tuple(sorted(ids[vi == s])) for s in single}
-    _, t = _run(name, dev)
+    _, t = _run(name, dev, triangulation="closed")
     ours = {tuple(sorted(x)): tuple(r) for x, r in zip(t, _rot(t))}
     ref = {tuple(sorted(x)): tuple(r) for x, r in zip(R[name + "_tris"], _rot(R[name + "_tris"]))}
     for key in want:
@@ -87,7 +115,7 @@ def test_single_triangle_cubes_match_reference(oracle, dev, name):
 
 @pytest.mark.gpu
 def test_sphere_closed_oriented_same_volume(dev):
-    v, t = _run("sphere", dev)
+    v, t = _run("sphere", dev, triangulation="closed")
     _, cnt, dcnt = _edges(t)
     assert (cnt == 2).all() and (dcnt == 1).all()        # closed, each edge once each way
     assert len(t) == len(R["sphere_tris"])
@@ -100,7 +128,7 @@ def test_lattice_manifold(dev):
     """Random values on a full 12^3 block (many ambiguous faces): every edge
     inside the block is in exactly two triangles, once in each direction;
     open edges lie on the block's outer faces only."""
-    v, t = _run("lattice", dev)
+    v, t = _run("lattice", dev, triangulation="closed")
     e, cnt, dcnt = _edges(t)
     assert (cnt <= 2).all() and (dcnt == 1).all()
     und, c2 = np.unique(np.sort(e, 1), axis=0, return_counts=True)
@@ -129,6 +157,7 @@ def test_live_reference_larger(oracle, dev):
         rv, rt = oracle.ref_sparse_mc(coords, corners, iso)
         v, t = cubvh.sparse_marching_cubes(torch.from_numpy(coords).to(dev), torch.from_numpy(corners).to(dev), iso)
         assert np.array_equal(v.cpu().numpy(), rv)
+        assert np.array_equal(t.cpu().numpy(), rt)
 
 
 @pytest.mark.gpu
@@ -181,7 +210,7 @@ def test_model_single_triangles_match_reference(oracle):
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_kernels_match_model(oracle, dev, name):
     coords, corners, iso = CASES[name]
-    _, t = _run(name, dev)
+    _, t = _run(name, dev, triangulation="closed")
     assert np.array_equal(t, _model_tris(oracle, coords, corners, iso))
 
 
