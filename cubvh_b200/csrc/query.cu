@@ -1138,7 +1138,7 @@ __global__ void __launch_bounds__(kQBlock) k_sign_raystab(Work w, const uint32_t
 // warp start at the same point, so the first levels of their walks read the
 // same nodes.  Warps take candidates from a counter in the order the first
 // pass appended them (near one another in space).
-__global__ void __launch_bounds__(kQBlock) k_sign_raystab_lines(const float* __restrict__ pts,
+__global__ void __launch_bounds__(kQBlock, 10) k_sign_raystab_lines(const float* __restrict__ pts,
                                                                 float* __restrict__ dist,
                                                                 const CNode* __restrict__ nodes,
                                                                 const CTri* __restrict__ tris,
