@@ -79,9 +79,58 @@ cudaError_t cubvh::ensure_constants(int device) {
     return e;
 }
 
+// The library's stream-ordered pool on the current device.  Calls take their
+// scratch (query, ray, backward and floodfill workspaces, sparse marching
+// cubes temporaries) from it with cudaMallocFromPoolAsync and return it with
+// cudaFreeAsync.  The default pool's release threshold is 0: every stream or
+// device wait hands freed memory back to the driver and the next call maps
+// it again (1.5-2 ms per call, more than a small query's kernels).  This pool
+// keeps up to kPoolKeepBytes between calls and returns what is above that at
+// each wait.
+cudaError_t cubvh::library_pool(cudaMemPool_t* out) {
+    static std::mutex mu;
+    static std::vector<cudaMemPool_t> pools;  // by device ordinal, created on first use
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    if ((int)pools.size() <= dev) pools.resize((size_t)dev + 1, nullptr);
+    if (!pools[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        if ((e = cudaMemPoolCreate(&p, &props)) != cudaSuccess) return e;
+        uint64_t keep = kPoolKeepBytes;
+        if ((e = cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) {
+            cudaMemPoolDestroy(p);
+            return e;
+        }
+        pools[dev] = p;
+    }
+    *out = pools[dev];
+    return cudaSuccess;
+}
+
 namespace {
 
 thread_local std::string g_err;
+
+// Scratch of `bytes` on stream s: from the library pool, or, while s is
+// being captured into a CUDA graph, with cudaMallocAsync (the graph then owns
+// the allocation as a memory node).
+cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s) {
+    if (bytes == 0) bytes = 16;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(s, &cap);
+    if (e != cudaSuccess) return e;
+    if (cap != cudaStreamCaptureStatusNone) return cudaMallocAsync(p, bytes, s);
+    cudaMemPool_t pool = nullptr;
+    if ((e = library_pool(&pool)) != cudaSuccess) return e;
+    return cudaMallocFromPoolAsync(p, bytes, pool, s);
+}
 
 int fail(int code, const std::string& msg) {
     g_err = msg;
@@ -489,7 +538,7 @@ int cubvh_signed_distance(cubvh_bvh* h, const float* points, int64_t n, uint32_t
     const size_t wsb = query_workspace_bytes(kmode, n);
     void* ws = nullptr;
     cudaError_t e;
-    if ((e = cudaMallocAsync(&ws, wsb, s)) != cudaSuccess) return cuda_fail(e, "cudaMallocAsync(query workspace)");
+    if ((e = pool_alloc(&ws, wsb, s)) != cudaSuccess) return cuda_fail(e, "query workspace allocation");
     e = launch_distance(kmode, uvw != nullptr, n, points, distances, face_id, uvw, d->nodes, d->tris,
                         (int)h->host.slot_of_face0, near, ws, s);
     if (ws) {
@@ -514,8 +563,8 @@ int cubvh_ray_trace(cubvh_bvh* h, const float* rays_o, const float* rays_d, int6
     if (rc != CUBVH_OK) return rc;
     cudaStream_t s = (cudaStream_t)stream;
     void* ws = nullptr;
-    cudaError_t e = cudaMallocAsync(&ws, query_workspace_bytes(-1, n), s);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync(ray workspace)");
+    cudaError_t e = pool_alloc(&ws, query_workspace_bytes(-1, n), s);
+    if (e != cudaSuccess) return cuda_fail(e, "ray workspace allocation");
     e = launch_ray(n, rays_o, rays_d, positions, face_id, depth, d->nodes, d->tris, ws, s);
     const cudaError_t e2 = cudaFreeAsync(ws, s);
     if (e == cudaSuccess) e = e2;
@@ -847,8 +896,8 @@ int cubvh_floodfill(const uint8_t* grid, int B, int H, int W, int D, int32_t* la
     if (ws) {
         if (workspace_bytes < need) return fail(CUBVH_ERR_INVALID, "workspace smaller than cubvh_floodfill_workspace_size()");
         if (reinterpret_cast<uintptr_t>(ws) & 255) return fail(CUBVH_ERR_INVALID, "workspace must be 256-byte aligned");
-    } else if ((e = cudaMallocAsync(&ws, need, s)) != cudaSuccess) {
-        return cuda_fail(e, "cudaMallocAsync(floodfill workspace)");
+    } else if ((e = pool_alloc(&ws, need, s)) != cudaSuccess) {
+        return cuda_fail(e, "floodfill workspace allocation");
     }
     e = launch_floodfill(grid, B, H, W, D, labels, ws, s);
     if (!workspace) {
@@ -875,8 +924,8 @@ int cubvh_udf_to_sdf(const float* udf, int B, int H, int W, int D, float eps, fl
     if (ws) {
         if (workspace_bytes < need) return fail(CUBVH_ERR_INVALID, "workspace smaller than cubvh_floodfill_workspace_size()");
         if (reinterpret_cast<uintptr_t>(ws) & 255) return fail(CUBVH_ERR_INVALID, "workspace must be 256-byte aligned");
-    } else if ((e = cudaMallocAsync(&ws, need, s)) != cudaSuccess) {
-        return cuda_fail(e, "cudaMallocAsync(udf_to_sdf workspace)");
+    } else if ((e = pool_alloc(&ws, need, s)) != cudaSuccess) {
+        return cuda_fail(e, "udf_to_sdf workspace allocation");
     }
     e = launch_udf_to_sdf(udf, B, H, W, D, eps, sdf, ws, s);
     if (!workspace) {
@@ -952,8 +1001,8 @@ int cubvh_distance_backward(cubvh_bvh* h, const float* points, int64_t n, const 
     cudaStream_t s = (cudaStream_t)stream;
     const int64_t nf = (int64_t)h->ids.size();
     void* ws = nullptr;
-    cudaError_t e = cudaMallocAsync(&ws, backward_workspace_bytes(n, nf), s);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync(backward workspace)");
+    cudaError_t e = pool_alloc(&ws, backward_workspace_bytes(n, nf), s);
+    if (e != cudaSuccess) return cuda_fail(e, "backward workspace allocation");
     e = launch_backward(n, points, face_id, grad_distances, distances, vertices, vertices ? d->face_vidx : nullptr,
                         d->face_slot, d->tris, nf, grad_points, grad_vertices, ws, s);
     const cudaError_t e2 = cudaFreeAsync(ws, s);

@@ -13,6 +13,10 @@ cudaError_t upload_constants();
 // upload_constants() once per device (the current one must be `device`):
 // every entry point that launches query kernels on a device calls it first.
 cudaError_t ensure_constants(int device);
+// The library's stream-ordered memory pool on the current device (created on
+// first use; abi.cu), which keeps up to kPoolKeepBytes between calls.
+constexpr uint64_t kPoolKeepBytes = 512ull << 20;
+cudaError_t library_pool(cudaMemPool_t* out);
 // Raystab stab directions of queries first .. first+n-1 into float [n, 32, 3].
 cudaError_t launch_stab_dirs(int64_t first, int64_t n, float* dirs, cudaStream_t stream);
 

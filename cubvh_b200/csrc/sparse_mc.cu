@@ -412,40 +412,6 @@ int bits_for(uint64_t v) {  // bits to hold values below v
     return b;
 }
 
-// The library's stream-ordered pool on the current device.  A call waits
-// for its stream three times (the output sizes depend on the data); with the
-// default pool's release threshold of 0 every such wait hands the freed
-// temporaries back to the driver and the next allocation maps them again,
-// which cost more than the kernels.  This pool keeps up to kPoolKeep bytes
-// between calls and returns what is above that at each wait.
-constexpr uint64_t kPoolKeep = 256ull << 20;
-cudaError_t smc_pool(cudaMemPool_t* out) {
-    static std::mutex mu;
-    static std::vector<cudaMemPool_t> pools;  // by device ordinal, created on first use
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    std::lock_guard<std::mutex> lk(mu);
-    if ((int)pools.size() <= dev) pools.resize((size_t)dev + 1, nullptr);
-    if (!pools[dev]) {
-        cudaMemPoolProps props = {};
-        props.allocType = cudaMemAllocationTypePinned;
-        props.handleTypes = cudaMemHandleTypeNone;
-        props.location.type = cudaMemLocationTypeDevice;
-        props.location.id = dev;
-        cudaMemPool_t p = nullptr;
-        if ((e = cudaMemPoolCreate(&p, &props)) != cudaSuccess) return e;
-        uint64_t keep = kPoolKeep;
-        if ((e = cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) {
-            cudaMemPoolDestroy(p);
-            return e;
-        }
-        pools[dev] = p;
-    }
-    *out = pools[dev];
-    return cudaSuccess;
-}
-
 template <class T>
 cudaError_t pool_get(cudaMemPool_t pool, cudaStream_t s, T** out, size_t count) {
     void* q = nullptr;
@@ -490,7 +456,7 @@ int sparse_mc_run(const int32_t* coords, const float* corners, int64_t n, float 
     cudaError_t e;
     auto fail = [&](cudaError_t x, const char* what) { err = std::string(what) + ": " + cudaGetErrorString(x); return 2; };
     cudaMemPool_t pool = nullptr;
-    if ((e = smc_pool(&pool)) != cudaSuccess) return fail(e, "memory pool");
+    if ((e = library_pool(&pool)) != cudaSuccess) return fail(e, "memory pool");
     AsyncTemps tmp(pool, s);
     // coordinate bounds -> key packing (host round trip)
     int32_t* d_b = nullptr;

@@ -167,8 +167,8 @@ int cubvh_signed_distance_host(cubvh_bvh* bvh, const float* points, int64_t n, u
  * its own `stream` (any stream: the copies wait for the building stream's
  * last kernels), cubvh_sparse_mc_free releases the result (it waits for this
  * result's build and fetches first, not for other work on the device).  The
- * result's memory, and the call's temporaries, come from a stream-ordered
- * pool of the library's own that keeps up to 256 MiB between calls.  The
+ * result's memory, and the call's temporaries, come from the library's
+ * stream-ordered pool (it keeps up to 512 MiB per device between calls).  The
  * vertex array equals the reference's (one vertex per cut voxel edge, merged
  * across voxels, sorted by edge), and so does the triangle array, index for
  * index (the reference's marching-cubes case table, voxel by voxel); with
@@ -260,7 +260,7 @@ int cubvh_stab_directions(int64_t first, int64_t n, float* dirs, void* stream);
  * as C-order [D][H][W]).  B*H*W*D must be below 2^31.
  * Scratch: pass `workspace` of at least cubvh_floodfill_workspace_size()
  * bytes (device memory, 256-byte aligned), or NULL to let the call take it
- * from the device's stream-ordered memory pool.  Asynchronous; when a
+ * from the library's stream-ordered pool.  Asynchronous; when a
  * workspace is passed, cubvh_floodfill_check() reports device-side bound
  * hits of the last call that used it.
  * Replaces floodfill (src/api_gpu.cu:136-152, include/gpu/floodfill.cuh:157-272). */

@@ -278,3 +278,30 @@ def test_reference_mirror_agreement(oracle, dev):
         a, _ = oracle.face_dist64(v, f, pts[diff], fid[diff])
         b, _ = oracle.face_dist64(v, f, pts[diff], rfid[diff])
         assert np.abs(a - b).max() <= 1e-7
+
+
+def test_queries_in_cuda_graph(dev):
+    """A device-resident query recorded in a CUDA graph (its scratch then
+    comes from the graph's memory nodes) replays to the direct call's
+    results; direct calls between synchronisations reuse the library pool."""
+    v, f = W.displaced_icosphere(3, 1)
+    bvh = cubvh.cuBVH(v, f)
+    pts = torch.from_numpy(W.uniform_points(6000, 11)).to(dev)
+    want = bvh.signed_distance(pts, mode="watertight")
+    want_r = bvh.ray_trace(torch.zeros(500, 3, device=dev), torch.nn.functional.normalize(pts[:500], dim=1))
+    torch.cuda.synchronize()
+    s = torch.cuda.Stream(dev)
+    s.wait_stream(torch.cuda.current_stream(dev))
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        got = bvh.signed_distance(pts, mode="watertight")
+        got_r = bvh.ray_trace(torch.zeros(500, 3, device=dev), torch.nn.functional.normalize(pts[:500], dim=1))
+    for _ in range(2):
+        g.replay()
+        torch.cuda.synchronize()
+        assert torch.equal(got[0], want[0]) and torch.equal(got[1], want[1])
+        assert all(torch.equal(a, b) for a, b in zip(got_r, want_r))
+    for _ in range(3):   # synchronising callers: same results from the pool's scratch
+        d, fid, _ = bvh.signed_distance(pts, mode="watertight")
+        torch.cuda.synchronize()
+        assert torch.equal(d, want[0]) and torch.equal(fid, want[1])
