@@ -1457,6 +1457,19 @@ size_t query_workspace_bytes(int mode, int64_t n) {
 }
 
 namespace {
+// Slots of the 256-byte counter block at the head of a launch's workspace
+// (32 uint64, zeroed at the start of every launch); each has one user.
+enum : int {
+    kCtUdf = 0,         // k_udf packet queue
+    kCtSign = 1,        // sign-pass packet queue (watertight, or the first raystab pass of a single BVH)
+    kCtArenaRs = 2,     // first raystab pass of an arena (its watertight pass takes kCtSign)
+    kCtHeavyN = 6,      // heavy-query list length
+    kCtHeavyNext = 7,   // k_udf_heavy queue
+    kCtStats = 8,       // k_udf tail statistics: node + leaf visits (8), packets finished (9)
+    kCtOvfN = 10,       // watertight overflow queue length
+    kCtCandN = 12,      // raystab second-pass candidates
+    kCtLinesNext = 13,  // raystab second-pass queue
+};
 // packets per atomic grab: about 64 grabs per warp of the launch
 int64_t grab_for(int64_t n, unsigned grid) {
     const int64_t packets = (n + 31) / 32;
@@ -1531,15 +1544,15 @@ cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts
         const float ppw_ = packets_per_warp((n + 31) / 32, g_); \
         if (ppw_ >= kTailPpw) { \
             k_udf<U, S, false><<<g_, kQBlock, 0, stream>>>(work, order, pts, dist, fid, uvw, slots, nodes, tris, \
-                                                           ctr, grab_for(n, g_), heavy, ctr + 6, hcap, ctr + 8, ppw_); count_launch(); \
+                                                           ctr + kCtUdf, grab_for(n, g_), heavy, ctr + kCtHeavyN, hcap, ctr + kCtStats, ppw_); count_launch(); \
         } else { \
             const unsigned gt_ = persistent_grid(k_udf<U, S, true>, n); \
             k_udf<U, S, true><<<gt_, kQBlock, 0, stream>>>(work, order, pts, dist, fid, uvw, slots, nodes, tris, \
-                                                           ctr, grab_for(n, gt_), heavy, ctr + 6, hcap, ctr + 8, \
+                                                           ctr + kCtUdf, grab_for(n, gt_), heavy, ctr + kCtHeavyN, hcap, ctr + kCtStats, \
                                                            packets_per_warp((n + 31) / 32, gt_)); count_launch(); \
             const unsigned gh_ = persistent_grid(k_udf_heavy<U, S>, 32 * hcap); \
-            k_udf_heavy<U, S><<<gh_, kQBlock, 0, stream>>>(heavy, ctr + 6, hcap, nullptr, slot_face0, pts, dist, \
-                                                           fid, uvw, slots, nodes, tris, ctr + 7); count_launch(); \
+            k_udf_heavy<U, S><<<gh_, kQBlock, 0, stream>>>(heavy, ctr + kCtHeavyN, hcap, nullptr, slot_face0, pts, dist, \
+                                                           fid, uvw, slots, nodes, tris, ctr + kCtHeavyNext); count_launch(); \
         } } while (0)
     if (mode == 0) { if (want_uvw) CUBVH_L(true, false); else CUBVH_L(false, false); }
     else { if (want_uvw) CUBVH_L(true, true); else CUBVH_L(false, true); }
@@ -1548,19 +1561,20 @@ cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts
         if (near.cnt) {
             const unsigned g = persistent_grid(k_sign_watertight<true>, n);
             k_sign_watertight<true><<<g, kQBlock, 0, stream>>>(work, order, pts, dist, slots, nodes, tris, near, ovf,
-                                                               ctr + 9, ctr + 1, grab_for(n, g)); count_launch();
+                                                               ctr + kCtOvfN, ctr + kCtSign, grab_for(n, g)); count_launch();
             if (near.ovf) {
                 const unsigned go = persistent_grid(k_sign_watertight_ovf, n);
-                k_sign_watertight_ovf<<<go, kQBlock, 0, stream>>>(ovf, ctr + 9, pts, dist, slots, nodes, tris); count_launch();
+                k_sign_watertight_ovf<<<go, kQBlock, 0, stream>>>(ovf, ctr + kCtOvfN, pts, dist, slots, nodes, tris); count_launch();
             }
         } else {
             const unsigned g = persistent_grid(k_sign_watertight<false>, n);
             k_sign_watertight<false><<<g, kQBlock, 0, stream>>>(work, order, pts, dist, slots, nodes, tris, near,
-                                                                nullptr, nullptr, ctr + 1, grab_for(n, g)); count_launch();
+                                                                nullptr, nullptr, ctr + kCtSign, grab_for(n, g)); count_launch();
         }
     } else if (mode == 2) {
         uint4* cand = reinterpret_cast<uint4*>(w);
-        launch_raystab(work, n, order, pts, dist, nodes, tris, ctr + 1, cand, ctr + 12, ctr + 13, stream);
+        launch_raystab(work, n, order, pts, dist, nodes, tris, ctr + kCtSign, cand, ctr + kCtCandN, ctr + kCtLinesNext,
+                       stream);
     }
     return cudaGetLastError();
 }
@@ -1582,7 +1596,7 @@ cudaError_t launch_ray(int64_t n, const float* ro, const float* rd, float* pos, 
     cudaError_t e = cudaMemsetAsync(ctr, 0, 256, stream);
     if (e != cudaSuccess) return e;
     const unsigned g = persistent_grid(k_ray, n);
-    k_ray<<<g, kQBlock, 0, stream>>>(n, ro, rd, pos, fid, depth, nodes, tris, ctr, grab_for(n, g)); count_launch();
+    k_ray<<<g, kQBlock, 0, stream>>>(n, ro, rd, pos, fid, depth, nodes, tris, ctr + kCtUdf, grab_for(n, g)); count_launch();
     return cudaGetLastError();
 }
 
@@ -1638,18 +1652,18 @@ cudaError_t launch_arena_distance(const ArenaLaunch& a, const float* pts, float*
         const float ppw_ = packets_per_warp(a.n_packets, g_); \
         if (ppw_ >= kTailPpw) { \
             k_udf<U, S, false><<<g_, kQBlock, 0, stream>>>(all, a.order, pts, dist, fid, uvw, a.slots, a.nodes, \
-                                                           a.tris, a.counters, grab_for(a.n_queries, g_), a.heavy, \
-                                                           a.counters + 6, a.heavy_cap, a.counters + 8, ppw_); count_launch(); \
+                                                           a.tris, a.counters + kCtUdf, grab_for(a.n_queries, g_), a.heavy, \
+                                                           a.counters + kCtHeavyN, a.heavy_cap, a.counters + kCtStats, ppw_); count_launch(); \
         } else { \
             const unsigned gt_ = persistent_grid(k_udf<U, S, true>, a.n_queries); \
             k_udf<U, S, true><<<gt_, kQBlock, 0, stream>>>(all, a.order, pts, dist, fid, uvw, a.slots, a.nodes, \
-                                                           a.tris, a.counters, grab_for(a.n_queries, gt_), a.heavy, \
-                                                           a.counters + 6, a.heavy_cap, a.counters + 8, \
+                                                           a.tris, a.counters + kCtUdf, grab_for(a.n_queries, gt_), a.heavy, \
+                                                           a.counters + kCtHeavyN, a.heavy_cap, a.counters + kCtStats, \
                                                            packets_per_warp(a.n_packets, gt_)); count_launch(); \
             const unsigned gh_ = persistent_grid(k_udf_heavy<U, S>, 32 * a.heavy_cap); \
-            k_udf_heavy<U, S><<<gh_, kQBlock, 0, stream>>>(a.heavy, a.counters + 6, a.heavy_cap, a.meshes, 0, pts, \
+            k_udf_heavy<U, S><<<gh_, kQBlock, 0, stream>>>(a.heavy, a.counters + kCtHeavyN, a.heavy_cap, a.meshes, 0, pts, \
                                                            dist, fid, uvw, a.slots, a.nodes, a.tris, \
-                                                           a.counters + 7); count_launch(); \
+                                                           a.counters + kCtHeavyNext); count_launch(); \
         } } while (0)
     if (uvw) { if (signed_any) CUBVH_L(true, true); else CUBVH_L(true, false); }
     else { if (signed_any) CUBVH_L(false, true); else CUBVH_L(false, false); }
@@ -1658,13 +1672,13 @@ cudaError_t launch_arena_distance(const ArenaLaunch& a, const float* pts, float*
         const Work w{a.wt_packets, a.meshes, a.n_wt_packets, 0};
         const unsigned gw = persistent_grid(k_sign_watertight<false>, 32 * a.n_wt_packets);
         k_sign_watertight<false><<<gw, kQBlock, 0, stream>>>(w, a.order, pts, dist, a.slots, a.nodes, a.tris,
-                                                             NearLists{}, nullptr, nullptr, a.counters + 1,
+                                                             NearLists{}, nullptr, nullptr, a.counters + kCtSign,
                                                              grab_for(32 * a.n_wt_packets, gw)); count_launch();
     }
     if (a.n_rs_packets > 0) {
         const Work w{a.rs_packets, a.meshes, a.n_rs_packets, 0};
-        launch_raystab(w, 32 * a.n_rs_packets, a.order, pts, dist, a.nodes, a.tris, a.counters + 2, a.rs_cand,
-                       a.counters + 12, a.counters + 13, stream);
+        launch_raystab(w, 32 * a.n_rs_packets, a.order, pts, dist, a.nodes, a.tris, a.counters + kCtArenaRs,
+                       a.rs_cand, a.counters + kCtCandN, a.counters + kCtLinesNext, stream);
     }
     return cudaGetLastError();
 }

@@ -67,3 +67,20 @@ def test_watertight_list_overflow(oracle, dev):
     pts = np.concatenate([rng.uniform(-0.8, 0.8, (2000, 3)),
                           apex[rng.integers(0, 2, 2000)] + rng.normal(0, 0.01, (2000, 3))]).astype(np.float32)
     _check(oracle, bvh, v, f, pts, dev)
+
+
+def test_watertight_overflow_repeated(oracle, dev):
+    """Back-to-back calls whose scratch is reused: the overflow queue of one
+    call holds only that call's queries (its length counter is its own, not
+    shared with the distance pass's tail statistics), so repeated calls with
+    few packets per warp (the distance pass's tail control on) and
+    overflowing lists keep every sign.  A triangle soup with every face four
+    times overflows every list."""
+    v, f = W.icosphere(2, 0.5)
+    f = np.concatenate([f, f, f, f[:7]])
+    bvh = cubvh.cuBVH(v, f)
+    for seed in range(4):
+        rng = np.random.default_rng(40 + seed)
+        pts = np.concatenate([rng.uniform(-0.7, 0.7, (3000, 3)),
+                              W.surface_points(v, f, 3000, 0.02, rng)]).astype(np.float32)
+        _check(oracle, bvh, v, f, pts, dev)
