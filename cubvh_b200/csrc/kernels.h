@@ -71,10 +71,12 @@ struct NearLists {
 };
 // qbase: index of query 0 within the caller's whole call (the raystab stab
 // directions follow the query index; a call split into chunks passes each
-// chunk's first index).
+// chunk's first index).  yield: the distance and watertight sign passes run
+// as many short-lived blocks instead of one persistent wave, so kernels of
+// higher-priority streams get SMs during them (host-buffer pipelines).
 cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts, float* dist, int64_t* fid,
                             float* uvw, const CNode* nodes, const CTri* tris, int slot_face0, NearLists near,
-                            void* ws, cudaStream_t stream, int64_t qbase = 0);
+                            void* ws, cudaStream_t stream, int64_t qbase = 0, bool yield = false);
 // any_ovf: one device int, set to 1 when some list overflowed.
 cudaError_t launch_near_lists(int64_t n_tris, const CNode* nodes, const CTri* tris, int32_t* cnt, int32_t* lst,
                               double* nrm, int* any_ovf, cudaStream_t stream);

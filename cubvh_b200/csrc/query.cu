@@ -291,16 +291,27 @@ __device__ __forceinline__ void leaf_range(int ref, int& s0, int& s1) {
 // Dynamic packet queue: a warp takes `grab` consecutive 32-query packets per
 // atomicAdd on a per-launch counter (zeroed before the launch), so warps that
 // drew cheap packets keep taking more and no SM idles while work remains.
+//
+// Block budget (left != nullptr): the block's warps take at most *left grabs
+// between them (a shared-memory count), then stop, and the block exits.  A
+// launch of many such blocks (yield_shape) drains the same queue in short
+// block lifetimes, so blocks of kernels on higher-priority streams get SMs
+// between them instead of waiting for the whole launch.
 struct PacketQueue {
     unsigned long long* ctr;
     int64_t npk, grab, next, end;
-    __device__ __forceinline__ PacketQueue(unsigned long long* c, int64_t npk_, int64_t g)
-        : ctr(c), npk(npk_), grab(g), next(0), end(0) {}
+    int* left;
+    __device__ __forceinline__ PacketQueue(unsigned long long* c, int64_t npk_, int64_t g, int* left_ = nullptr)
+        : ctr(c), npk(npk_), grab(g), next(0), end(0), left(left_) {}
+    __device__ __forceinline__ unsigned long long grab_start() {
+        if (left && atomicSub(left, 1) <= 0) return (unsigned long long)npk;  // budget spent: done
+        return atomicAdd(ctr, (unsigned long long)grab);
+    }
     // index of the warp's next packet, or -1 when done
     __device__ __forceinline__ int64_t take() {
         if (next == end) {
             unsigned long long b = 0;
-            if ((threadIdx.x & 31) == 0) b = atomicAdd(ctr, (unsigned long long)grab);
+            if ((threadIdx.x & 31) == 0) b = grab_start();
             next = (int64_t)__shfl_sync(kFull, b, 0);
             end = next + grab;
         }
@@ -310,7 +321,7 @@ struct PacketQueue {
     // the warp's next range of packets [b, e), false when done (warp-collective)
     __device__ __forceinline__ bool take_range(int64_t& b, int64_t& e) {
         unsigned long long v = 0;
-        if ((threadIdx.x & 31) == 0) v = atomicAdd(ctr, (unsigned long long)grab);
+        if ((threadIdx.x & 31) == 0) v = grab_start();
         b = (int64_t)__shfl_sync(kFull, v, 0);
         e = b + grab < npk ? b + grab : npk;
         return b < npk;
@@ -412,11 +423,16 @@ __global__ void __launch_bounds__(kQBlock) k_udf(Work w, const uint32_t* __restr
                                                  unsigned long long* __restrict__ ctr, int64_t grab,
                                                  uint2* __restrict__ heavy, unsigned long long* __restrict__ n_heavy,
                                                  int64_t heavy_cap, unsigned long long* __restrict__ stats,
-                                                 float ppw) {
+                                                 float ppw, int block_grabs) {
     const int lane = threadIdx.x & 31;
     __shared__ __align__(16) float s_box[kQBlock / 32][64];
+    __shared__ int s_left;
     float* sb = s_box[threadIdx.x >> 5];
-    PacketQueue pq(ctr, w.packets(), grab);
+    if (block_grabs > 0) {  // uniform: the launch's block budget
+        if (threadIdx.x == 0) s_left = block_grabs;
+        __syncthreads();
+    }
+    PacketQueue pq(ctr, w.packets(), grab, block_grabs > 0 ? &s_left : nullptr);
     for (int64_t pk = pq.take(); pk >= 0; pk = pq.take()) {
         int64_t start, qoff;
         int cnt, root, slot_face0;
@@ -940,8 +956,13 @@ __global__ void __launch_bounds__(kQBlock)
 k_sign_watertight(Work w, const uint32_t* __restrict__ order, const float* __restrict__ pts, float* __restrict__ dist,
                   const int32_t* __restrict__ slots, const CNode* __restrict__ nodes, const CTri* __restrict__ tris,
                   const NearLists near, uint32_t* __restrict__ ovf, unsigned long long* __restrict__ ovf_n,
-                  unsigned long long* __restrict__ ctr, int64_t grab) {
-    PacketQueue pq(ctr, w.packets(), grab);
+                  unsigned long long* __restrict__ ctr, int64_t grab, int block_grabs) {
+    __shared__ int s_left;
+    if (block_grabs > 0) {
+        if (threadIdx.x == 0) s_left = block_grabs;
+        __syncthreads();
+    }
+    PacketQueue pq(ctr, w.packets(), grab, block_grabs > 0 ? &s_left : nullptr);
     for (int64_t pk = pq.take(); pk >= 0; pk = pq.take()) {
         int64_t start, qoff;
         int cnt, root, s0;
@@ -1477,6 +1498,22 @@ int64_t grab_for(int64_t n, unsigned grid) {
     const int64_t g = packets / (warps * 64);
     return g < 1 ? 1 : g;
 }
+// Launch shape of a yielding launch (PacketQueue block budget): kYieldWaves
+// times the persistent grid g, each block taking at most block_grabs grabs,
+// twice the queue's grabs in all, so the queue is always drained (a warp
+// stops only when its block's budget is spent or the queue is empty) and a
+// block lives for about 1 / (kYieldWaves / 2) of the launch.  off: the
+// persistent launch (g blocks, no budget).
+constexpr unsigned kYieldWaves = 4;  // measured against 8 and 16
+struct LaunchShape { unsigned grid; int block_grabs; };
+LaunchShape yield_shape(unsigned g, int64_t n, int64_t grab, bool on) {
+    if (!on) return {g, 0};
+    const int64_t grabs = ((n + 31) / 32 + grab - 1) / grab;
+    int64_t G = (int64_t)g * kYieldWaves;
+    if (G > 2 * grabs) G = 2 * grabs > 0 ? 2 * grabs : 1;
+    const int64_t bg = (2 * grabs + G - 1) / G;
+    return {(unsigned)G, (int)(bg > 0 ? bg : 1)};
+}
 // raystab chunk: kChunkMax packets (64 queries for 32 lanes: a lane whose
 // query ends early takes another one; larger chunks cost more in lane-by-lane
 // query setup than they save), one packet when the launch has fewer than two
@@ -1509,7 +1546,7 @@ void launch_raystab(const Work& w, int64_t n, const uint32_t* order, const float
 
 cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts, float* dist, int64_t* fid,
                             float* uvw, const CNode* nodes, const CTri* tris, int slot_face0, NearLists near,
-                            void* ws, cudaStream_t stream, int64_t qbase) {
+                            void* ws, cudaStream_t stream, int64_t qbase, bool yield) {
     if (n <= 0) return cudaSuccess;
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     char* w = static_cast<char*>(ws);
@@ -1543,13 +1580,16 @@ cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts
 #define CUBVH_L(U, S) do { const unsigned g_ = persistent_grid(k_udf<U, S, false>, n); \
         const float ppw_ = packets_per_warp((n + 31) / 32, g_); \
         if (ppw_ >= kTailPpw) { \
-            k_udf<U, S, false><<<g_, kQBlock, 0, stream>>>(work, order, pts, dist, fid, uvw, slots, nodes, tris, \
-                                                           ctr + kCtUdf, grab_for(n, g_), heavy, ctr + kCtHeavyN, hcap, ctr + kCtStats, ppw_); count_launch(); \
+            const LaunchShape y_ = yield_shape(g_, n, grab_for(n, g_), yield); \
+            k_udf<U, S, false><<<y_.grid, kQBlock, 0, stream>>>(work, order, pts, dist, fid, uvw, slots, nodes, tris, \
+                                                           ctr + kCtUdf, grab_for(n, g_), heavy, ctr + kCtHeavyN, hcap, ctr + kCtStats, ppw_, \
+                                                           y_.block_grabs); count_launch(); \
         } else { \
             const unsigned gt_ = persistent_grid(k_udf<U, S, true>, n); \
-            k_udf<U, S, true><<<gt_, kQBlock, 0, stream>>>(work, order, pts, dist, fid, uvw, slots, nodes, tris, \
+            const LaunchShape y_ = yield_shape(gt_, n, grab_for(n, gt_), yield); \
+            k_udf<U, S, true><<<y_.grid, kQBlock, 0, stream>>>(work, order, pts, dist, fid, uvw, slots, nodes, tris, \
                                                            ctr + kCtUdf, grab_for(n, gt_), heavy, ctr + kCtHeavyN, hcap, ctr + kCtStats, \
-                                                           packets_per_warp((n + 31) / 32, gt_)); count_launch(); \
+                                                           packets_per_warp((n + 31) / 32, gt_), y_.block_grabs); count_launch(); \
             const unsigned gh_ = persistent_grid(k_udf_heavy<U, S>, 32 * hcap); \
             k_udf_heavy<U, S><<<gh_, kQBlock, 0, stream>>>(heavy, ctr + kCtHeavyN, hcap, nullptr, slot_face0, pts, dist, \
                                                            fid, uvw, slots, nodes, tris, ctr + kCtHeavyNext); count_launch(); \
@@ -1560,16 +1600,20 @@ cudaError_t launch_distance(int mode, bool want_uvw, int64_t n, const float* pts
     if (mode == 1) {
         if (near.cnt) {
             const unsigned g = persistent_grid(k_sign_watertight<true>, n);
-            k_sign_watertight<true><<<g, kQBlock, 0, stream>>>(work, order, pts, dist, slots, nodes, tris, near, ovf,
-                                                               ctr + kCtOvfN, ctr + kCtSign, grab_for(n, g)); count_launch();
+            const LaunchShape y = yield_shape(g, n, grab_for(n, g), yield);
+            k_sign_watertight<true><<<y.grid, kQBlock, 0, stream>>>(work, order, pts, dist, slots, nodes, tris, near, ovf,
+                                                                    ctr + kCtOvfN, ctr + kCtSign, grab_for(n, g),
+                                                                    y.block_grabs); count_launch();
             if (near.ovf) {
                 const unsigned go = persistent_grid(k_sign_watertight_ovf, n);
                 k_sign_watertight_ovf<<<go, kQBlock, 0, stream>>>(ovf, ctr + kCtOvfN, pts, dist, slots, nodes, tris); count_launch();
             }
         } else {
             const unsigned g = persistent_grid(k_sign_watertight<false>, n);
-            k_sign_watertight<false><<<g, kQBlock, 0, stream>>>(work, order, pts, dist, slots, nodes, tris, near,
-                                                                nullptr, nullptr, ctr + kCtSign, grab_for(n, g)); count_launch();
+            const LaunchShape y = yield_shape(g, n, grab_for(n, g), yield);
+            k_sign_watertight<false><<<y.grid, kQBlock, 0, stream>>>(work, order, pts, dist, slots, nodes, tris, near,
+                                                                     nullptr, nullptr, ctr + kCtSign, grab_for(n, g),
+                                                                     y.block_grabs); count_launch();
         }
     } else if (mode == 2) {
         uint4* cand = reinterpret_cast<uint4*>(w);
@@ -1653,13 +1697,13 @@ cudaError_t launch_arena_distance(const ArenaLaunch& a, const float* pts, float*
         if (ppw_ >= kTailPpw) { \
             k_udf<U, S, false><<<g_, kQBlock, 0, stream>>>(all, a.order, pts, dist, fid, uvw, a.slots, a.nodes, \
                                                            a.tris, a.counters + kCtUdf, grab_for(a.n_queries, g_), a.heavy, \
-                                                           a.counters + kCtHeavyN, a.heavy_cap, a.counters + kCtStats, ppw_); count_launch(); \
+                                                           a.counters + kCtHeavyN, a.heavy_cap, a.counters + kCtStats, ppw_, 0); count_launch(); \
         } else { \
             const unsigned gt_ = persistent_grid(k_udf<U, S, true>, a.n_queries); \
             k_udf<U, S, true><<<gt_, kQBlock, 0, stream>>>(all, a.order, pts, dist, fid, uvw, a.slots, a.nodes, \
                                                            a.tris, a.counters + kCtUdf, grab_for(a.n_queries, gt_), a.heavy, \
                                                            a.counters + kCtHeavyN, a.heavy_cap, a.counters + kCtStats, \
-                                                           packets_per_warp(a.n_packets, gt_)); count_launch(); \
+                                                           packets_per_warp(a.n_packets, gt_), 0); count_launch(); \
             const unsigned gh_ = persistent_grid(k_udf_heavy<U, S>, 32 * a.heavy_cap); \
             k_udf_heavy<U, S><<<gh_, kQBlock, 0, stream>>>(a.heavy, a.counters + kCtHeavyN, a.heavy_cap, a.meshes, 0, pts, \
                                                            dist, fid, uvw, a.slots, a.nodes, a.tris, \
@@ -1673,7 +1717,7 @@ cudaError_t launch_arena_distance(const ArenaLaunch& a, const float* pts, float*
         const unsigned gw = persistent_grid(k_sign_watertight<false>, 32 * a.n_wt_packets);
         k_sign_watertight<false><<<gw, kQBlock, 0, stream>>>(w, a.order, pts, dist, a.slots, a.nodes, a.tris,
                                                              NearLists{}, nullptr, nullptr, a.counters + kCtSign,
-                                                             grab_for(32 * a.n_wt_packets, gw)); count_launch();
+                                                             grab_for(32 * a.n_wt_packets, gw), 0); count_launch();
     }
     if (a.n_rs_packets > 0) {
         const Work w{a.rs_packets, a.meshes, a.n_rs_packets, 0};

@@ -60,7 +60,9 @@ def test_host_queries_one_chunk(dev, pinned):
 
 @pytest.mark.gpu
 def test_host_queries_several_chunks(dev):
-    n = 2 * CHUNK + 123_457          # three chunks, the last one partial
+    # five chunks, the last one partial: more chunks than the pipe's four
+    # staging sets, so sets are reused
+    n = 4 * CHUNK + 123_457
     v, f = W.icosphere(3, 0.8)
     bvh = cubvh.cuBVH(v, f)
     rng = np.random.default_rng(17)
