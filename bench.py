@@ -678,10 +678,15 @@ def run_ours(args):
             check(L.cubvh_floodfill_workspace_size(1, res, res, res, ctypes.byref(nb)), "ws")
             ws = torch.empty(nb.value, dtype=torch.uint8, device=dev)
 
-            def fn(res=res, grid=grid, lab=lab, ws=ws, nb=nb.value):
+            # the occupancy grid (the floodfill's input) is made from this
+            # step's UDF by its own timed op, so floodfill times its kernels only
+            def occ(res=res, grid=grid):
                 torch.lt(occ_src.view(res, res, res), 2.0 / res, out=grid)
+
+            def fn(res=res, grid=grid, lab=lab, ws=ws, nb=nb.value):
                 check(L.cubvh_floodfill(P(grid), 1, res, res, res, P(lab), P(ws), nb, sp), "floodfill")
-            dev_ops.append((op, 0, fn, "floodfill: 11 kernels"))
+            dev_ops.append(("occupancy", 0, occ, "occupancy: udf < 2/res (torch.lt)"))
+            dev_ops.append((op, 0, fn, "floodfill: tile, merge, resolve and label kernels"))
 
     q_per_step = sum(n for _, n, _, _ in dev_ops)
 
@@ -835,6 +840,10 @@ def run_ours(args):
                     d["ref_traversal_tris_per_query"] = counts[o][1]
             if o == "floodfill" and ff_host_ms is not None:
                 d["e2e_host_pageable_ms"] = ff_host_ms
+            if o in GRID_OPS:  # 1 B in + 4 B out (floodfill), 4 B in + 4 B out (udf_to_sdf) per voxel
+                gbs = (5.0 if o == "floodfill" else 8.0) * args.grid ** 3 / (per_op_ms[i] / 1e3) / 1e9
+                d["hbm_gbs"] = gbs
+                d["hbm_frac"] = gbs / peak
             ops_detail[o] = d
         parity = parity_sample(wl, op_outs)
         ref_cuda = None

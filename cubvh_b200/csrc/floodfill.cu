@@ -12,23 +12,31 @@
 //
 // Algorithm (four kernels, no host round trip).  A row is W consecutive
 // voxels of memory; a run is a maximal stretch of free voxels in a row.
-//   1. tile     one block per tile of T consecutive rows of one z-slice:
-//               packs the tile's free-voxel bitmask (one 32-bit word per 32
-//               voxels) into shared memory and global memory, counts run
-//               starts per row and per word, numbers the tile's runs in
-//               linear order (run id = tile * capacity + index in tile, so
+//   1. tile     one block per tile of T consecutive rows of one z-slice,
+//               four bitmask words per thread: packs the tile's free-voxel
+//               bitmask (one 32-bit word per 32 voxels) into shared and
+//               global memory, marks run starts per word, numbers the tile's
+//               runs in linear order with one block-wide scan of the words'
+//               start counts (run id = tile * capacity + index in tile, so
 //               run ids are ordered like the runs' first voxels), unites the
-//               runs of adjacent rows of the tile (y - 1) in a union-find in
-//               shared memory (global memory for tiles with more runs than
-//               fit), and stores every run's root within the tile
+//               runs of adjacent rows of the tile (y - 1) word by word in a
+//               union-find in shared memory (global memory for tiles with
+//               more runs than fit), and stores every run's root within the
+//               tile
 //   2. merge    unites runs across tiles: every row with its z - 1 row, and
 //               the first row of each tile with the last row of the tile
 //               above; lock-free union-find on the global roots that always
 //               links the larger root under the smaller, so every root is
 //               its component's smallest run id, i.e. smallest voxel index
 //   3. resolve  every run's label = its root's first voxel
-//   4. label    the int32 labels, 16-byte streaming stores (or the signed
-//               distances of udf_to_sdf)
+//   4. label    one block per tile: the tile's run labels, start marks and
+//               run bases staged in shared memory, then the int32 labels (or
+//               the signed distances of udf_to_sdf) written with 16-byte
+//               streaming stores; rows of W % 32 != 0 voxels: a warp per 32
+//               words
+// Per bitmask word the tile kernel keeps its run starts (starts) and the
+// global id of the last run that starts before it (wbase: the run covering
+// bit x of word w is wbase[w] + popc(starts[w] & bits 0..x) - 1).
 #include <algorithm>
 #include <climits>
 #include <cstdint>
@@ -41,19 +49,23 @@ namespace cubvh {
 namespace {
 
 constexpr int kStepLimit = 1 << 24;   // bound on any union-find walk
-constexpr int kTileThreads = 512;
-constexpr int kTileWords = 2048;       // bitmask words of a tile (8 KB of shared memory)
-constexpr int kSmemRuns = 6144;        // a tile's runs unite in shared memory up to this count
+// 256 threads and 1,024 words per tile: four tiles in flight per SM (512
+// threads: tile kernel 93 -> 73 us at 512^3; 128 threads: the tile kernel is
+// faster still but the merge, with twice the tile boundaries, slower)
+constexpr int kTileThreads = 256;
+constexpr int kTileWarps = kTileThreads / 32;
+constexpr int kTileBlocksPerSM = 1024 / kTileThreads;
+constexpr int kTileWords = 4 * kTileThreads;   // bitmask words per tile chunk: four per thread
+constexpr int kSmemRuns = 12 * kTileThreads;   // a tile's runs unite (and are labelled) in shared memory up to this count
 
 struct FFPlan {
     int64_t rows, wpr, words, ntot;
     int H, W;
+    int wpr_shift;                     // log2(wpr) when wpr is a power of two, else -1
     int tile_rows;                     // T: rows per tile; a tile never spans two z-slices
     int64_t tiles_per_slice, ntiles;
     int64_t cap;                       // run ids per tile: T * ceil(W / 2)
-    bool bits_in_smem;
-    size_t smem_bytes;
-    size_t off_bits, off_wpref, off_rowoff, off_tcount, off_start, off_parent, off_status, total;
+    size_t off_bits, off_starts, off_wbase, off_tcount, off_start, off_parent, off_status, total;
 };
 
 inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -65,7 +77,11 @@ FFPlan make_plan(int B, int H, int W, int D) {
     p.wpr = (W + 31) / 32;
     p.words = p.rows * p.wpr;
     p.ntot = p.rows * W;
-    // rows per tile: about kTileWords words, the slice split evenly
+    p.wpr_shift = -1;
+    for (int k = 0; k < 31; ++k)
+        if (((int64_t)1 << k) == p.wpr) p.wpr_shift = k;
+    // rows per tile: about kTileWords words (one chunk), the slice split evenly;
+    // rows of more than kTileWords words: one row per tile, in several chunks
     const int64_t tmax = std::max<int64_t>(1, std::min<int64_t>(H, kTileWords / std::max<int64_t>(p.wpr, 1)));
     p.tiles_per_slice = (H + tmax - 1) / tmax;
     p.tile_rows = (int)((H + p.tiles_per_slice - 1) / p.tiles_per_slice);
@@ -77,19 +93,22 @@ FFPlan make_plan(int B, int H, int W, int D) {
         p.cap = (W + 1) / 2;
     }
     p.ntiles = (int64_t)B * D * p.tiles_per_slice;
-    p.bits_in_smem = (int64_t)p.tile_rows * p.wpr <= kTileWords;
-    p.smem_bytes = sizeof(uint32_t) * ((p.bits_in_smem ? (size_t)p.tile_rows * p.wpr : 0) + (p.tile_rows + 1) + 32 +
-                                       kSmemRuns);
     size_t o = 0;
     p.off_bits = o; o = align256(o + sizeof(uint32_t) * p.words);
-    p.off_wpref = o; o = align256(o + sizeof(uint32_t) * p.words);
-    p.off_rowoff = o; o = align256(o + sizeof(uint32_t) * p.rows);
+    p.off_starts = o; o = align256(o + sizeof(uint32_t) * p.words);
+    p.off_wbase = o; o = align256(o + sizeof(uint32_t) * p.words);
     p.off_tcount = o; o = align256(o + sizeof(uint32_t) * p.ntiles);
     p.off_start = o; o = align256(o + sizeof(int32_t) * p.ntiles * p.cap);
     p.off_parent = o; o = align256(o + sizeof(int32_t) * p.ntiles * p.cap);
     p.off_status = o; o = align256(o + 16);
     p.total = o;
     return p;
+}
+
+// Row and position in the row of bitmask word w.
+__device__ __forceinline__ void word_pos(int64_t w, int64_t wpr, int shift, int64_t& row, int64_t& wi) {
+    if (shift >= 0) { row = w >> shift; wi = w & (wpr - 1); }
+    else { row = w / wpr; wi = w - row * wpr; }
 }
 
 __device__ __forceinline__ uint32_t starts_of(uint32_t f, uint32_t prev_word) {
@@ -229,117 +248,155 @@ __device__ __forceinline__ void pack_vec(const UdfSrc& s, int64_t v0, int nwords
     }
 }
 
-// 1. One block per tile (rows r0 .. r0 + T - 1 of one z-slice).
+// Exclusive scan of one value per thread over the block (kTileThreads
+// threads); *total receives the block's sum.  Called by all threads; wsum:
+// kTileWarps + 1 words of shared memory, free again after the next barrier.
+__device__ __forceinline__ uint32_t block_exclusive(uint32_t v, uint32_t* wsum, uint32_t* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+        if (lane >= o) inc += t;
+    }
+    if (lane == 31) wsum[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t x = lane < kTileWarps ? wsum[lane] : 0u;
+        uint32_t xi = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, xi, o);
+            if (lane >= o) xi += t;
+        }
+        if (lane < kTileWarps) wsum[lane] = xi - x;     // exclusive warp offsets
+        if (lane == kTileWarps - 1) wsum[kTileWarps] = xi;
+    }
+    __syncthreads();
+    *total = wsum[kTileWarps];
+    return wsum[warp] + inc - v;
+}
+
+// 1. One block per tile (rows r0 .. r0 + T - 1 of one z-slice), in chunks
+// of kTileWords bitmask words (one chunk unless a row has more words; such
+// tiles hold one row, whose runs have no y - 1 neighbour inside the tile).
+// Thread t owns words 4t .. 4t + 3 of the chunk.
 template <class Src>
-__global__ void __launch_bounds__(kTileThreads, 2)
-k_ff_tile(Src src, int W, int64_t wpr, int T, int64_t tiles_per_slice, int H, int64_t cap, bool bits_in_smem,
-          uint32_t* __restrict__ bits, uint32_t* __restrict__ wpref, uint32_t* __restrict__ rowoff,
+__global__ void __launch_bounds__(kTileThreads, kTileBlocksPerSM)
+k_ff_tile(Src src, int W, int64_t wpr, int shift, int T, int64_t tiles_per_slice, int H, int64_t cap,
+          uint32_t* __restrict__ bits, uint32_t* __restrict__ starts, uint32_t* __restrict__ wbase,
           uint32_t* __restrict__ tcount, int32_t* __restrict__ start, int32_t* __restrict__ parent,
           int* __restrict__ status) {
-    extern __shared__ uint32_t smem[];
+    __shared__ __align__(16) uint32_t sbits[kTileWords];
+    __shared__ __align__(16) uint32_t sw[kTileWords];   // runs of the tile before each word
+    __shared__ uint32_t wsum[32];
+    __shared__ int32_t spar[kSmemRuns];
     const int64_t tile = blockIdx.x;
     const int64_t slice = tile / tiles_per_slice;
     const int y0 = (int)(tile - slice * tiles_per_slice) * T;
     const int nrow = min(T, H - y0);                  // rows of this tile
     const int64_t r0 = slice * H + y0;                // first row
     const int64_t tbase = tile * cap;                 // first run id of the tile
-    const int nwords = (int)(nrow * wpr);
-    uint32_t* sbits = smem;
-    uint32_t* rowbase = smem + (bits_in_smem ? (int64_t)T * wpr : 0);   // [T + 1]
-    uint32_t* wsum = rowbase + T + 1;                                  // [32]
-    int32_t* spar = reinterpret_cast<int32_t*>(wsum + 32);             // [kSmemRuns]
-    uint32_t* gbits = bits + r0 * wpr;
-
-    // bitmask of the tile
-    uint32_t* sout = bits_in_smem ? sbits : nullptr;
-    if (src.vec) {
-        pack_vec(src, r0 * W, nwords, sout, gbits);
-    } else {
-        const int lane = threadIdx.x & 31;
-        for (int k = threadIdx.x >> 5; k < nwords; k += kTileThreads / 32) {
-            const int row = (int)(k / wpr);
-            const int x = (int)(k - (int64_t)row * wpr) * 32 + lane;
-            const bool fr = x < W && src.free_at((r0 + row) * W + x);
-            const uint32_t m = __ballot_sync(0xFFFFFFFFu, fr);
-            if (lane == 0) put_word(sout, gbits, k, m);
-        }
-    }
-    __syncthreads();
-    const uint32_t* tb = bits_in_smem ? sbits : gbits;
-    // run starts per row and per word
-    for (int k = threadIdx.x; k < nrow; k += kTileThreads) {
-        uint32_t prev = 0, acc = 0;
-        for (int64_t w = 0; w < wpr; ++w) {
-            const uint32_t f = tb[k * wpr + w];
-            wpref[(r0 + k) * wpr + w] = acc;
-            acc += __popc(starts_of(f, prev));
-            prev = f;
-        }
-        rowbase[k] = acc;
-    }
-    __syncthreads();
-    // exclusive scan of the row counts (rowbase[nrow] = the tile's runs)
-    {
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        constexpr int kWarps = kTileThreads / 32;
-        const int per = (nrow + kTileThreads - 1) / kTileThreads;
-        const int b0 = threadIdx.x * per, b1 = min(b0 + per, nrow);
-        uint32_t sum = 0;
-        for (int i = b0; i < b1; ++i) sum += rowbase[i];
-        uint32_t inc = sum;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, inc, o);
-            if (lane >= o) inc += t;
-        }
-        if (lane == 31) wsum[warp] = inc;
-        __syncthreads();
-        if (warp == 0) {
-            uint32_t v = lane < kWarps ? wsum[lane] : 0u, vi = v;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, vi, o);
-                if (lane >= o) vi += t;
-            }
-            if (lane < kWarps) wsum[lane] = vi - v;   // exclusive warp offsets
-        }
-        __syncthreads();
-        uint32_t run = wsum[warp] + inc - sum;
-        for (int i = b0; i < b1; ++i) {
-            const uint32_t c = rowbase[i];
-            rowbase[i] = run;
-            run += c;
-        }
-        if (b0 < nrow && b1 == nrow) rowbase[nrow] = run;
-    }
-    __syncthreads();
-    const int32_t nruns = (int32_t)rowbase[nrow];
-    int32_t* par = nruns <= kSmemRuns ? spar : parent + tbase;
-    if (threadIdx.x == 0) tcount[tile] = (uint32_t)nruns;
-    // run records: rowoff, the runs' first voxels, self parents
-    for (int k = threadIdx.x; k < nrow; k += kTileThreads) {
-        const int64_t r = r0 + k;
-        rowoff[r] = (uint32_t)(tbase + rowbase[k]);
-        int32_t id = (int32_t)rowbase[k];
-        uint32_t prev = 0;
-        for (int64_t w = 0; w < wpr; ++w) {
-            const uint32_t f = tb[k * wpr + w];
-            uint32_t sw = starts_of(f, prev);
-            prev = f;
-            while (sw) {
-                const int x = __ffs(sw) - 1;
-                sw &= sw - 1;
-                start[tbase + id] = (int32_t)(r * W + w * 32 + x);   // < 2^31 voxels (host check)
-                par[id] = id;
-                ++id;
+    const int64_t w0 = r0 * wpr;                      // first word
+    const int64_t nwords = (int64_t)nrow * wpr;
+    const bool one = nwords <= kTileWords;
+    const int t4 = 4 * (int)threadIdx.x;
+    int32_t* par = parent + tbase;                    // shared memory when the tile's runs fit
+    uint32_t carry = 0;                               // runs in earlier chunks
+    for (int64_t c0 = 0; c0 < nwords; c0 += kTileWords) {
+        const int nw = (int)min((int64_t)kTileWords, nwords - c0);
+        const int64_t g0 = w0 + c0;                   // first word of the chunk
+        // free-voxel bitmask of the chunk
+        if (src.vec) {
+            pack_vec(src, g0 * 32, nw, sbits, bits + g0);
+        } else {
+            const int lane = threadIdx.x & 31;
+            for (int k = threadIdx.x >> 5; k < nw; k += kTileWarps) {
+                int64_t row, wi;
+                word_pos(g0 + k, wpr, shift, row, wi);
+                const int x = (int)wi * 32 + lane;
+                const bool fr = x < W && src.free_at(row * W + x);
+                const uint32_t m = __ballot_sync(0xFFFFFFFFu, fr);
+                if (lane == 0) put_word(sbits, bits + g0, k, m);
             }
         }
+        __syncthreads();
+        // run starts of the thread's words, their counts scanned over the block
+        uint32_t st[4], tot = 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int w = t4 + j;
+            st[j] = 0u;
+            if (w < nw) {
+                int64_t row, wi;
+                word_pos(g0 + w, wpr, shift, row, wi);
+                const uint32_t prev = wi == 0 ? 0u : (w > 0 ? sbits[w - 1] : bits[g0 - 1]);
+                st[j] = starts_of(sbits[w], prev);
+            }
+            tot += __popc(st[j]);
+        }
+        uint32_t total;
+        const uint32_t ex = carry + block_exclusive(tot, wsum, &total);
+        if (one) par = carry + total <= (uint32_t)kSmemRuns ? spar : parent + tbase;
+        // per word: its starts, its run base, and each run's first voxel and self parent
+        uint32_t run = ex;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int w = t4 + j;
+            if (w < nw) {
+                sw[w] = run;
+                starts[g0 + w] = st[j];
+                wbase[g0 + w] = (uint32_t)(tbase + run);
+                if (st[j]) {
+                    int64_t row, wi;
+                    word_pos(g0 + w, wpr, shift, row, wi);
+                    const int64_t v0 = row * W + wi * 32;   // < 2^31 voxels (host check)
+                    uint32_t sj = st[j];
+                    int32_t id = (int32_t)run;
+                    while (sj) {
+                        const int x = __ffs(sj) - 1;
+                        sj &= sj - 1;
+                        start[tbase + id] = (int32_t)(v0 + x);
+                        par[id] = id;
+                        ++id;
+                    }
+                }
+            }
+            run += __popc(st[j]);
+        }
+        carry += total;
+        __syncthreads();
     }
-    __syncthreads();
-    // y - 1 neighbours inside the tile
-    for (int k = threadIdx.x + 1; k < nrow; k += kTileThreads)
-        unite_rows(tb + k * wpr, tb + (k - 1) * wpr, wpr, (int32_t)rowbase[k], (int32_t)rowbase[k - 1], par, status);
-    __syncthreads();
+    const int32_t nruns = (int32_t)carry;
+    if (threadIdx.x == 0) tcount[tile] = carry;
+    // y - 1 neighbours inside the tile, word by word: at every maximal common
+    // free segment and every run start inside one, unite the two runs
+    // covering that voxel (uniting rows in binary-tree rounds instead, which
+    // bounds the forest's depth, measured 40 % slower: the rounds' barriers
+    // cost more than the longer paths)
+    if (one && nrow > 1) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int w = t4 + j;
+            if (w < wpr || w >= nwords) continue;
+            const int q = w - (int)wpr;
+            int64_t row, wi;
+            word_pos(w0 + w, wpr, shift, row, wi);
+            const uint32_t pw = wi ? sbits[w - 1] : 0u, pq = wi ? sbits[q - 1] : 0u;
+            const uint32_t f = sbits[w], fq = sbits[q];
+            const uint32_t sr = starts_of(f, pw), sq = starts_of(fq, pq);
+            const uint32_t m = f & fq;
+            uint32_t ev = m & (starts_of(m, pw & pq) | sr | sq);
+            while (ev) {
+                const int x = __ffs(ev) - 1;
+                ev &= ev - 1;
+                const uint32_t upto = (x == 31) ? 0xFFFFFFFFu : ((2u << x) - 1u);
+                uf_union(par, (int32_t)(sw[w] + __popc(sr & upto)) - 1, (int32_t)(sw[q] + __popc(sq & upto)) - 1,
+                         status);
+            }
+        }
+        __syncthreads();
+    }
     // roots within the tile (in place, local ids), then as global run ids
     for (int32_t i = threadIdx.x; i < nruns; i += kTileThreads) par[i] = uf_root(par, i, status);
     __syncthreads();
@@ -348,7 +405,8 @@ k_ff_tile(Src src, int W, int64_t wpr, int T, int64_t tiles_per_slice, int H, in
 
 // 2. Unions across tiles: row r with its z - 1 row (r - H), and the first row
 // of a tile with the row above it (y - 1) when that row is in another tile.
-__global__ void k_ff_merge(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ rowoff,
+// A row's first run is the run base of its first word.
+__global__ void k_ff_merge(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ wbase,
                            int32_t* __restrict__ parent, int* __restrict__ status, int64_t rows, int64_t wpr, int H,
                            int D, int T) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -360,7 +418,8 @@ __global__ void k_ff_merge(const uint32_t* __restrict__ bits, const uint32_t* __
     if (dir == 0 && (y == 0 || y % T != 0)) return;
     if (dir == 1 && z == 0) return;
     const int64_t q = r - (dir == 0 ? 1 : H);
-    unite_rows(bits + r * wpr, bits + q * wpr, wpr, (int32_t)rowoff[r], (int32_t)rowoff[q], parent, status);
+    unite_rows(bits + r * wpr, bits + q * wpr, wpr, (int32_t)wbase[r * wpr], (int32_t)wbase[q * wpr], parent,
+               status);
 }
 
 // 3. start[run] := start[root] for every run (a root's own entry is already
@@ -380,94 +439,87 @@ __global__ void k_ff_resolve(const uint32_t* __restrict__ tcount, int64_t ntiles
     }
 }
 
-// 5b. labels: one warp writes 32 consecutive voxels per store (128 B).  Lane
-// k of the warp decodes word w0 + k once (its row, its first voxel and how
-// many of its 32 bits lie inside the row); the loop over the 32 words then
-// only shuffles those values.
-__global__ void k_write(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ rowoff,
-                        const uint32_t* __restrict__ wpref, const int32_t* __restrict__ runlab,
-                        int32_t* __restrict__ labels, int64_t rows, int64_t wpr, int W) {
-    const int lane = threadIdx.x & 31;
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    const int64_t words = rows * wpr;
-    const uint32_t below = (lane == 31) ? 0xFFFFFFFFu : ((2u << lane) - 1u);
-    for (int64_t w0 = warp * 32; w0 < words; w0 += nwarps * 32) {
-        const int64_t wk = w0 + lane;
-        uint32_t f = 0, s = 0, base = 0, vb = 0;
-        int nval = 0;
-        if (wk < words) {
-            const int64_t r = wk / wpr, wi = wk - r * wpr;
-            f = bits[wk];
-            const uint32_t prev = wi > 0 ? bits[wk - 1] : 0u;
-            s = starts_of(f, prev);
-            base = rowoff[r] + wpref[wk];
-            vb = (uint32_t)(r * W + wi * 32);   // < 2^31 voxels (checked on the host)
-            nval = min(32, W - (int)wi * 32);
+// 4 (W % 32 == 0, 16-byte aligned output).  One block per tile: the tile's
+// run labels (up to kSmemRuns) and its words' free bits, run starts and run
+// bases (tile-relative) are staged in shared memory with coalesced loads,
+// then each thread writes groups of 4 voxels (bits 4k .. 4k + 3 of a word)
+// with 16-byte streaming stores, consecutive threads consecutive groups.
+// SDF: the signed distance s = udf - eps instead of the label, negated where
+// the voxel's label (-1 when occupied) differs from the label of its
+// volume's first voxel (b, 0, 0, 0) and s > 0.
+template <bool SDF>
+__global__ void __launch_bounds__(kTileThreads)
+k_write_tile(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ starts,
+             const uint32_t* __restrict__ wbase, const uint32_t* __restrict__ tcount,
+             const int32_t* __restrict__ runlab, int64_t wpr, int T, int64_t tiles_per_slice, int H, int64_t cap,
+             int4* __restrict__ labels, const float4* __restrict__ udf, float4* __restrict__ sdf,
+             int64_t rows_per_volume, float eps) {
+    __shared__ int32_t slab[kSmemRuns];
+    __shared__ __align__(16) uint32_t sf[kTileWords], ss[kTileWords], sb[kTileWords];
+    const int64_t tile = blockIdx.x;
+    const int64_t slice = tile / tiles_per_slice;
+    const int y0 = (int)(tile - slice * tiles_per_slice) * T;
+    const int nrow = min(T, H - y0);
+    const int64_t r0 = slice * H + y0;
+    const int64_t tbase = tile * cap;
+    const int64_t w0 = r0 * wpr;
+    const int64_t nwords = (int64_t)nrow * wpr;
+    const uint32_t n = tcount[tile];
+    const bool inl = n <= (uint32_t)kSmemRuns;
+    if (inl)
+        for (uint32_t i = threadIdx.x; i < n; i += kTileThreads) slab[i] = runlab[tbase + i];
+    const int32_t* lab = inl ? slab : runlab + tbase;
+    int32_t empty = -1;
+    if (SDF) {
+        const int64_t rv = (r0 / rows_per_volume) * rows_per_volume;
+        if (bits[rv * wpr] & 1u) empty = runlab[wbase[rv * wpr]];
+    }
+    for (int64_t c0 = 0; c0 < nwords; c0 += kTileWords) {
+        const int nw = (int)min((int64_t)kTileWords, nwords - c0);
+        const int64_t g0 = w0 + c0;
+        for (int k = threadIdx.x; k < nw; k += kTileThreads) {
+            sf[k] = bits[g0 + k];
+            ss[k] = starts[g0 + k];
+            sb[k] = (uint32_t)(wbase[g0 + k] - tbase);
         }
-        const int nw = (int)min((int64_t)32, words - w0);
-        for (int k = 0; k < nw; ++k) {
-            const uint32_t fk = __shfl_sync(0xFFFFFFFFu, f, k);
-            const uint32_t sk = __shfl_sync(0xFFFFFFFFu, s, k);
-            const uint32_t bk = __shfl_sync(0xFFFFFFFFu, base, k);
-            const uint32_t vk = __shfl_sync(0xFFFFFFFFu, vb, k);
-            const int nk = __shfl_sync(0xFFFFFFFFu, nval, k);
-            if (lane < nk) {
-                int32_t lab = -1;
-                if ((fk >> lane) & 1u) lab = __ldg(runlab + (bk + __popc(sk & below) - 1));
-                __stcs(labels + vk + lane, lab);
+        __syncthreads();
+        for (int g = threadIdx.x; g < 8 * nw; g += kTileThreads) {
+            const size_t i4 = (size_t)g0 * 8 + g;     // 16-byte group of the whole grid
+            float4 u = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (SDF) u = __ldcs(udf + i4);
+            const int k = g >> 3;
+            const uint32_t q = (uint32_t)(g & 7) * 4;
+            const uint32_t f = sf[k], st = ss[k], base = sb[k];
+            uint32_t cnt = base + __popc(st & ((1u << q) - 1u));   // runs starting before bit q, plus the base
+            int32_t o[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                cnt += (st >> (q + j)) & 1u;
+                o[j] = ((f >> (q + j)) & 1u) ? lab[cnt - 1] : -1;
+            }
+            if (SDF) {
+                float d[4] = {__fsub_rn(u.x, eps), __fsub_rn(u.y, eps), __fsub_rn(u.z, eps), __fsub_rn(u.w, eps)};
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (o[j] != empty && d[j] > 0.f) d[j] = -d[j];
+                __stcs(sdf + i4, make_float4(d[0], d[1], d[2], d[3]));
+            } else {
+                __stcs(labels + i4, make_int4(o[0], o[1], o[2], o[3]));
             }
         }
+        __syncthreads();
     }
 }
 
-// 5b (W % 32 == 0, 16-byte aligned output).  Rows hold whole words, so voxel
-// 32 w + b is bit b of word w.  A warp covers 4 words (128 voxels) per step:
-// lane l takes word l / 8 and its 4 bits from 4 (l % 8), and writes their
-// labels with one 16-byte streaming store (512 contiguous bytes per warp).
-struct WordRuns {
-    uint32_t f, s, base;   // free bits, run starts, run id of the run before the word's first start
-};
-__device__ __forceinline__ WordRuns word_runs(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ rowoff,
-                                              const uint32_t* __restrict__ wpref, uint32_t w, uint32_t wpr) {
-    const uint32_t r = w / wpr, wi = w - r * wpr;
-    const uint32_t f = bits[w];
-    return WordRuns{f, starts_of(f, wi ? bits[w - 1] : 0u), rowoff[r] + wpref[w]};
-}
-// labels of bits q .. q + 3 of the word (-1 where occupied)
-__device__ __forceinline__ void labels4(const WordRuns& wr, const int32_t* __restrict__ runlab, uint32_t q,
-                                        int32_t o[4]) {
-    uint32_t cnt = __popc(wr.s & ((1u << q) - 1u));   // run starts below bit q
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        cnt += (wr.s >> (q + j)) & 1u;
-        o[j] = ((wr.f >> (q + j)) & 1u) ? __ldg(runlab + (wr.base + cnt - 1)) : -1;
-    }
-}
-__global__ void k_write4(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ rowoff,
-                         const uint32_t* __restrict__ wpref, const int32_t* __restrict__ runlab,
-                         int4* __restrict__ labels, uint32_t words, uint32_t wpr) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t sub = (uint32_t)lane >> 3, q = (uint32_t)(lane & 7) * 4;
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t c = warp; c * 4 < (int64_t)words; c += nwarps) {
-        const uint32_t w = (uint32_t)(c * 4) + sub;
-        if (w >= words) continue;
-        int32_t o[4];
-        labels4(word_runs(bits, rowoff, wpref, w, wpr), runlab, q, o);
-        __stcs(labels + (size_t)w * 8 + (lane & 7), make_int4(o[0], o[1], o[2], o[3]));
-    }
-}
-
-// 5'. signed distances instead of labels: s = udf - eps, negated where the
-// voxel's label (-1 when occupied) differs from the label of its volume's
-// first voxel (b, 0, 0, 0) and s > 0.  Same traversal of the run tables as
-// k_write; the first voxel's label is its row's first run when it is free.
-__global__ void k_write_sdf(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ rowoff,
-                            const uint32_t* __restrict__ wpref, const int32_t* __restrict__ runlab,
-                            const float* __restrict__ udf, float* __restrict__ sdf, int64_t rows, int64_t wpr,
-                            int W, int64_t rows_per_volume, float eps) {
+// 4 (rows of W % 32 != 0 voxels): one warp writes 32 consecutive voxels per
+// store (128 B).  Lane k of the warp decodes word w0 + k once (its row, its
+// first voxel and how many of its 32 bits lie inside the row); the loop over
+// the 32 words then only shuffles those values.  SDF as k_write_tile.
+template <bool SDF>
+__global__ void k_write_rows(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ starts,
+                             const uint32_t* __restrict__ wbase, const int32_t* __restrict__ runlab,
+                             int32_t* __restrict__ labels, const float* __restrict__ udf, float* __restrict__ sdf,
+                             int64_t rows, int64_t wpr, int W, int64_t rows_per_volume, float eps) {
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -481,13 +533,14 @@ __global__ void k_write_sdf(const uint32_t* __restrict__ bits, const uint32_t* _
         if (wk < words) {
             const int64_t r = wk / wpr, wi = wk - r * wpr;
             f = bits[wk];
-            const uint32_t prev = wi > 0 ? bits[wk - 1] : 0u;
-            s = starts_of(f, prev);
-            base = rowoff[r] + wpref[wk];
-            vb = (uint32_t)(r * W + wi * 32);
+            s = starts[wk];
+            base = wbase[wk];
+            vb = (uint32_t)(r * W + wi * 32);   // < 2^31 voxels (checked on the host)
             nval = min(32, W - (int)wi * 32);
-            const int64_t r0 = (r / rows_per_volume) * rows_per_volume;
-            if (bits[r0 * wpr] & 1u) empty = __ldg(runlab + rowoff[r0]);
+            if (SDF) {
+                const int64_t rv = (r / rows_per_volume) * rows_per_volume;
+                if (bits[rv * wpr] & 1u) empty = __ldg(runlab + wbase[rv * wpr]);
+            }
         }
         const int nw = (int)min((int64_t)32, words - w0);
         for (int k = 0; k < nw; ++k) {
@@ -496,54 +549,32 @@ __global__ void k_write_sdf(const uint32_t* __restrict__ bits, const uint32_t* _
             const uint32_t bk = __shfl_sync(0xFFFFFFFFu, base, k);
             const uint32_t vk = __shfl_sync(0xFFFFFFFFu, vb, k);
             const int nk = __shfl_sync(0xFFFFFFFFu, nval, k);
-            const int32_t ek = __shfl_sync(0xFFFFFFFFu, empty, k);
+            const int32_t ek = SDF ? __shfl_sync(0xFFFFFFFFu, empty, k) : -1;
             if (lane < nk) {
                 int32_t lab = -1;
                 if ((fk >> lane) & 1u) lab = __ldg(runlab + (bk + __popc(sk & below) - 1));
-                const float d = __fsub_rn(__ldcs(udf + vk + lane), eps);
-                __stcs(sdf + vk + lane, (lab != ek && d > 0.f) ? -d : d);
+                if (SDF) {
+                    const float d = __fsub_rn(__ldcs(udf + vk + lane), eps);
+                    __stcs(sdf + vk + lane, (lab != ek && d > 0.f) ? -d : d);
+                } else {
+                    __stcs(labels + vk + lane, lab);
+                }
             }
         }
-    }
-}
-// 5' (W % 32 == 0, 16-byte aligned udf and sdf): the k_write4 layout, one
-// 16-byte load of udf and one 16-byte store of sdf per lane.
-__global__ void k_write_sdf4(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ rowoff,
-                             const uint32_t* __restrict__ wpref, const int32_t* __restrict__ runlab,
-                             const float4* __restrict__ udf, float4* __restrict__ sdf, uint32_t words,
-                             uint32_t wpr, uint32_t rows_per_volume, float eps) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t sub = (uint32_t)lane >> 3, q = (uint32_t)(lane & 7) * 4;
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t c = warp; c * 4 < (int64_t)words; c += nwarps) {
-        const uint32_t w = (uint32_t)(c * 4) + sub;
-        if (w >= words) continue;
-        int32_t o[4];
-        labels4(word_runs(bits, rowoff, wpref, w, wpr), runlab, q, o);
-        const uint32_t r0 = (w / wpr / rows_per_volume) * rows_per_volume;
-        const int32_t empty = (bits[(size_t)r0 * wpr] & 1u) ? __ldg(runlab + rowoff[r0]) : -1;
-        const size_t i4 = (size_t)w * 8 + (lane & 7);
-        const float4 u = __ldcs(udf + i4);
-        float d[4] = {__fsub_rn(u.x, eps), __fsub_rn(u.y, eps), __fsub_rn(u.z, eps), __fsub_rn(u.w, eps)};
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-            if (o[j] != empty && d[j] > 0.f) d[j] = -d[j];
-        __stcs(sdf + i4, make_float4(d[0], d[1], d[2], d[3]));
     }
 }
 
 __global__ void k_zero(int* p) { *p = 0; }
 
 struct FFBufs {
-    uint32_t *bits, *wpref, *rowoff, *tcount;
+    uint32_t *bits, *starts, *wbase, *tcount;
     int32_t *start, *parent;
     int* status;
 };
 FFBufs carve(const FFPlan& p, void* ws) {
     char* base = static_cast<char*>(ws);
-    return FFBufs{reinterpret_cast<uint32_t*>(base + p.off_bits), reinterpret_cast<uint32_t*>(base + p.off_wpref),
-                  reinterpret_cast<uint32_t*>(base + p.off_rowoff), reinterpret_cast<uint32_t*>(base + p.off_tcount),
+    return FFBufs{reinterpret_cast<uint32_t*>(base + p.off_bits), reinterpret_cast<uint32_t*>(base + p.off_starts),
+                  reinterpret_cast<uint32_t*>(base + p.off_wbase), reinterpret_cast<uint32_t*>(base + p.off_tcount),
                   reinterpret_cast<int32_t*>(base + p.off_start), reinterpret_cast<int32_t*>(base + p.off_parent),
                   reinterpret_cast<int*>(base + p.off_status)};
 }
@@ -552,11 +583,11 @@ FFBufs carve(const FFPlan& p, void* ws) {
 template <class Src>
 void label_runs(const FFPlan& p, int D, const Src& src, const FFBufs& b, unsigned sgrid, cudaStream_t stream) {
     k_zero<<<1, 1, 0, stream>>>(b.status); count_launch();
-    k_ff_tile<Src><<<(unsigned)p.ntiles, kTileThreads, p.smem_bytes, stream>>>(
-        src, p.W, p.wpr, p.tile_rows, p.tiles_per_slice, p.H, p.cap, p.bits_in_smem, b.bits, b.wpref, b.rowoff,
+    k_ff_tile<Src><<<(unsigned)p.ntiles, kTileThreads, 0, stream>>>(
+        src, p.W, p.wpr, p.wpr_shift, p.tile_rows, p.tiles_per_slice, p.H, p.cap, b.bits, b.starts, b.wbase,
         b.tcount, b.start, b.parent, b.status); count_launch();
     const unsigned mgrid = (unsigned)((2 * p.rows + 255) / 256);
-    k_ff_merge<<<mgrid, 256, 0, stream>>>(b.bits, b.rowoff, b.parent, b.status, p.rows, p.wpr, p.H, D,
+    k_ff_merge<<<mgrid, 256, 0, stream>>>(b.bits, b.wbase, b.parent, b.status, p.rows, p.wpr, p.H, D,
                                           p.tile_rows); count_launch();
     k_ff_resolve<<<sgrid, 256, 0, stream>>>(b.tcount, p.ntiles, p.cap, b.parent, b.start, b.status); count_launch();
 }
@@ -582,10 +613,12 @@ cudaError_t launch_floodfill(const uint8_t* grid, int B, int H, int W, int D, in
     const GridSrc src{grid, W % 32 == 0 && (reinterpret_cast<uintptr_t>(grid) & 15) == 0};
     label_runs(p, D, src, b, sgrid, stream);
     if (W % 32 == 0 && (reinterpret_cast<uintptr_t>(labels) & 15) == 0) {
-        k_write4<<<sgrid, 256, 0, stream>>>(b.bits, b.rowoff, b.wpref, b.start, reinterpret_cast<int4*>(labels),
-                                            (uint32_t)p.words, (uint32_t)p.wpr); count_launch();
+        k_write_tile<false><<<(unsigned)p.ntiles, kTileThreads, 0, stream>>>(
+            b.bits, b.starts, b.wbase, b.tcount, b.start, p.wpr, p.tile_rows, p.tiles_per_slice, p.H, p.cap,
+            reinterpret_cast<int4*>(labels), nullptr, nullptr, 1, 0.f); count_launch();
     } else {
-        k_write<<<sgrid, 256, 0, stream>>>(b.bits, b.rowoff, b.wpref, b.start, labels, p.rows, p.wpr, W); count_launch();
+        k_write_rows<false><<<sgrid, 256, 0, stream>>>(b.bits, b.starts, b.wbase, b.start, labels, nullptr, nullptr,
+                                                       p.rows, p.wpr, W, 1, 0.f); count_launch();
     }
     return cudaGetLastError();
 }
@@ -600,13 +633,13 @@ cudaError_t launch_udf_to_sdf(const float* udf, int B, int H, int W, int D, floa
     const UdfSrc src{udf, eps, vec};
     label_runs(p, D, src, b, sgrid, stream);
     if (vec) {
-        k_write_sdf4<<<sgrid, 256, 0, stream>>>(b.bits, b.rowoff, b.wpref, b.start,
-                                                reinterpret_cast<const float4*>(udf), reinterpret_cast<float4*>(sdf),
-                                                (uint32_t)p.words, (uint32_t)p.wpr, (uint32_t)((int64_t)D * H), eps);
+        k_write_tile<true><<<(unsigned)p.ntiles, kTileThreads, 0, stream>>>(
+            b.bits, b.starts, b.wbase, b.tcount, b.start, p.wpr, p.tile_rows, p.tiles_per_slice, p.H, p.cap, nullptr,
+            reinterpret_cast<const float4*>(udf), reinterpret_cast<float4*>(sdf), (int64_t)D * H, eps);
         count_launch();
     } else {
-        k_write_sdf<<<sgrid, 256, 0, stream>>>(b.bits, b.rowoff, b.wpref, b.start, udf, sdf, p.rows, p.wpr, W,
-                                               (int64_t)D * H, eps); count_launch();
+        k_write_rows<true><<<sgrid, 256, 0, stream>>>(b.bits, b.starts, b.wbase, b.start, nullptr, udf, sdf, p.rows,
+                                                      p.wpr, W, (int64_t)D * H, eps); count_launch();
     }
     return cudaGetLastError();
 }

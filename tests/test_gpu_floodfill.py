@@ -13,6 +13,11 @@ pytestmark = pytest.mark.gpu
 @pytest.mark.parametrize("shape,p", [
     ((32, 32, 32), 0.45), ((1, 17, 9, 40), 0.3), ((3, 33, 31, 29), 0.35), ((2, 64, 64, 64), 0.55),
     ((1, 5, 7, 3), 0.2), ((1, 1, 1, 1), 0.0), ((1, 2, 3, 100), 0.4), ((1, 40, 1, 1), 0.1),
+    # tiles with more runs than the shared-memory union-find holds (global parents)
+    ((1, 64, 512, 4), 0.5),
+    # rows of more than 2048 bitmask words (tiles of one row in several chunks), with and
+    # without whole words per row
+    ((1, 3, 70016, 2), 0.3), ((1, 2, 70000, 1), 0.3),
 ])
 def test_floodfill_random(oracle, dev, shape, p):
     rng = np.random.default_rng(abs(hash(shape)) % 1000)
@@ -59,7 +64,8 @@ def test_floodfill_rejects_non_bool(dev):
         cubvh.floodfill(torch.zeros(4, 4, 4, dtype=torch.int32, device=dev))
 
 
-@pytest.mark.parametrize("shape", [(32, 32, 32), (2, 24, 17, 40), (1, 9, 64, 7), (3, 16, 16, 16)])
+@pytest.mark.parametrize("shape", [(32, 32, 32), (2, 24, 17, 40), (1, 9, 64, 7), (3, 16, 16, 16), (1, 64, 512, 4),
+                                   (1, 3, 70016, 2)])
 def test_udf_to_sdf_random(oracle, dev, shape):
     """Fused occupancy -> floodfill -> signed grid against the reference recipe
     (oracle floodfill + the same float32 arithmetic), bit for bit; includes
