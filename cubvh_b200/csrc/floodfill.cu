@@ -190,6 +190,7 @@ struct UdfSrc {
     const float* u;
     float eps;
     bool vec;
+    float* d;   // vec: receives udf - eps (the unsigned part of the signed grid) as the udf is read
     __device__ __forceinline__ bool free_at(int64_t i) const { return !(__ldg(u + i) < eps); }
 };
 
@@ -227,17 +228,21 @@ __device__ __forceinline__ void pack_vec(const GridSrc& s, int64_t v0, int nword
 }
 __device__ __forceinline__ void pack_vec(const UdfSrc& s, int64_t v0, int nwords, uint32_t* sout, uint32_t* gout) {
     const float4* u = reinterpret_cast<const float4*>(s.u + v0);
+    float4* d = reinterpret_cast<float4*>(s.d + v0);
     const int nch = 8 * nwords;  // 4 voxels per chunk
     for (int c0 = 0; c0 < nch; c0 += 4 * kTileThreads) {
         float4 v[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const int c = c0 + j * kTileThreads + (int)threadIdx.x;
-            v[j] = c < nch ? __ldg(u + c) : make_float4(0.f, 0.f, 0.f, 0.f);
+            v[j] = c < nch ? __ldcs(u + c) : make_float4(0.f, 0.f, 0.f, 0.f);
         }
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const int c = c0 + j * kTileThreads + (int)threadIdx.x;
+            if (c < nch)
+                __stcs(d + c, make_float4(__fsub_rn(v[j].x, s.eps), __fsub_rn(v[j].y, s.eps), __fsub_rn(v[j].z, s.eps),
+                                          __fsub_rn(v[j].w, s.eps)));
             uint32_t m = (!(v[j].x < s.eps) ? 1u : 0u) | (!(v[j].y < s.eps) ? 2u : 0u) |
                          (!(v[j].z < s.eps) ? 4u : 0u) | (!(v[j].w < s.eps) ? 8u : 0u);
             m |= __shfl_down_sync(0xFFFFFFFFu, m, 1) << 4;
@@ -446,14 +451,15 @@ __global__ void k_ff_resolve(const uint32_t* __restrict__ tcount, int64_t ntiles
 // with 16-byte streaming stores, consecutive threads consecutive groups.
 // SDF: the signed distance s = udf - eps instead of the label, negated where
 // the voxel's label (-1 when occupied) differs from the label of its
-// volume's first voxel (b, 0, 0, 0) and s > 0.
+// volume's first voxel (b, 0, 0, 0) and s > 0; the tile kernel has already
+// stored s (reading the udf once), so only groups holding a voxel to negate
+// are read and rewritten.
 template <bool SDF>
 __global__ void __launch_bounds__(kTileThreads)
 k_write_tile(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ starts,
              const uint32_t* __restrict__ wbase, const uint32_t* __restrict__ tcount,
              const int32_t* __restrict__ runlab, int64_t wpr, int T, int64_t tiles_per_slice, int H, int64_t cap,
-             int4* __restrict__ labels, const float4* __restrict__ udf, float4* __restrict__ sdf,
-             int64_t rows_per_volume, float eps) {
+             int4* __restrict__ labels, float4* __restrict__ sdf, int64_t rows_per_volume) {
     __shared__ int32_t slab[kSmemRuns];
     __shared__ __align__(16) uint32_t sf[kTileWords], ss[kTileWords], sb[kTileWords];
     const int64_t tile = blockIdx.x;
@@ -485,8 +491,6 @@ k_write_tile(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ sta
         __syncthreads();
         for (int g = threadIdx.x; g < 8 * nw; g += kTileThreads) {
             const size_t i4 = (size_t)g0 * 8 + g;     // 16-byte group of the whole grid
-            float4 u = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (SDF) u = __ldcs(udf + i4);
             const int k = g >> 3;
             const uint32_t q = (uint32_t)(g & 7) * 4;
             const uint32_t f = sf[k], st = ss[k], base = sb[k];
@@ -498,11 +502,22 @@ k_write_tile(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ sta
                 o[j] = ((f >> (q + j)) & 1u) ? lab[cnt - 1] : -1;
             }
             if (SDF) {
-                float d[4] = {__fsub_rn(u.x, eps), __fsub_rn(u.y, eps), __fsub_rn(u.z, eps), __fsub_rn(u.w, eps)};
+                // sdf already holds udf - eps (written by the tile kernel); a
+                // voxel flips when its label differs from the volume's first
+                // voxel's and the value is positive, which needs a free voxel
+                // (occupied ones have udf < eps), so groups without a free
+                // voxel of another component stay as they are
+                bool any = false;
 #pragma unroll
-                for (int j = 0; j < 4; ++j)
-                    if (o[j] != empty && d[j] > 0.f) d[j] = -d[j];
-                __stcs(sdf + i4, make_float4(d[0], d[1], d[2], d[3]));
+                for (int j = 0; j < 4; ++j) any |= o[j] >= 0 && o[j] != empty;
+                if (any) {
+                    const float4 v = sdf[i4];
+                    float d[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+                        if (o[j] != empty && d[j] > 0.f) d[j] = -d[j];
+                    __stcs(sdf + i4, make_float4(d[0], d[1], d[2], d[3]));
+                }
             } else {
                 __stcs(labels + i4, make_int4(o[0], o[1], o[2], o[3]));
             }
@@ -615,7 +630,7 @@ cudaError_t launch_floodfill(const uint8_t* grid, int B, int H, int W, int D, in
     if (W % 32 == 0 && (reinterpret_cast<uintptr_t>(labels) & 15) == 0) {
         k_write_tile<false><<<(unsigned)p.ntiles, kTileThreads, 0, stream>>>(
             b.bits, b.starts, b.wbase, b.tcount, b.start, p.wpr, p.tile_rows, p.tiles_per_slice, p.H, p.cap,
-            reinterpret_cast<int4*>(labels), nullptr, nullptr, 1, 0.f); count_launch();
+            reinterpret_cast<int4*>(labels), nullptr, 1); count_launch();
     } else {
         k_write_rows<false><<<sgrid, 256, 0, stream>>>(b.bits, b.starts, b.wbase, b.start, labels, nullptr, nullptr,
                                                        p.rows, p.wpr, W, 1, 0.f); count_launch();
@@ -630,12 +645,12 @@ cudaError_t launch_udf_to_sdf(const float* udf, int B, int H, int W, int D, floa
     const FFBufs b = carve(p, ws);
     const unsigned sgrid = stream_grid();
     const bool vec = W % 32 == 0 && ((reinterpret_cast<uintptr_t>(udf) | reinterpret_cast<uintptr_t>(sdf)) & 15) == 0;
-    const UdfSrc src{udf, eps, vec};
+    const UdfSrc src{udf, eps, vec, sdf};
     label_runs(p, D, src, b, sgrid, stream);
     if (vec) {
         k_write_tile<true><<<(unsigned)p.ntiles, kTileThreads, 0, stream>>>(
             b.bits, b.starts, b.wbase, b.tcount, b.start, p.wpr, p.tile_rows, p.tiles_per_slice, p.H, p.cap, nullptr,
-            reinterpret_cast<const float4*>(udf), reinterpret_cast<float4*>(sdf), (int64_t)D * H, eps);
+            reinterpret_cast<float4*>(sdf), (int64_t)D * H);
         count_launch();
     } else {
         k_write_rows<true><<<sgrid, 256, 0, stream>>>(b.bits, b.starts, b.wbase, b.start, nullptr, udf, sdf, p.rows,
