@@ -153,30 +153,6 @@ __device__ __forceinline__ int32_t uf_root(const int32_t* parent, int32_t x, int
     return x;
 }
 
-// Unites the runs of row r (run ids from cr0) with the overlapping runs of
-// row q (run ids from cq0): at every maximal common free segment and every
-// run start inside one, the two runs covering that voxel are united.
-__device__ __forceinline__ void unite_rows(const uint32_t* br, const uint32_t* bq, int64_t wpr, int32_t cr0,
-                                           int32_t cq0, int32_t* parent, int* status) {
-    uint32_t pr = 0, pq = 0, pm = 0;
-    int32_t cr = cr0, cq = cq0;
-    for (int64_t w = 0; w < wpr; ++w) {
-        const uint32_t fr = br[w], fq = bq[w];
-        const uint32_t sr = starts_of(fr, pr), sq = starts_of(fq, pq);
-        const uint32_t m = fr & fq;
-        uint32_t ev = m & (starts_of(m, pm) | sr | sq);
-        pr = fr; pq = fq; pm = m;
-        while (ev) {
-            const int x = __ffs(ev) - 1;
-            ev &= ev - 1;
-            const uint32_t upto = (x == 31) ? 0xFFFFFFFFu : ((2u << x) - 1u);
-            uf_union(parent, cr + __popc(sr & upto) - 1, cq + __popc(sq & upto) - 1, status);
-        }
-        cr += __popc(sr);
-        cq += __popc(sq);
-    }
-}
-
 // Free-voxel sources of the tile kernel: a bool grid (free = 0) or an
 // unsigned-distance grid thresholded at eps (free = !(udf < eps), so a NaN
 // distance is free).  vec: W % 32 == 0 and a 16-byte aligned array, so a
@@ -410,21 +386,86 @@ k_ff_tile(Src src, int W, int64_t wpr, int shift, int T, int64_t tiles_per_slice
 
 // 2. Unions across tiles: row r with its z - 1 row (r - H), and the first row
 // of a tile with the row above it (y - 1) when that row is in another tile.
-// A row's first run is the run base of its first word.
+// A row's first run is the run base of its first word.  At every maximal
+// common free segment of the two rows and every run start inside one, the
+// two runs covering that voxel are united, through their current parents
+// (the tile kernel left every run pointing at its tile root): consecutive
+// rows of a tile mostly give the same pair of roots, so each thread keeps
+// its first kMergePairs distinct pairs, lanes holding equal pairs are
+// matched across the warp, and one lane per pair unites it (further pairs
+// are united directly).
+constexpr int kMergePairs = 4;
 __global__ void k_ff_merge(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ wbase,
                            int32_t* __restrict__ parent, int* __restrict__ status, int64_t rows, int64_t wpr, int H,
                            int D, int T) {
+    const int lane = threadIdx.x & 31;
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 2 * rows) return;
     const int64_t r = t >> 1;
     const int dir = (int)(t & 1);
-    const int64_t rl = r % ((int64_t)D * H);
-    const int y = (int)(rl % H), z = (int)(rl / H);
-    if (dir == 0 && (y == 0 || y % T != 0)) return;
-    if (dir == 1 && z == 0) return;
-    const int64_t q = r - (dir == 0 ? 1 : H);
-    unite_rows(bits + r * wpr, bits + q * wpr, wpr, (int32_t)wbase[r * wpr], (int32_t)wbase[q * wpr], parent,
-               status);
+    bool valid = t < 2 * rows;
+    if (valid) {
+        const int64_t rl = r % ((int64_t)D * H);
+        const int y = (int)(rl % H), z = (int)(rl / H);
+        valid = dir == 0 ? (y != 0 && y % T == 0) : z != 0;
+    }
+    uint64_t pairs[kMergePairs];
+    int np = 0;
+    if (valid) {
+        const int64_t q = r - (dir == 0 ? 1 : H);
+        const uint32_t* br = bits + r * wpr;
+        const uint32_t* bq = bits + q * wpr;
+        int32_t cr = (int32_t)wbase[r * wpr], cq = (int32_t)wbase[q * wpr];
+        uint32_t pr = 0, pq = 0, pm = 0;
+        // words four at a time (16-byte loads when the rows are 16-byte aligned)
+        const bool v4 = (wpr & 3) == 0;
+        for (int64_t w0 = 0; w0 < wpr; w0 += 4) {
+            uint32_t fr4[4], fq4[4];
+            if (v4) {
+                const uint4 a = *reinterpret_cast<const uint4*>(br + w0), c = *reinterpret_cast<const uint4*>(bq + w0);
+                fr4[0] = a.x; fr4[1] = a.y; fr4[2] = a.z; fr4[3] = a.w;
+                fq4[0] = c.x; fq4[1] = c.y; fq4[2] = c.z; fq4[3] = c.w;
+            } else {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    fr4[j] = w0 + j < wpr ? br[w0 + j] : 0u;
+                    fq4[j] = w0 + j < wpr ? bq[w0 + j] : 0u;
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t fr = fr4[j], fq = fq4[j];
+                const uint32_t sr = starts_of(fr, pr), sq = starts_of(fq, pq);
+                const uint32_t m = fr & fq;
+                uint32_t ev = m & (starts_of(m, pm) | sr | sq);
+                pr = fr; pq = fq; pm = m;
+                while (ev) {
+                    const int x = __ffs(ev) - 1;
+                    ev &= ev - 1;
+                    const uint32_t upto = (x == 31) ? 0xFFFFFFFFu : ((2u << x) - 1u);
+                    const int32_t ra = parent[cr + __popc(sr & upto) - 1], rb = parent[cq + __popc(sq & upto) - 1];
+                    if (ra == rb) continue;
+                    const uint64_t key = ra < rb ? ((uint64_t)(uint32_t)ra << 32) | (uint32_t)rb
+                                                 : ((uint64_t)(uint32_t)rb << 32) | (uint32_t)ra;
+                    if (np > 0 && pairs[np - 1] == key) continue;
+                    if (np < kMergePairs) pairs[np++] = key;
+                    else uf_union(parent, ra, rb, status);
+                }
+                cr += __popc(sr);
+                cq += __popc(sq);
+            }
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < kMergePairs; ++e) {
+        const bool has = e < np;
+        const unsigned act = __ballot_sync(0xFFFFFFFFu, has);
+        if (!act) break;
+        if (has) {
+            const unsigned same = __match_any_sync(act, pairs[e]);
+            if (__ffs(same) - 1 == lane)
+                uf_union(parent, (int32_t)(pairs[e] >> 32), (int32_t)(uint32_t)pairs[e], status);
+        }
+    }
 }
 
 // 3. start[run] := start[root] for every run (a root's own entry is already
