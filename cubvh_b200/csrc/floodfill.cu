@@ -54,7 +54,9 @@ constexpr int kStepLimit = 1 << 24;   // bound on any union-find walk
 // faster still but the merge, with twice the tile boundaries, slower)
 constexpr int kTileThreads = 256;
 constexpr int kTileWarps = kTileThreads / 32;
-constexpr int kTileBlocksPerSM = 1024 / kTileThreads;
+// the tile kernel at 40 registers: six tiles in flight per SM (512^3 tile
+// kernel 74 -> 65 us against four; eight spill and are slower)
+constexpr int kTileBlocksPerSM = 6;
 constexpr int kTileWords = 4 * kTileThreads;   // bitmask words per tile chunk: four per thread
 constexpr int kSmemRuns = 12 * kTileThreads;   // a tile's runs unite (and are labelled) in shared memory up to this count
 
