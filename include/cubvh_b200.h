@@ -136,11 +136,14 @@ int cubvh_ray_trace(cubvh_bvh* bvh, const float* rays_o, const float* rays_d, in
  * handle is host memory (page-locked for asynchronous copies), the results
  * are those of cubvh_ray_trace / cubvh_signed_distance on the same inputs,
  * bit for bit.  The queries run in chunks of 2,097,152 whose upload, kernels
- * and download overlap on four internal streams; on return the work is
- * queued behind `stream` and `stream` waits for it: synchronize `stream`
- * before reading the outputs.  Calls on different streams overlap.  The
- * device staging memory (two chunks of inputs, outputs and workspace:
- * ~200 MB for rays) is kept per caller stream until the BVH is destroyed;
+ * and download overlap on six internal streams (copy-in, copy-out, one
+ * compute stream per staging set), with the priority of `stream`; on
+ * return the work is queued behind `stream` and `stream` waits for it:
+ * synchronize `stream` before reading the outputs.  Calls on different
+ * streams overlap, and the distance kernels of these calls yield SMs to
+ * higher-priority streams between short-lived blocks.  The device staging
+ * memory (four chunks of inputs, outputs and workspace: ~400 MB for rays)
+ * is kept per caller stream until the BVH is destroyed;
  * a call that needs more than its stream's staging synchronizes that
  * staging's earlier work and reallocates it.  A stream being captured into
  * a graph is rejected (status 1).
