@@ -28,12 +28,14 @@
 //               above; lock-free union-find on the global roots that always
 //               links the larger root under the smaller, so every root is
 //               its component's smallest run id, i.e. smallest voxel index
-//   3. resolve  every run's label = its root's first voxel
-//   4. label    one block per tile: the tile's run labels, start marks and
-//               run bases staged in shared memory, then the int32 labels (or
-//               the signed distances of udf_to_sdf) written with 16-byte
-//               streaming stores; rows of W % 32 != 0 voxels: a warp per 32
-//               words
+//   3. resolve  every run's label = its root's first voxel (for the tiles
+//               the label writer does not stage)
+//   4. label    one block per tile: the tile's run labels (each run's
+//               root's first voxel), start marks and run bases staged in
+//               shared memory, then the int32 labels (or the signed
+//               distances of udf_to_sdf) written with 16-byte streaming
+//               stores; rows of W % 32 != 0 voxels: a warp per 32 words
+//               over the resolved labels
 // Per bitmask word the tile kernel keeps its run starts (starts) and the
 // global id of the last run that starts before it (wbase: the run covering
 // bit x of word w is wbase[w] + popc(starts[w] & bits 0..x) - 1).
@@ -470,14 +472,17 @@ __global__ void k_ff_merge(const uint32_t* __restrict__ bits, const uint32_t* __
     }
 }
 
-// 3. start[run] := start[root] for every run (a root's own entry is already
-// its label, and only non-root entries are written, so concurrent readers of
-// roots' entries see final values).
+// 3. start[run] := start[root] for every run of the tiles with more than
+// `skip_upto` runs (a root's own entry is already its label, and only
+// non-root entries are written, so concurrent readers of roots' entries see
+// final values).  The tile label writer resolves the runs of the tiles it
+// stages in shared memory itself (skip_upto = kSmemRuns).
 __global__ void k_ff_resolve(const uint32_t* __restrict__ tcount, int64_t ntiles, int64_t cap,
                              const int32_t* __restrict__ parent, int32_t* __restrict__ start,
-                             int* __restrict__ status) {
+                             int* __restrict__ status, uint32_t skip_upto) {
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int32_t n = (int32_t)tcount[tile];
+        if ((uint32_t)n <= skip_upto) continue;
         const int32_t base = (int32_t)(tile * cap);
         for (int32_t i = threadIdx.x; i < n; i += blockDim.x) {
             const int32_t g = base + i;
@@ -501,8 +506,9 @@ template <bool SDF>
 __global__ void __launch_bounds__(kTileThreads)
 k_write_tile(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ starts,
              const uint32_t* __restrict__ wbase, const uint32_t* __restrict__ tcount,
-             const int32_t* __restrict__ runlab, int64_t wpr, int T, int64_t tiles_per_slice, int H, int64_t cap,
-             int4* __restrict__ labels, float4* __restrict__ sdf, int64_t rows_per_volume) {
+             const int32_t* __restrict__ runlab, const int32_t* __restrict__ parent, int* __restrict__ status,
+             int64_t wpr, int T, int64_t tiles_per_slice, int H, int64_t cap, int4* __restrict__ labels,
+             float4* __restrict__ sdf, int64_t rows_per_volume) {
     __shared__ int32_t slab[kSmemRuns];
     __shared__ __align__(16) uint32_t sf[kTileWords], ss[kTileWords], sb[kTileWords];
     const int64_t tile = blockIdx.x;
@@ -515,13 +521,16 @@ k_write_tile(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ sta
     const int64_t nwords = (int64_t)nrow * wpr;
     const uint32_t n = tcount[tile];
     const bool inl = n <= (uint32_t)kSmemRuns;
+    // staged tiles: each run's label is its root's first voxel (k_ff_resolve
+    // skipped these tiles); other tiles' labels were resolved in place
     if (inl)
-        for (uint32_t i = threadIdx.x; i < n; i += kTileThreads) slab[i] = runlab[tbase + i];
+        for (uint32_t i = threadIdx.x; i < n; i += kTileThreads)
+            slab[i] = runlab[uf_root(parent, (int32_t)(tbase + i), status)];
     const int32_t* lab = inl ? slab : runlab + tbase;
     int32_t empty = -1;
     if (SDF) {
         const int64_t rv = (r0 / rows_per_volume) * rows_per_volume;
-        if (bits[rv * wpr] & 1u) empty = runlab[wbase[rv * wpr]];
+        if (bits[rv * wpr] & 1u) empty = runlab[uf_root(parent, (int32_t)wbase[rv * wpr], status)];
     }
     for (int64_t c0 = 0; c0 < nwords; c0 += kTileWords) {
         const int nw = (int)min((int64_t)kTileWords, nwords - c0);
@@ -638,8 +647,11 @@ FFBufs carve(const FFPlan& p, void* ws) {
 }
 
 // 1-3: tiles, cross-tile unions, run labels (start[] := label of each run)
+// tile_writer: the labels are written by k_write_tile, which resolves the
+// runs of the tiles it stages itself.
 template <class Src>
-void label_runs(const FFPlan& p, int D, const Src& src, const FFBufs& b, unsigned sgrid, cudaStream_t stream) {
+void label_runs(const FFPlan& p, int D, const Src& src, const FFBufs& b, unsigned sgrid, bool tile_writer,
+                cudaStream_t stream) {
     k_zero<<<1, 1, 0, stream>>>(b.status); count_launch();
     k_ff_tile<Src><<<(unsigned)p.ntiles, kTileThreads, 0, stream>>>(
         src, p.W, p.wpr, p.wpr_shift, p.tile_rows, p.tiles_per_slice, p.H, p.cap, b.bits, b.starts, b.wbase,
@@ -647,7 +659,8 @@ void label_runs(const FFPlan& p, int D, const Src& src, const FFBufs& b, unsigne
     const unsigned mgrid = (unsigned)((2 * p.rows + 255) / 256);
     k_ff_merge<<<mgrid, 256, 0, stream>>>(b.bits, b.wbase, b.parent, b.status, p.rows, p.wpr, p.H, D,
                                           p.tile_rows); count_launch();
-    k_ff_resolve<<<sgrid, 256, 0, stream>>>(b.tcount, p.ntiles, p.cap, b.parent, b.start, b.status); count_launch();
+    k_ff_resolve<<<sgrid, 256, 0, stream>>>(b.tcount, p.ntiles, p.cap, b.parent, b.start, b.status,
+                                            tile_writer ? (uint32_t)kSmemRuns : 0u); count_launch();
 }
 
 unsigned stream_grid() {
@@ -669,11 +682,12 @@ cudaError_t launch_floodfill(const uint8_t* grid, int B, int H, int W, int D, in
     const FFBufs b = carve(p, ws);
     const unsigned sgrid = stream_grid();
     const GridSrc src{grid, W % 32 == 0 && (reinterpret_cast<uintptr_t>(grid) & 15) == 0};
-    label_runs(p, D, src, b, sgrid, stream);
-    if (W % 32 == 0 && (reinterpret_cast<uintptr_t>(labels) & 15) == 0) {
+    const bool tile_writer = W % 32 == 0 && (reinterpret_cast<uintptr_t>(labels) & 15) == 0;
+    label_runs(p, D, src, b, sgrid, tile_writer, stream);
+    if (tile_writer) {
         k_write_tile<false><<<(unsigned)p.ntiles, kTileThreads, 0, stream>>>(
-            b.bits, b.starts, b.wbase, b.tcount, b.start, p.wpr, p.tile_rows, p.tiles_per_slice, p.H, p.cap,
-            reinterpret_cast<int4*>(labels), nullptr, 1); count_launch();
+            b.bits, b.starts, b.wbase, b.tcount, b.start, b.parent, b.status, p.wpr, p.tile_rows, p.tiles_per_slice,
+            p.H, p.cap, reinterpret_cast<int4*>(labels), nullptr, 1); count_launch();
     } else {
         k_write_rows<false><<<sgrid, 256, 0, stream>>>(b.bits, b.starts, b.wbase, b.start, labels, nullptr, nullptr,
                                                        p.rows, p.wpr, W, 1, 0.f); count_launch();
@@ -689,11 +703,11 @@ cudaError_t launch_udf_to_sdf(const float* udf, int B, int H, int W, int D, floa
     const unsigned sgrid = stream_grid();
     const bool vec = W % 32 == 0 && ((reinterpret_cast<uintptr_t>(udf) | reinterpret_cast<uintptr_t>(sdf)) & 15) == 0;
     const UdfSrc src{udf, eps, vec, sdf};
-    label_runs(p, D, src, b, sgrid, stream);
+    label_runs(p, D, src, b, sgrid, vec, stream);
     if (vec) {
         k_write_tile<true><<<(unsigned)p.ntiles, kTileThreads, 0, stream>>>(
-            b.bits, b.starts, b.wbase, b.tcount, b.start, p.wpr, p.tile_rows, p.tiles_per_slice, p.H, p.cap, nullptr,
-            reinterpret_cast<float4*>(sdf), (int64_t)D * H);
+            b.bits, b.starts, b.wbase, b.tcount, b.start, b.parent, b.status, p.wpr, p.tile_rows, p.tiles_per_slice,
+            p.H, p.cap, nullptr, reinterpret_cast<float4*>(sdf), (int64_t)D * H);
         count_launch();
     } else {
         k_write_rows<true><<<sgrid, 256, 0, stream>>>(b.bits, b.starts, b.wbase, b.start, nullptr, udf, sdf, p.rows,
