@@ -36,9 +36,11 @@
 //               distances of udf_to_sdf) written with 16-byte streaming
 //               stores; rows of W % 32 != 0 voxels: a warp per 32 words
 //               over the resolved labels
-// Per bitmask word the tile kernel keeps its run starts (starts) and the
-// global id of the last run that starts before it (wbase: the run covering
-// bit x of word w is wbase[w] + popc(starts[w] & bits 0..x) - 1).
+// The tile kernel keeps the bitmask and every row's first run id (rowid);
+// for the row-wise label writer (rows of W % 32 != 0 voxels) also per word
+// its run starts (starts) and the id of the last run that starts before it
+// (wbase: the run covering bit x of word w is wbase[w] + popc(starts[w] &
+// bits 0..x) - 1).  The tile label writer recomputes both from the bitmask.
 #include <algorithm>
 #include <climits>
 #include <cstdint>
@@ -69,7 +71,7 @@ struct FFPlan {
     int tile_rows;                     // T: rows per tile; a tile never spans two z-slices
     int64_t tiles_per_slice, ntiles;
     int64_t cap;                       // run ids per tile: T * ceil(W / 2)
-    size_t off_bits, off_starts, off_wbase, off_tcount, off_start, off_parent, off_status, total;
+    size_t off_bits, off_starts, off_wbase, off_rowid, off_tcount, off_start, off_parent, off_status, total;
 };
 
 inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -101,6 +103,7 @@ FFPlan make_plan(int B, int H, int W, int D) {
     p.off_bits = o; o = align256(o + sizeof(uint32_t) * p.words);
     p.off_starts = o; o = align256(o + sizeof(uint32_t) * p.words);
     p.off_wbase = o; o = align256(o + sizeof(uint32_t) * p.words);
+    p.off_rowid = o; o = align256(o + sizeof(uint32_t) * p.rows);
     p.off_tcount = o; o = align256(o + sizeof(uint32_t) * p.ntiles);
     p.off_start = o; o = align256(o + sizeof(int32_t) * p.ntiles * p.cap);
     p.off_parent = o; o = align256(o + sizeof(int32_t) * p.ntiles * p.cap);
@@ -269,7 +272,8 @@ __device__ __forceinline__ uint32_t block_exclusive(uint32_t v, uint32_t* wsum, 
 template <class Src>
 __global__ void __launch_bounds__(kTileThreads, kTileBlocksPerSM)
 k_ff_tile(Src src, int W, int64_t wpr, int shift, int T, int64_t tiles_per_slice, int H, int64_t cap,
-          uint32_t* __restrict__ bits, uint32_t* __restrict__ starts, uint32_t* __restrict__ wbase,
+          bool store_words, uint32_t* __restrict__ bits, uint32_t* __restrict__ starts, uint32_t* __restrict__ wbase,
+          uint32_t* __restrict__ rowid,
           uint32_t* __restrict__ tcount, int32_t* __restrict__ start, int32_t* __restrict__ parent,
           int* __restrict__ status) {
     __shared__ __align__(16) uint32_t sbits[kTileWords];
@@ -330,11 +334,14 @@ k_ff_tile(Src src, int W, int64_t wpr, int shift, int T, int64_t tiles_per_slice
             const int w = t4 + j;
             if (w < nw) {
                 sw[w] = run;
-                starts[g0 + w] = st[j];
-                wbase[g0 + w] = (uint32_t)(tbase + run);
+                if (store_words) {
+                    starts[g0 + w] = st[j];
+                    wbase[g0 + w] = (uint32_t)(tbase + run);
+                }
+                int64_t row, wi;
+                word_pos(g0 + w, wpr, shift, row, wi);
+                if (wi == 0) rowid[row] = (uint32_t)(tbase + run);   // the row's first run
                 if (st[j]) {
-                    int64_t row, wi;
-                    word_pos(g0 + w, wpr, shift, row, wi);
                     const int64_t v0 = row * W + wi * 32;   // < 2^31 voxels (host check)
                     uint32_t sj = st[j];
                     int32_t id = (int32_t)run;
@@ -390,7 +397,7 @@ k_ff_tile(Src src, int W, int64_t wpr, int shift, int T, int64_t tiles_per_slice
 
 // 2. Unions across tiles: row r with its z - 1 row (r - H), and the first row
 // of a tile with the row above it (y - 1) when that row is in another tile.
-// A row's first run is the run base of its first word.  At every maximal
+// A row's first run id is rowid[row].  At every maximal
 // common free segment of the two rows and every run start inside one, the
 // two runs covering that voxel are united, through their current parents
 // (the tile kernel left every run pointing at its tile root): consecutive
@@ -399,7 +406,7 @@ k_ff_tile(Src src, int W, int64_t wpr, int shift, int T, int64_t tiles_per_slice
 // matched across the warp, and one lane per pair unites it (further pairs
 // are united directly).
 constexpr int kMergePairs = 4;
-__global__ void k_ff_merge(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ wbase,
+__global__ void k_ff_merge(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ rowid,
                            int32_t* __restrict__ parent, int* __restrict__ status, int64_t rows, int64_t wpr, int H,
                            int D, int T) {
     const int lane = threadIdx.x & 31;
@@ -418,7 +425,7 @@ __global__ void k_ff_merge(const uint32_t* __restrict__ bits, const uint32_t* __
         const int64_t q = r - (dir == 0 ? 1 : H);
         const uint32_t* br = bits + r * wpr;
         const uint32_t* bq = bits + q * wpr;
-        int32_t cr = (int32_t)wbase[r * wpr], cq = (int32_t)wbase[q * wpr];
+        int32_t cr = (int32_t)rowid[r], cq = (int32_t)rowid[q];
         uint32_t pr = 0, pq = 0, pm = 0;
         // words four at a time (16-byte loads when the rows are 16-byte aligned)
         const bool v4 = (wpr & 3) == 0;
@@ -493,10 +500,11 @@ __global__ void k_ff_resolve(const uint32_t* __restrict__ tcount, int64_t ntiles
 }
 
 // 4 (W % 32 == 0, 16-byte aligned output).  One block per tile: the tile's
-// run labels (up to kSmemRuns) and its words' free bits, run starts and run
-// bases (tile-relative) are staged in shared memory with coalesced loads,
-// then each thread writes groups of 4 voxels (bits 4k .. 4k + 3 of a word)
-// with 16-byte streaming stores, consecutive threads consecutive groups.
+// run labels (up to kSmemRuns) and its words' free bits are staged in shared
+// memory with coalesced loads, the words' run starts and run bases
+// (tile-relative) recomputed from the bits with one block-wide scan, then
+// each thread writes groups of 4 voxels (bits 4k .. 4k + 3 of a word) with
+// 16-byte streaming stores, consecutive threads consecutive groups.
 // SDF: the signed distance s = udf - eps instead of the label, negated where
 // the voxel's label (-1 when occupied) differs from the label of its
 // volume's first voxel (b, 0, 0, 0) and s > 0; the tile kernel has already
@@ -504,13 +512,14 @@ __global__ void k_ff_resolve(const uint32_t* __restrict__ tcount, int64_t ntiles
 // are read and rewritten.
 template <bool SDF>
 __global__ void __launch_bounds__(kTileThreads)
-k_write_tile(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ starts,
-             const uint32_t* __restrict__ wbase, const uint32_t* __restrict__ tcount,
-             const int32_t* __restrict__ runlab, const int32_t* __restrict__ parent, int* __restrict__ status,
-             int64_t wpr, int T, int64_t tiles_per_slice, int H, int64_t cap, int4* __restrict__ labels,
-             float4* __restrict__ sdf, int64_t rows_per_volume) {
+k_write_tile(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ rowid,
+             const uint32_t* __restrict__ tcount, const int32_t* __restrict__ runlab,
+             const int32_t* __restrict__ parent, int* __restrict__ status, int64_t wpr, int shift, int T,
+             int64_t tiles_per_slice, int H, int64_t cap, int4* __restrict__ labels, float4* __restrict__ sdf,
+             int64_t rows_per_volume) {
     __shared__ int32_t slab[kSmemRuns];
     __shared__ __align__(16) uint32_t sf[kTileWords], ss[kTileWords], sb[kTileWords];
+    __shared__ uint32_t wsum[32];
     const int64_t tile = blockIdx.x;
     const int64_t slice = tile / tiles_per_slice;
     const int y0 = (int)(tile - slice * tiles_per_slice) * T;
@@ -530,16 +539,39 @@ k_write_tile(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ sta
     int32_t empty = -1;
     if (SDF) {
         const int64_t rv = (r0 / rows_per_volume) * rows_per_volume;
-        if (bits[rv * wpr] & 1u) empty = runlab[uf_root(parent, (int32_t)wbase[rv * wpr], status)];
+        if (bits[rv * wpr] & 1u) empty = runlab[uf_root(parent, (int32_t)rowid[rv], status)];
     }
+    const int t4 = 4 * (int)threadIdx.x;
+    uint32_t carry = 0;   // runs of the tile in earlier chunks
     for (int64_t c0 = 0; c0 < nwords; c0 += kTileWords) {
         const int nw = (int)min((int64_t)kTileWords, nwords - c0);
         const int64_t g0 = w0 + c0;
-        for (int k = threadIdx.x; k < nw; k += kTileThreads) {
-            sf[k] = bits[g0 + k];
-            ss[k] = starts[g0 + k];
-            sb[k] = (uint32_t)(wbase[g0 + k] - tbase);
+        __syncthreads();   // the previous chunk's words have been read
+        for (int k = threadIdx.x; k < nw; k += kTileThreads) sf[k] = bits[g0 + k];
+        __syncthreads();
+        // run starts of the thread's words and the tile-relative index of the
+        // last run before each word (block-wide scan of the start counts)
+        uint32_t stw[4], tot = 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int w = t4 + j;
+            stw[j] = 0u;
+            if (w < nw) {
+                int64_t k, wi;
+                word_pos(c0 + w, wpr, shift, k, wi);
+                const uint32_t prev = wi == 0 ? 0u : (w > 0 ? sf[w - 1] : bits[g0 - 1]);
+                stw[j] = starts_of(sf[w], prev);
+            }
+            tot += __popc(stw[j]);
         }
+        uint32_t total;
+        uint32_t run = carry + block_exclusive(tot, wsum, &total);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (t4 + j < nw) { ss[t4 + j] = stw[j]; sb[t4 + j] = run; }
+            run += __popc(stw[j]);
+        }
+        carry += total;
         __syncthreads();
         for (int g = threadIdx.x; g < 8 * nw; g += kTileThreads) {
             const size_t i4 = (size_t)g0 * 8 + g;     // 16-byte group of the whole grid
@@ -634,14 +666,15 @@ __global__ void k_write_rows(const uint32_t* __restrict__ bits, const uint32_t* 
 __global__ void k_zero(int* p) { *p = 0; }
 
 struct FFBufs {
-    uint32_t *bits, *starts, *wbase, *tcount;
+    uint32_t *bits, *starts, *wbase, *rowid, *tcount;
     int32_t *start, *parent;
     int* status;
 };
 FFBufs carve(const FFPlan& p, void* ws) {
     char* base = static_cast<char*>(ws);
     return FFBufs{reinterpret_cast<uint32_t*>(base + p.off_bits), reinterpret_cast<uint32_t*>(base + p.off_starts),
-                  reinterpret_cast<uint32_t*>(base + p.off_wbase), reinterpret_cast<uint32_t*>(base + p.off_tcount),
+                  reinterpret_cast<uint32_t*>(base + p.off_wbase), reinterpret_cast<uint32_t*>(base + p.off_rowid),
+                  reinterpret_cast<uint32_t*>(base + p.off_tcount),
                   reinterpret_cast<int32_t*>(base + p.off_start), reinterpret_cast<int32_t*>(base + p.off_parent),
                   reinterpret_cast<int*>(base + p.off_status)};
 }
@@ -654,10 +687,10 @@ void label_runs(const FFPlan& p, int D, const Src& src, const FFBufs& b, unsigne
                 cudaStream_t stream) {
     k_zero<<<1, 1, 0, stream>>>(b.status); count_launch();
     k_ff_tile<Src><<<(unsigned)p.ntiles, kTileThreads, 0, stream>>>(
-        src, p.W, p.wpr, p.wpr_shift, p.tile_rows, p.tiles_per_slice, p.H, p.cap, b.bits, b.starts, b.wbase,
-        b.tcount, b.start, b.parent, b.status); count_launch();
+        src, p.W, p.wpr, p.wpr_shift, p.tile_rows, p.tiles_per_slice, p.H, p.cap, !tile_writer, b.bits, b.starts,
+        b.wbase, b.rowid, b.tcount, b.start, b.parent, b.status); count_launch();
     const unsigned mgrid = (unsigned)((2 * p.rows + 255) / 256);
-    k_ff_merge<<<mgrid, 256, 0, stream>>>(b.bits, b.wbase, b.parent, b.status, p.rows, p.wpr, p.H, D,
+    k_ff_merge<<<mgrid, 256, 0, stream>>>(b.bits, b.rowid, b.parent, b.status, p.rows, p.wpr, p.H, D,
                                           p.tile_rows); count_launch();
     k_ff_resolve<<<sgrid, 256, 0, stream>>>(b.tcount, p.ntiles, p.cap, b.parent, b.start, b.status,
                                             tile_writer ? (uint32_t)kSmemRuns : 0u); count_launch();
@@ -686,8 +719,8 @@ cudaError_t launch_floodfill(const uint8_t* grid, int B, int H, int W, int D, in
     label_runs(p, D, src, b, sgrid, tile_writer, stream);
     if (tile_writer) {
         k_write_tile<false><<<(unsigned)p.ntiles, kTileThreads, 0, stream>>>(
-            b.bits, b.starts, b.wbase, b.tcount, b.start, b.parent, b.status, p.wpr, p.tile_rows, p.tiles_per_slice,
-            p.H, p.cap, reinterpret_cast<int4*>(labels), nullptr, 1); count_launch();
+            b.bits, b.rowid, b.tcount, b.start, b.parent, b.status, p.wpr, p.wpr_shift, p.tile_rows,
+            p.tiles_per_slice, p.H, p.cap, reinterpret_cast<int4*>(labels), nullptr, 1); count_launch();
     } else {
         k_write_rows<false><<<sgrid, 256, 0, stream>>>(b.bits, b.starts, b.wbase, b.start, labels, nullptr, nullptr,
                                                        p.rows, p.wpr, W, 1, 0.f); count_launch();
@@ -706,8 +739,8 @@ cudaError_t launch_udf_to_sdf(const float* udf, int B, int H, int W, int D, floa
     label_runs(p, D, src, b, sgrid, vec, stream);
     if (vec) {
         k_write_tile<true><<<(unsigned)p.ntiles, kTileThreads, 0, stream>>>(
-            b.bits, b.starts, b.wbase, b.tcount, b.start, b.parent, b.status, p.wpr, p.tile_rows, p.tiles_per_slice,
-            p.H, p.cap, nullptr, reinterpret_cast<float4*>(sdf), (int64_t)D * H);
+            b.bits, b.rowid, b.tcount, b.start, b.parent, b.status, p.wpr, p.wpr_shift, p.tile_rows,
+            p.tiles_per_slice, p.H, p.cap, nullptr, reinterpret_cast<float4*>(sdf), (int64_t)D * H);
         count_launch();
     } else {
         k_write_rows<true><<<sgrid, 256, 0, stream>>>(b.bits, b.starts, b.wbase, b.start, nullptr, udf, sdf, p.rows,
