@@ -530,17 +530,25 @@ k_write_tile(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ row
     const int64_t nwords = (int64_t)nrow * wpr;
     const uint32_t n = tcount[tile];
     const bool inl = n <= (uint32_t)kSmemRuns;
-    // staged tiles: each run's label is its root's first voxel (k_ff_resolve
-    // skipped these tiles); other tiles' labels were resolved in place
-    if (inl)
-        for (uint32_t i = threadIdx.x; i < n; i += kTileThreads)
-            slab[i] = runlab[uf_root(parent, (int32_t)(tbase + i), status)];
-    const int32_t* lab = inl ? slab : runlab + tbase;
     int32_t empty = -1;
     if (SDF) {
         const int64_t rv = (r0 / rows_per_volume) * rows_per_volume;
         if (bits[rv * wpr] & 1u) empty = runlab[uf_root(parent, (int32_t)rowid[rv], status)];
     }
+    // staged tiles: each run's label is its root's first voxel (k_ff_resolve
+    // skipped these tiles); other tiles' labels were resolved in place
+    bool other = !inl;   // SDF: the tile may hold a run whose label differs from empty
+    if (inl)
+        for (uint32_t i = threadIdx.x; i < n; i += kTileThreads) {
+            const int32_t l = runlab[uf_root(parent, (int32_t)(tbase + i), status)];
+            slab[i] = l;
+            other |= l != empty;
+        }
+    // SDF: sdf already holds udf - eps, and only free voxels of runs labelled
+    // differently from the volume's first voxel can flip; a tile with none
+    // is done
+    if (SDF && !__syncthreads_or(other)) return;
+    const int32_t* lab = inl ? slab : runlab + tbase;
     const int t4 = 4 * (int)threadIdx.x;
     uint32_t carry = 0;   // runs of the tile in earlier chunks
     for (int64_t c0 = 0; c0 < nwords; c0 += kTileWords) {
