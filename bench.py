@@ -796,7 +796,7 @@ def run_ours(args):
 
     # floodfill from a pageable host grid to host labels through the public
     # API, the same footing as the reference arm's CUDA floodfill timing
-    ff_host_ms = None
+    ff_host_ms = ff_cpu = None
     if any(op == "floodfill" for op, _ in wl["ops"]):
         res = next(a[0] for op, a in wl["ops"] if op == "floodfill")
         g_host = (occ_src.view(res, res, res) < 2.0 / res).cpu()
@@ -809,6 +809,15 @@ def run_ours(args):
             cubvh.floodfill(g_host).cpu()
             tt.append(time.perf_counter() - w0)
         ff_host_ms = 1e3 * statistics.median(tt)
+        # CPU-baseline leg: the oracle's single-thread floodfill (union-find
+        # giving min-index labels) on the same grid, timed beside ours, and
+        # the full-grid labels compared with it (outside every timed region)
+        from oracle import oracle as O
+        g_np = g_host.numpy()
+        w0 = time.perf_counter()
+        cpu_lab = O.floodfill(g_np)
+        ff_cpu = {"ms": 1e3 * (time.perf_counter() - w0), "threads": 1,
+                  "labels_equal_ours": bool(np.array_equal(cpu_lab, cubvh.floodfill(g_host).cpu().numpy()))}
 
     line = None
     if rank == 0:
@@ -840,6 +849,7 @@ def run_ours(args):
                     d["ref_traversal_tris_per_query"] = counts[o][1]
             if o == "floodfill" and ff_host_ms is not None:
                 d["e2e_host_pageable_ms"] = ff_host_ms
+                d["cpu_oracle_single_thread"] = ff_cpu
             if o in GRID_OPS:  # 1 B in + 4 B out (floodfill), 4 B in + 4 B out (udf_to_sdf) per voxel
                 gbs = (5.0 if o == "floodfill" else 8.0) * args.grid ** 3 / (per_op_ms[i] / 1e3) / 1e9
                 d["hbm_gbs"] = gbs
