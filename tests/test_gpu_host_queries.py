@@ -123,3 +123,44 @@ def test_host_queries_non_blocking_two_streams(dev):
             assert torch.equal(a, b.cpu())
     with pytest.raises(ValueError):
         bvh.ray_trace(ro.double(), rd, out=out_r, non_blocking=True)
+
+
+@pytest.mark.gpu
+def test_host_queries_priority_streams(dev):
+    """A compute-heavy call on a low-priority stream and a copy-heavy one on a
+    high-priority stream (the C1 end-to-end arrangement: the distance kernels
+    of the first yield SMs to the second's chunk kernels) give the blocking
+    results, several chunks each."""
+    v, f = W.displaced_icosphere(5, 2)
+    bvh = cubvh.cuBVH(v, f)
+    ro, rd = (torch.from_numpy(x).pin_memory() for x in W.camera_rays(2, 1448, 50.0, 2.5, 3))  # ~4.2M rays
+    pts = torch.from_numpy(W.uniform_points(5 * CHUNK // 2, 8)).pin_memory()
+    n, m = ro.shape[0], pts.shape[0]
+    want_r = bvh.ray_trace(ro.to(dev), rd.to(dev))
+    want_s = bvh.signed_distance(pts.to(dev), mode="watertight")
+    want_u = bvh.unsigned_distance(pts.to(dev), return_uvw=True)
+    out_r = (torch.empty((n, 3), pin_memory=True), torch.empty(n, dtype=torch.int64, pin_memory=True),
+             torch.empty(n, pin_memory=True))
+    out_s = (torch.empty(m, pin_memory=True), torch.empty(m, dtype=torch.int64, pin_memory=True))
+    out_u = (torch.empty(m, pin_memory=True), torch.empty(m, dtype=torch.int64, pin_memory=True),
+             torch.empty((m, 3), pin_memory=True))
+    lo = torch.cuda.Stream(dev, priority=0)
+    lo2 = torch.cuda.Stream(dev, priority=0)
+    hi = torch.cuda.Stream(dev, priority=-1)
+    for _ in range(2):
+        for t in out_r + out_s + out_u:
+            t.zero_()
+        with torch.cuda.stream(lo):
+            bvh.signed_distance(pts, mode="watertight", out=out_s, non_blocking=True)
+        with torch.cuda.stream(lo2):
+            bvh.unsigned_distance(pts, return_uvw=True, out=out_u, non_blocking=True)
+        with torch.cuda.stream(hi):
+            bvh.ray_trace(ro, rd, out=out_r, non_blocking=True)
+        for s in (lo, lo2, hi):
+            s.synchronize()
+        for a, b in zip(out_r, want_r):
+            assert torch.equal(a, b.cpu())
+        for a, b in zip(out_s, want_s):
+            assert torch.equal(a, b.cpu())
+        for a, b in zip(out_u, want_u):
+            assert torch.equal(a, b.cpu())
