@@ -401,3 +401,25 @@ def test_state_dict_sizes_for_many_face_counts():
         leaf_ranges = sorted((-l - 1, -r - 1) for l, r in zip(recs["left"][~inner], recs["right"][~inner]))
         assert leaf_ranges[0][0] == 0 and leaf_ranges[-1][1] == nf
         assert all(a[1] == b[0] for a, b in zip(leaf_ranges, leaf_ranges[1:]))
+
+
+def test_bench_reference_arm_contract():
+    """`bench.py --impl reference` (the reference's host traversals timed on
+    the CPU) prints one JSON line with the contract's keys, on a tiny
+    rays_displaced workload."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--res", "32",
+                          "--sdf-points", "2048", "--steps", "1", "--warmup", "3"],
+                         cwd=root, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["value"] > 0 and d["unit"] == "queries/s"
+    assert d["higher_is_better"] is True and d["n_gpus"] == 1 and d["steps"] == 1
+    assert d["cpu_baseline"]["kind"] in ("reference", "port") and d["cpu_baseline"]["value"] == d["value"]
+    assert d["e2e"] == {"value": d["value"], "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    assert d["config"]["workload"] == "rays_displaced"
