@@ -305,3 +305,43 @@ def test_queries_in_cuda_graph(dev):
         d, fid, _ = bvh.signed_distance(pts, mode="watertight")
         torch.cuda.synchronize()
         assert torch.equal(d, want[0]) and torch.equal(fid, want[1])
+
+
+def test_non_finite_queries_leave_the_others_unchanged(dev):
+    """NaN and infinite query points / rays in a batch: the calls succeed, and
+    every finite query's result equals its result in the same batch with the
+    bad entries replaced by finite ones (a packet's shared walk never lets one
+    lane's values change another's; raystab stab rays follow the query index,
+    which both batches share)."""
+    v, f = W.displaced_icosphere(4, 1)
+    bvh = cubvh.cuBVH(v, f)
+    rng = np.random.default_rng(21)
+    n = 4096
+    good = rng.uniform(-1.2, 1.2, (n, 3)).astype(np.float32)
+    bad_idx = rng.choice(n, 64, replace=False)
+    bad = good.copy()
+    vals = np.array([np.nan, np.inf, -np.inf, 1e30], np.float32)
+    bad[bad_idx, rng.integers(0, 3, 64)] = vals[rng.integers(0, 4, 64)]
+    keep = np.ones(n, bool)
+    keep[bad_idx] = False
+    P = lambda a: torch.from_numpy(a).to(dev)
+    for mode in (None, "watertight", "raystab"):
+        if mode is None:
+            a, b = bvh.unsigned_distance(P(bad), return_uvw=True), bvh.unsigned_distance(P(good), return_uvw=True)
+        else:
+            a, b = bvh.signed_distance(P(bad), mode=mode), bvh.signed_distance(P(good), mode=mode)
+        for x, y in zip(a, b):
+            if x is None:
+                continue
+            assert torch.equal(x[torch.from_numpy(keep).to(dev)], y[torch.from_numpy(keep).to(dev)]), mode
+    ro, rd = W.camera_rays(1, 64, 50.0, 2.5, 4)
+    rbad = rd.copy()
+    ridx = rng.choice(len(rd), 64, replace=False)
+    rbad[ridx, rng.integers(0, 3, 64)] = vals[rng.integers(0, 4, 64)]
+    rkeep = np.ones(len(rd), bool)
+    rkeep[ridx] = False
+    a = bvh.ray_trace(P(ro), P(rbad))
+    b = bvh.ray_trace(P(ro), P(rd))
+    for x, y in zip(a, b):
+        m = torch.from_numpy(rkeep).to(dev)
+        assert torch.equal(x[m], y[m])
