@@ -284,18 +284,18 @@ void set_frame(CNode& nd, const Box& b) {
     nd.ez = (int8_t)pick_exponent(b.lo[2], b.hi[2]);
 }
 
-// Error scales used by the single-precision filters of the query kernels.
+// Error scales used by the single-precision distance filter of the query
+// kernels: K and K * squared longest edge.
 void set_error_scales(CTri& t) {
     const float v[3][3] = {{t.ax, t.ay, t.az}, {t.bx, t.by, t.bz}, {t.cx, t.cy, t.cz}};
-    float e2 = 0.f, einf = 0.f;
+    float e2 = 0.f;
     for (int u = 0; u < 3; ++u) {
         const float* q0 = v[u]; const float* q1 = v[(u + 1) % 3];
         const float dx = q1[0] - q0[0], dy = q1[1] - q0[1], dz = q1[2] - q0[2];
         e2 = std::max(e2, dx * dx + dy * dy + dz * dz);
     }
-    for (int u = 1; u < 3; ++u)
-        for (int k = 0; k < 3; ++k) einf = std::max(einf, std::fabs(v[u][k] - v[0][k]));
-    t.e2 = e2; t.einf = einf;
+    t.k = tri_error_factor(v[0], v[1], v[2]);
+    t.ke2 = t.k * e2;
 }
 
 Box tri_box(const CTri& t) {

@@ -41,15 +41,15 @@ __device__ __forceinline__ d3 dcross(d3 a, d3 b) {
 }
 __device__ __forceinline__ d3 to_d3(float3 v) { return d3{(double)v.x, (double)v.y, (double)v.z}; }
 
-struct TriV { float3 a, b, c; float e2, einf; int id; };
+struct TriV { float3 a, b, c; float ke2, k; int id; };
 
 __device__ __forceinline__ TriV load_tri(const CTri* __restrict__ tris, int slot) {
     const float4* p = reinterpret_cast<const float4*>(tris + slot);
     const float4 w0 = __ldg(p), w1 = __ldg(p + 1), w2 = __ldg(p + 2);
     TriV t;
     t.a = make_float3(w0.x, w0.y, w0.z); t.id = __float_as_int(w0.w);
-    t.b = make_float3(w1.x, w1.y, w1.z); t.e2 = w1.w;
-    t.c = make_float3(w2.x, w2.y, w2.z); t.einf = w2.w;
+    t.b = make_float3(w1.x, w1.y, w1.z); t.ke2 = w1.w;
+    t.c = make_float3(w2.x, w2.y, w2.z); t.k = w2.w;
     return t;
 }
 
@@ -152,8 +152,12 @@ __device__ __forceinline__ float sat(float x) { return fminf(fmaxf(x, 0.0f), 1.0
 
 // Single-precision squared point-triangle distance (edge / face selection of
 // Quilez's udTriangle) and an absolute bound on its rounding error:
-// 8e-6 * (|p-a|^2 + longest edge^2) covers ~130 single roundings of the
-// local scale, several times what the expression performs.
+// 8e-6 * K * (|p-a|^2 + longest edge^2).  With K = 1 it covers ~130 single
+// roundings of the local scale, several times what the expression performs
+// when the triangle's normal at a is well conditioned; K > 1 widens it for
+// the others, degenerate triangles included (layout.h, tri_error_factor).
+// The face value's denominator |n|^2 is floored at 1e-36, so a zero normal
+// gives a number (at most |p-a|^2) rather than 0 / 0.
 __device__ __forceinline__ float tri_d2_f(float3 p, const TriV& t, float* err) {
     const float3 v21 = f3sub(t.b, t.a), p1 = f3sub(p, t.a);
     const float3 v32 = f3sub(t.c, t.b), p2 = f3sub(p, t.b);
@@ -172,9 +176,9 @@ __device__ __forceinline__ float tri_d2_f(float3 p, const TriV& t, float* err) {
         d2 = fminf(fminf(f3dot(q1, q1), f3dot(q2, q2)), f3dot(q3, q3));
     } else {
         const float nd = f3dot(nor, p1);
-        d2 = __fdividef(nd * nd, f3dot(nor, nor));
+        d2 = __fdividef(nd * nd, fmaxf(f3dot(nor, nor), 1e-36f));
     }
-    *err = 8e-6f * (f3dot(p1, p1) + t.e2);
+    *err = 8e-6f * fmaf(t.k, f3dot(p1, p1), t.ke2);
     return d2;
 }
 
@@ -193,7 +197,7 @@ __device__ __forceinline__ int ray_tri_f(float3 o, float3 d, float dinf, const T
     const float3 qv = f3cross(s, e1);
     const float vn = f3dot(d, qv);
     const float tn = f3dot(e2, qv);
-    const float E = t.einf, S = f3inf(s);
+    const float E = fmaxf(f3inf(e1), f3inf(e2)), S = f3inf(s);
     const float c = 8e-6f;
     const float Bdet = c * dinf * E * E;
     const float Bsd = c * S * dinf * E;

@@ -109,20 +109,19 @@ __global__ void k_prep(const float* __restrict__ v, const int64_t* __restrict__ 
         atomicMin(&cbounds[6 * m + c], f2o(mc));
         atomicMax(&cbounds[6 * m + 3 + c], f2o(mc));
     }
-    // error scales of the FP32 filters, with the host builder's operations
-    float e2 = 0.f, einf = 0.f;
+    // error scales of the FP32 distance filter, with the host builder's operations
+    float e2 = 0.f;
     for (int u = 0; u < 3; ++u) {
         const float* q0 = p[u];
         const float* q1 = p[(u + 1) % 3];
         const float dx = __fsub_rn(q1[0], q0[0]), dy = __fsub_rn(q1[1], q0[1]), dz = __fsub_rn(q1[2], q0[2]);
         e2 = fmaxf(e2, __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)));
     }
-    for (int u = 1; u < 3; ++u)
-        for (int c = 0; c < 3; ++c) einf = fmaxf(einf, fabsf(__fsub_rn(p[u][c], p[0][c])));
     CTri t;
     t.ax = p[0][0]; t.ay = p[0][1]; t.az = p[0][2]; t.id = (int32_t)(i - foff[m]);
-    t.bx = p[1][0]; t.by = p[1][1]; t.bz = p[1][2]; t.e2 = e2;
-    t.cx = p[2][0]; t.cy = p[2][1]; t.cz = p[2][2]; t.einf = einf;
+    t.k = tri_error_factor(p[0], p[1], p[2]);
+    t.bx = p[1][0]; t.by = p[1][1]; t.bz = p[1][2]; t.ke2 = __fmul_rn(t.k, e2);
+    t.cx = p[2][0]; t.cy = p[2][1]; t.cz = p[2][2];
     rec[i] = t;
 }
 

@@ -43,15 +43,15 @@ __global__ void k_refit_soup(int64_t nt, CTri* __restrict__ tris, const int32_t*
     t.ax = a.x; t.ay = a.y; t.az = a.z;
     t.bx = b.x; t.by = b.y; t.bz = b.z;
     t.cx = c.x; t.cy = c.y; t.cz = c.z;
-    // error scales as on the host: squared longest edge, max |b-a|, |c-a|
+    // error scales as on the host: K, K * squared longest edge
     const float3 e[3] = {f3sub(b, a), f3sub(c, b), f3sub(a, c)};
     float e2 = 0.f;
 #pragma unroll
     for (int u = 0; u < 3; ++u) e2 = fmaxf(e2, __fadd_rn(__fadd_rn(__fmul_rn(e[u].x, e[u].x), __fmul_rn(e[u].y, e[u].y)),
                                                          __fmul_rn(e[u].z, e[u].z)));
-    const float3 ca = f3sub(c, a);
-    t.e2 = e2;
-    t.einf = fmaxf(f3inf(e[0]), f3inf(ca));
+    const float va[3] = {a.x, a.y, a.z}, vb[3] = {b.x, b.y, b.z}, vc[3] = {c.x, c.y, c.z};
+    t.k = tri_error_factor(va, vb, vc);
+    t.ke2 = __fmul_rn(t.k, e2);
     tris[s] = t;
 }
 

@@ -141,8 +141,8 @@ __device__ __forceinline__ TriV warp_tri(const float* s, int i) {
     const float4 w0 = p[0], w1 = p[1], w2 = p[2];
     TriV t;
     t.a = make_float3(w0.x, w0.y, w0.z); t.id = __float_as_int(w0.w);
-    t.b = make_float3(w1.x, w1.y, w1.z); t.e2 = w1.w;
-    t.c = make_float3(w2.x, w2.y, w2.z); t.einf = w2.w;
+    t.b = make_float3(w1.x, w1.y, w1.z); t.ke2 = w1.w;
+    t.c = make_float3(w2.x, w2.y, w2.z); t.k = w2.w;
     return t;
 }
 __device__ __forceinline__ void warp_box(const float* s, int j, float3& lo, float3& hi) {

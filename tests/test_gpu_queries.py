@@ -345,3 +345,39 @@ def test_non_finite_queries_leave_the_others_unchanged(dev):
     for x, y in zip(a, b):
         m = torch.from_numpy(rkeep).to(dev)
         assert torch.equal(x[m], y[m])
+
+
+def test_degenerate_triangles(oracle, dev, stab_dirs):
+    """Zero-area faces (a segment, a point, a sphere edge, the segment again
+    with its vertices reordered) added to a closed sphere, outside it and near
+    it: every mode still equals the oracle bit for bit, including the queries
+    whose closest face is a degenerate one, and no ray reports a hit on one."""
+    v, f = W.icosphere(3, 0.8)
+    nv, nf = len(v), len(f)
+    extra = np.array([[0.2, 0.1, 0.85], [0.3, 0.1, 0.85], [0.4, 0.1, 0.85],
+                      [-0.3, -0.2, 0.9]], np.float32)
+    v = np.concatenate([v, extra]).astype(np.float32)
+    f = np.concatenate([f, [[nv, nv + 1, nv + 2], [nv + 3, nv + 3, nv + 3],
+                            [0, 0, 1], [nv, nv + 2, nv + 1]]]).astype(np.int64)
+    rng = np.random.default_rng(31)
+    pts = np.concatenate([rng.uniform(-1, 1, (3000, 3)),
+                          np.repeat(extra, 100, 0) + rng.normal(0, 0.03, (400, 3)),
+                          extra]).astype(np.float32)
+    bvh = cubvh.cuBVH(v, f)
+    P = torch.from_numpy(pts).to(dev)
+    out = bvh.unsigned_distance(P, return_uvw=True)
+    check_udf(oracle, v, f, pts, out)
+    assert (_np(out[1]) >= nf).sum() > 100
+    got = bvh.signed_distance(P, return_uvw=True, mode="watertight")
+    sd, fid, _ = oracle.sdf_watertight64(v, f, pts)
+    check_sdf(got, sd, fid, "watertight")
+    got = bvh.signed_distance(P, mode="raystab")
+    sd, fid, _ = oracle.sdf_raystab64(v, f, pts, dirs=stab_dirs(len(pts)))
+    check_sdf(got, sd, fid, "raystab")
+    ro = rng.normal(0, 2, (2000, 3)).astype(np.float32)
+    tgt = np.concatenate([np.repeat(extra, 400, 0), rng.uniform(-0.5, 0.5, (400, 3))])
+    rd = tgt + rng.normal(0, 0.01, tgt.shape) - ro
+    rd = (rd / np.linalg.norm(rd, axis=1, keepdims=True)).astype(np.float32)
+    out = bvh.ray_trace(torch.from_numpy(ro).to(dev), torch.from_numpy(rd).to(dev))
+    check_rays(oracle, v, f, ro, rd, out)
+    assert not (_np(out[1]) >= nf).any()

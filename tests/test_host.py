@@ -20,7 +20,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 NODE = np.dtype([('o', '<f4', 3), ('e', 'i1', 3), ('nint', 'u1'), ('cb', '<i4'), ('tb', '<i4'), ('meta', 'u1', 8),
                  ('qlx', 'u1', 8), ('qly', 'u1', 8), ('qlz', 'u1', 8), ('qhx', 'u1', 8), ('qhy', 'u1', 8),
                  ('qhz', 'u1', 8)])
-TRI = np.dtype([('a', '<f4', 3), ('id', '<i4'), ('b', '<f4', 3), ('e2', '<f4'), ('c', '<f4', 3), ('einf', '<f4')])
+TRI = np.dtype([('a', '<f4', 3), ('id', '<i4'), ('b', '<f4', 3), ('ke2', '<f4'), ('c', '<f4', 3), ('k', '<f4')])
 REFNODE = np.dtype([('lo', '<f4', 3), ('hi', '<f4', 3), ('left', '<i4'), ('right', '<i4'), ('escape', '<i4')])
 
 
@@ -249,9 +249,9 @@ LAYOUT_SHA256 = {
     # sha256 of the node and triangle arrays (cubvh_bvh_layout) of the host
     # build; the build splits large ranges across threads, and the tree must
     # not depend on how they are scheduled
-    "ico6": "d6f798fcb377fbc07b62e2d818314a1ed15ab49483290a3d1db4a90e1639aa18",
-    "tori": "ff842ae599bcdd508be50c66afc69923de7f22d936805246ae9e7bbb345da908",
-    "ico3": "7dd8dd1e51f207b2e627fd6a9eb2e309ba2d859a6c51110806558832f9d8a9dc",
+    "ico6": "cbd9bfb9d61c2d311a3d0a082e9ebfd14603362bb27c64da15979a0af5d52596",
+    "tori": "087878f061f19febd794558cfa5f6f961b4c98d0d7097a9c46862118821e646e",
+    "ico3": "7f0e5649b0dcbb5ef1dc884eb1f0686ad9db985fb5076507bf35891cb406ead5",
 }
 
 
@@ -263,6 +263,31 @@ def test_host_build_is_deterministic(mesh):
     for _ in range(2):
         nodes, tris, _ = layout(cubvh.cuBVH(v, f))
         assert hashlib.sha256(nodes.tobytes() + tris.tobytes()).hexdigest() == LAYOUT_SHA256[mesh]
+
+
+def test_triangle_error_factors():
+    """Each triangle record carries the FP32 distance filter's error factor
+    K = max(1, 0.3 (1 + g) + 1e-7 g^2), g = |b-a| |c-a| / |(b-a) x (c-a)|,
+    and K times its squared longest edge; zero-area triangles (a point, a
+    segment, repeated vertices) carry K = 1e30."""
+    v, f = W.random_tori(2, n_tori=2, n_major=40, n_minor=6)
+    nv = len(v)
+    extra = np.array([[0.2, 0.1, 0.85], [0.3, 0.1, 0.85], [0.4, 0.1, 0.85], [-0.3, -0.2, 0.9]], np.float32)
+    v = np.concatenate([v, extra]).astype(np.float32)
+    f = np.concatenate([f, [[nv, nv + 1, nv + 2], [nv + 3, nv + 3, nv + 3], [0, 0, 1]]]).astype(np.int64)
+    _, tris, _ = layout(cubvh.cuBVH(v, f))
+    a, b, c = (tris[k].astype(np.float64) for k in "abc")
+    u, w = b - a, a - c
+    nn = (np.cross(u, w) ** 2).sum(1)
+    degenerate = nn < 1e-30
+    assert degenerate.sum() == 3
+    assert (tris["k"][degenerate] == np.float32(1e30)).all()
+    g = np.sqrt((u * u).sum(1)[~degenerate] * (w * w).sum(1)[~degenerate] / nn[~degenerate])
+    want = np.maximum(1.0, 0.3 * (1 + g) + 1e-7 * g * g)
+    np.testing.assert_allclose(tris["k"][~degenerate], want, rtol=1e-6)
+    assert 0.05 < (tris["k"] > 1).mean() < 0.95
+    l2 = np.stack([(u * u).sum(1), ((c - b) ** 2).sum(1), (w * w).sum(1)]).max(0)
+    np.testing.assert_allclose(tris["ke2"], tris["k"] * l2, rtol=1e-6)
 
 
 def test_c_abi_rejects_bad_arguments_before_any_device_work():
