@@ -381,3 +381,54 @@ def test_degenerate_triangles(oracle, dev, stab_dirs):
     out = bvh.ray_trace(torch.from_numpy(ro).to(dev), torch.from_numpy(rd).to(dev))
     check_rays(oracle, v, f, ro, rd, out)
     assert not (_np(out[1]) >= nf).any()
+
+
+def sliver_mesh(n, seed):
+    """n disjoint slivers: needles with the small angle at a, caps with an
+    angle near 180 degrees at a, and needles with the small angle at b; the
+    sine of that angle is 1/g with g log-uniform in [1, 1e7]."""
+    rng = np.random.default_rng(seed)
+    g = 10 ** rng.uniform(0, 7, n)
+    cen = rng.uniform(-0.8, 0.8, (n, 3))
+    R = np.linalg.qr(rng.normal(size=(n, 3, 3)))[0]
+    L = rng.uniform(0.02, 0.1, n)
+    th, z, kind = 1.0 / g, 0 * L, rng.integers(0, 3, n)
+    b0 = np.stack([L, z, z], 1)
+    c = np.where(kind[:, None] == 0, np.stack([L * np.cos(th), L * np.sin(th), z], 1),
+                 np.where(kind[:, None] == 1, np.stack([-L * np.cos(th), L * np.sin(th), z], 1),
+                          np.stack([z, L * th, z], 1)))
+    tri = np.stack([cen, cen + np.einsum("nij,nj->ni", R, b0), cen + np.einsum("nij,nj->ni", R, c)], 1)
+    v = tri.reshape(-1, 3).astype(np.float32)
+    f = np.arange(3 * n, dtype=np.int64).reshape(n, 3)
+    t = v[f].astype(np.float64)
+    w = rng.dirichlet([1, 1, 1], n)
+    inside = np.einsum("nk,nkj->nj", w, t)
+    nrm = np.cross(t[:, 1] - t[:, 0], t[:, 2] - t[:, 0])
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True) + 1e-300
+    h = 10 ** rng.uniform(-4, 0, n) * rng.choice([-1, 1], n)
+    lat = rng.normal(0, 1e-3, (n, 3)) * (rng.random(n) < 0.5)[:, None]
+    pts = np.concatenate([inside + h[:, None] * nrm + lat, rng.uniform(-1, 1, (n, 3))]).astype(np.float32)
+    return v, f, pts, rng
+
+
+def test_sliver_triangles(oracle, dev, stab_dirs):
+    """Slivers, whose float plane normal is inaccurate (up to g = 1e7 times
+    the rounding of a well-shaped triangle), with points above their
+    interiors at heights 1e-4 .. 1 and off to the side: UDF + uvw, both signs
+    and rays equal the oracle bit for bit."""
+    v, f, pts, rng = sliver_mesh(3000, 51)
+    bvh = cubvh.cuBVH(v, f)
+    P = torch.from_numpy(pts).to(dev)
+    check_udf(oracle, v, f, pts, bvh.unsigned_distance(P, return_uvw=True))
+    got = bvh.signed_distance(P, return_uvw=True, mode="watertight")
+    sd, fid, _ = oracle.sdf_watertight64(v, f, pts)
+    check_sdf(got, sd, fid, "watertight")
+    got = bvh.signed_distance(P, mode="raystab")
+    sd, fid, _ = oracle.sdf_raystab64(v, f, pts, dirs=stab_dirs(len(pts)))
+    check_sdf(got, sd, fid, "raystab")
+    ro = rng.uniform(-1.5, 1.5, (6000, 3)).astype(np.float32)
+    rd = pts[rng.integers(0, 3000, 6000)] - ro
+    rd = (rd / np.linalg.norm(rd, axis=1, keepdims=True)).astype(np.float32)
+    out = bvh.ray_trace(torch.from_numpy(ro).to(dev), torch.from_numpy(rd).to(dev))
+    check_rays(oracle, v, f, ro, rd, out)
+    assert (_np(out[1]) >= 0).mean() > 0.05
