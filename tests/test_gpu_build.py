@@ -34,10 +34,20 @@ def _mesh(name):
         i = np.arange(n * n).reshape(n, n)
         a, b, c, d = i[:-1, :-1].ravel(), i[1:, :-1].ravel(), i[1:, 1:].ravel(), i[:-1, 1:].ravel()
         return v, np.concatenate([np.stack([a, b, c], 1), np.stack([a, c, d], 1)])
+    if name == "degenerate":  # zero-area faces: a segment, a point, a sphere edge
+        v, f = W.icosphere(2, 0.8)
+        nv = len(v)
+        extra = np.array([[0.2, 0.1, 0.85], [0.3, 0.1, 0.85], [0.4, 0.1, 0.85], [-0.3, -0.2, 0.9]], np.float32)
+        return (np.concatenate([v, extra]).astype(np.float32),
+                np.concatenate([f, [[nv, nv + 1, nv + 2], [nv + 3, nv + 3, nv + 3], [0, 0, 1]]]))
+    if name == "slivers":
+        from test_gpu_queries import sliver_mesh
+        v, f, _, _ = sliver_mesh(2000, 71)
+        return v, f
     raise KeyError(name)
 
 
-MESHES = ["ico4", "disp4", "tori", "dodeca", "duplicates", "flat"]
+MESHES = ["ico4", "disp4", "tori", "dodeca", "duplicates", "flat", "degenerate", "slivers"]
 
 
 @pytest.mark.parametrize("mesh", MESHES)
@@ -81,6 +91,13 @@ def test_device_build_layout(dev, mesh):
 
     walk(0)
     assert (seen == 1).all(), "every soup slot belongs to exactly one leaf"
+    # the filter's error factors equal the host builder's, face by face
+    _, htris, _ = layout(cubvh.cuBVH(v, f))
+    hk, dk = np.empty(len(f), np.float32), np.empty(len(f), np.float32)
+    hk[htris['id']], dk[tris['id']] = htris['k'], tris['k']
+    assert np.array_equal(hk, dk)
+    hk[htris['id']], dk[tris['id']] = htris['ke2'], tris['ke2']
+    assert np.array_equal(hk, dk)
 
 
 @pytest.mark.parametrize("mesh", MESHES)

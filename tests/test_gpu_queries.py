@@ -432,3 +432,34 @@ def test_sliver_triangles(oracle, dev, stab_dirs):
     out = bvh.ray_trace(torch.from_numpy(ro).to(dev), torch.from_numpy(rd).to(dev))
     check_rays(oracle, v, f, ro, rd, out)
     assert (_np(out[1]) >= 0).mean() > 0.05
+
+
+@pytest.mark.parametrize("scale,shift", [(1e-3, 0.0), (1e3, 0.0), (1.0, 3000.0), (0.05, -700.0)])
+def test_scaled_and_translated_meshes(oracle, dev, stab_dirs, scale, shift):
+    """A displaced sphere shrunk, enlarged and moved far from the origin
+    (coordinates whose float spacing is up to 2.4e-4): node quantisation,
+    the FP32 filters' error bounds (relative to |p - a|) and the fixed
+    constants of the reference's semantics (1e-3 normal radius, 1000-unit
+    stab rays) all meet the oracle bit for bit."""
+    v, f = W.displaced_icosphere(3, 1)
+    v = (v.astype(np.float64) * scale + np.array([shift, -0.5 * shift, 0.25 * shift])).astype(np.float32)
+    rng = np.random.default_rng(61)
+    lo, hi = v.min(0).astype(np.float64), v.max(0).astype(np.float64)
+    c, h = (lo + hi) / 2, (hi - lo) / 2
+    pts = np.concatenate([c + rng.uniform(-1.3, 1.3, (3000, 3)) * h,
+                          W.surface_points(v, f, 2000, 0.02 * scale, rng)]).astype(np.float32)
+    bvh = cubvh.cuBVH(v, f)
+    P = torch.from_numpy(pts).to(dev)
+    check_udf(oracle, v, f, pts, bvh.unsigned_distance(P, return_uvw=True))
+    got = bvh.signed_distance(P, return_uvw=True, mode="watertight")
+    sd, fid, _ = oracle.sdf_watertight64(v, f, pts)
+    check_sdf(got, sd, fid, "watertight")
+    got = bvh.signed_distance(P, mode="raystab")
+    sd, fid, _ = oracle.sdf_raystab64(v, f, pts, dirs=stab_dirs(len(pts)))
+    check_sdf(got, sd, fid, "raystab")
+    ro = (c + rng.uniform(-2, 2, (4000, 3)) * h).astype(np.float32)
+    rd = (c + rng.uniform(-0.5, 0.5, (4000, 3)) * h) - ro
+    rd = (rd / np.linalg.norm(rd, axis=1, keepdims=True)).astype(np.float32)
+    out = bvh.ray_trace(torch.from_numpy(ro).to(dev), torch.from_numpy(rd).to(dev))
+    check_rays(oracle, v, f, ro, rd, out)
+    assert (_np(out[1]) >= 0).mean() > 0.2

@@ -45,6 +45,38 @@ def test_watertight_after_refit(oracle, dev):
     _check(oracle, bvh, V2, F, pts2, dev)
 
 
+def test_refit_to_degenerate_faces(oracle, dev):
+    """A refit that collapses faces (an edge shrunk to a point, a vertex moved
+    onto the opposite edge) recomputes their filter error factors: distances,
+    face ids and uvw after the refit equal the oracle's, with the collapsed
+    faces among the nearest."""
+    V, F = W.displaced_icosphere(3, 2)
+    bvh = cubvh.cuBVH(V, F)
+    rng = np.random.default_rng(13)
+    pts = W.uniform_points(4000, 7)
+    bvh.unsigned_distance(torch.from_numpy(pts).to(dev))
+    V2 = V.copy()
+    sel = rng.choice(len(F), 40, replace=False)
+    for k, t in enumerate(sel):
+        a, b, c = F[t]
+        if k % 2 == 0:
+            V2[b] = V2[a]                      # edge a-b shrunk to a point
+        else:
+            V2[c] = 0.5 * (V2[a] + V2[b])      # c on the edge a-b
+    bvh.refit(torch.from_numpy(V2).to(dev))
+    around = V2[F[sel]].mean(1).repeat(50, 0) + rng.normal(0, 0.01, (2000, 3))
+    near = np.concatenate([pts, around]).astype(np.float32)
+    d, fid, uvw = bvh.unsigned_distance(torch.from_numpy(near).to(dev), return_uvw=True)
+    od, ofid, ouvw, _, _ = oracle.udf64(V2, F, near)
+    assert np.array_equal(_np(d), od.astype(np.float32))
+    assert np.array_equal(_np(fid), ofid)
+    assert np.array_equal(_np(uvw), ouvw.astype(np.float32))
+    t = V2[F].astype(np.float64)
+    zero = np.linalg.norm(np.cross(t[:, 1] - t[:, 0], t[:, 2] - t[:, 0]), axis=1) == 0
+    assert zero.sum() >= 20 and zero[ofid].sum() > 0
+    _check(oracle, bvh, V2, F, near, dev)
+
+
 def _double_cone(n=40, r=0.5, h=0.6):
     a = np.linspace(0, 2 * np.pi, n, endpoint=False)
     ring = np.stack([r * np.cos(a), r * np.sin(a), np.zeros(n)], 1)
