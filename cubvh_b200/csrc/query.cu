@@ -26,6 +26,7 @@
 #include <climits>
 #include <cstdint>
 #include <cooperative_groups.h>
+#include <cub/block/block_radix_sort.cuh>
 #include <cuda_runtime.h>
 #include <math_constants.h>
 
@@ -1271,14 +1272,19 @@ __global__ void __launch_bounds__(kQBlock, 10) k_sign_raystab_lines(const float*
 }
 
 // ---------------------------------------------------------------- rays
-// Closest hit of 32 consecutive rays per warp (a packet): warp-uniform walk of
+constexpr int kUnit = 8;   // rays per unit of the ray packet order (k_ray_order), 4 units per packet
+// Closest hit of 32 rays per warp (a packet: the rays of 4 consecutive
+// entries of `order`, units of 8 consecutive rays sorted so that nearby ones
+// are side by side (k_ray_order), or 32 consecutive rays when it is null):
+// warp-uniform walk of
 // the union of the rays' paths, children in the order of the smallest entry
 // distance of any ray that needs them.  Each lane keeps U, an upper bound of
 // its closest hit (certain FP32 hits: t + error bound), and a short list of
 // triangles that may still be closer (certain or undecided hits whose lower
 // bound is within U); the list is settled in double at the end: exact t of
 // the closest hit, ties -> lowest face index.
-__global__ void __launch_bounds__(kQBlock) k_ray(int64_t n, const float* __restrict__ ro,
+__global__ void __launch_bounds__(kQBlock) k_ray(int64_t n, const uint32_t* __restrict__ order,
+                                                 const float* __restrict__ ro,
                                                  const float* __restrict__ rd, float* __restrict__ pos,
                                                  int64_t* __restrict__ face_id, float* __restrict__ depth,
                                                  const CNode* __restrict__ nodes, const CTri* __restrict__ tris,
@@ -1289,8 +1295,13 @@ __global__ void __launch_bounds__(kQBlock) k_ray(int64_t n, const float* __restr
     __shared__ int s_sref[kQBlock / 32][kSmemStack];
     __shared__ uint32_t s_skey[kQBlock / 32][kSmemStack];
     PacketQueue pq(ctr, (n + 31) >> 5, grab);
+    const int64_t units = (n + kUnit - 1) / kUnit;
     for (int64_t pk = pq.take(); pk >= 0; pk = pq.take()) {
-        const int64_t q = pk * 32 + lane;
+        int64_t q = pk * 32 + lane;
+        if (order) {                  // unit lane / 8 of the packet, ray lane % 8 of the unit
+            const int64_t slot = pk * (32 / kUnit) + lane / kUnit;
+            q = slot < units ? (int64_t)__ldg(order + slot) * kUnit + lane % kUnit : n;
+        }
         const bool act = q < n;
         const float3 o = act ? load3(ro, q) : make_float3(0.f, 0.f, 0.f);
         const float3 d = act ? load3(rd, q) : make_float3(1.f, 1.f, 1.f);
@@ -1445,6 +1456,116 @@ __global__ void k_cell_scatter(int64_t n, const float* __restrict__ pts, const u
         order[atomicAdd(&offs[cell_of(load3(pts, i), box, bits)], 1u)] = (uint32_t)i;
 }
 
+// ---------------------------------------------------------- ray windows
+// Packet order of rays.  Rays are taken in units of kUnit consecutive rays,
+// and each window of kOrdUnits consecutive units is sorted by the Morton
+// code of the point where one ray of the unit (its fourth) enters the root
+// node's box (its origin when it starts inside; units whose ray misses the
+// box go last, then the window's tail past the last unit), on cells of one
+// size on all three axes (the window's largest extent / 1024).  A packet is
+// four consecutive units of the sorted order.  Camera rays stored row by row
+// then make packets of 8 pixels from each of 4 neighbouring rows instead of
+// 32 x 1 strips, and the union of the 32 rays' walks visits far fewer nodes
+// (C1 camera rays: 6.4 -> 5.3 ms in k_ray, for a sort of 1,024 keys per
+// 8,192 rays that reads one ray in eight).  The order changes no result:
+// each ray's hit is its own.
+constexpr int kOrdThreads = 256, kOrdItems = 4;
+constexpr int kOrdUnits = kOrdThreads * kOrdItems;    // 1024 units = 8192 rays per window
+constexpr int64_t kOrdMinRays = 1 << 16;
+// Entry point of ray q into the box [lo, lo + 255 * 2^ex] (the origin when
+// the ray starts inside; non-finite coordinates become 0): 0, or 1 when the
+// ray misses the box (e = the origin).
+__device__ __forceinline__ int ray_entry(const float* __restrict__ ro, const float* __restrict__ rd, int64_t q,
+                                         const float lo[3], const int ex[3], float e[3]) {
+    const float3 o = load3(ro, q), d = load3(rd, q);
+    const float oc[3] = {o.x, o.y, o.z}, dc[3] = {d.x, d.y, d.z};
+    float tn = 0.f, tf = CUDART_INF_F;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float hi = fmaf(255.f, exp2i(ex[k]), lo[k]);
+        const float inv = 1.f / dc[k];
+        const float ta = (lo[k] - oc[k]) * inv, tb = (hi - oc[k]) * inv;
+        tn = fmaxf(tn, fminf(ta, tb));   // NaN (0 * inf) leaves the bound as it was
+        tf = fminf(tf, fmaxf(ta, tb));
+    }
+    const int miss = tn <= tf ? 0 : 1;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float v = miss ? oc[k] : fmaf(dc[k], tn, oc[k]);
+        e[k] = isfinite(v) ? v : 0.f;
+    }
+    return miss;
+}
+// One block per window: entry points of the units' rays, the box of those
+// that enter, Morton keys, a block radix sort of (key, unit in the window),
+// and the sorted unit indices written to order[].
+__global__ void __launch_bounds__(kOrdThreads) k_ray_order(int64_t n, const float* __restrict__ ro,
+                                                           const float* __restrict__ rd,
+                                                           const CNode* __restrict__ nodes,
+                                                           uint32_t* __restrict__ order) {
+    using Sort = cub::BlockRadixSort<uint32_t, kOrdThreads, kOrdItems, uint16_t>;
+    __shared__ typename Sort::TempStorage s_sort;
+    __shared__ uint32_t s_box[6];
+    const int64_t units = (n + kUnit - 1) / kUnit;
+    const int64_t u0 = (int64_t)blockIdx.x * kOrdUnits;
+    const int t = threadIdx.x;
+    if (t < 3) s_box[t] = 0xFFFFFFFFu;
+    else if (t < 6) s_box[t] = 0u;
+    const float blo[3] = {nodes[0].ox, nodes[0].oy, nodes[0].oz};
+    const int bex[3] = {nodes[0].ex, nodes[0].ey, nodes[0].ez};
+    float ep[kOrdItems][3];
+    int kind[kOrdItems];              // 0 enters the box, 1 misses it, 2 past the last unit
+    uint32_t lo[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, hi[3] = {0u, 0u, 0u};
+#pragma unroll
+    for (int i = 0; i < kOrdItems; ++i) {
+        const int64_t u = u0 + i * kOrdThreads + t;
+        kind[i] = 2;
+        ep[i][0] = ep[i][1] = ep[i][2] = 0.f;
+        if (u >= units) continue;
+        const int64_t q = min(u * kUnit + 3, n - 1);
+        kind[i] = ray_entry(ro, rd, q, blo, bex, ep[i]);
+        if (kind[i] == 0) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) { lo[k] = min(lo[k], f2o(ep[i][k])); hi[k] = max(hi[k], f2o(ep[i][k])); }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = __reduce_min_sync(kFull, lo[k]);
+        hi[k] = __reduce_max_sync(kFull, hi[k]);
+    }
+    __syncthreads();                  // s_box initialised
+    if ((t & 31) == 0) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { atomicMin(&s_box[k], lo[k]); atomicMax(&s_box[3 + k], hi[k]); }
+    }
+    __syncthreads();
+    float wlo[3], ext = 0.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        wlo[k] = o2f(s_box[k]);
+        ext = fmaxf(ext, o2f(s_box[3 + k]) - wlo[k]);   // no entry point: the box is empty, ext stays 0
+    }
+    const float sc = ext > 0.f ? 1024.f / ext : 0.f;
+    uint32_t key[kOrdItems];
+    uint16_t val[kOrdItems];
+#pragma unroll
+    for (int i = 0; i < kOrdItems; ++i) {
+        val[i] = (uint16_t)(i * kOrdThreads + t);
+        if (kind[i] != 0) { key[i] = kind[i] == 1 ? 0x40000000u : 0x80000000u; continue; }
+        uint32_t g[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) g[k] = (uint32_t)fminf(fmaxf((ep[i][k] - wlo[k]) * sc, 0.f), 1023.f);
+        key[i] = spread3(g[0]) | (spread3(g[1]) << 1) | (spread3(g[2]) << 2);
+    }
+    Sort(s_sort).SortBlockedToStriped(key, val, 0, 32);
+#pragma unroll
+    for (int i = 0; i < kOrdItems; ++i) {
+        const int64_t r = u0 + i * kOrdThreads + t;      // rank i * kOrdThreads + t of the window
+        if (r < units) order[r] = (uint32_t)(u0 + val[i]);
+    }
+}
+
 // --------------------------------------------------------------- launchers
 namespace {
 
@@ -1502,6 +1623,7 @@ size_t query_workspace_bytes(int mode, int64_t n) {
     if (mode == 1) b += al(sizeof(uint32_t) * n);                 // watertight overflow queue
     if (mode >= 0) b += al(sizeof(uint2) * heavy_cap_for(n));     // heavy-query list
     if (mode == 2) b += al(sizeof(uint4) * n);                    // raystab candidates (second pass)
+    if (mode == -1 && n >= kOrdMinRays) b += al(sizeof(uint32_t) * ((n + kUnit - 1) / kUnit));   // ray unit order
     return b;
 }
 
@@ -1667,8 +1789,15 @@ cudaError_t launch_ray(int64_t n, const float* ro, const float* rd, float* pos, 
     unsigned long long* ctr = reinterpret_cast<unsigned long long*>(ws);
     cudaError_t e = cudaMemsetAsync(ctr, 0, 256, stream);
     if (e != cudaSuccess) return e;
+    uint32_t* order = nullptr;
+    if (n >= kOrdMinRays) {
+        order = reinterpret_cast<uint32_t*>(static_cast<char*>(ws) + 256);
+        const int64_t units = (n + kUnit - 1) / kUnit;
+        k_ray_order<<<(unsigned)((units + kOrdUnits - 1) / kOrdUnits), kOrdThreads, 0, stream>>>(n, ro, rd, nodes,
+                                                                                                order); count_launch();
+    }
     const unsigned g = persistent_grid(k_ray, n);
-    k_ray<<<g, kQBlock, 0, stream>>>(n, ro, rd, pos, fid, depth, nodes, tris, ctr + kCtUdf, grab_for(n, g)); count_launch();
+    k_ray<<<g, kQBlock, 0, stream>>>(n, order, ro, rd, pos, fid, depth, nodes, tris, ctr + kCtUdf, grab_for(n, g)); count_launch();
     return cudaGetLastError();
 }
 

@@ -463,3 +463,79 @@ def test_scaled_and_translated_meshes(oracle, dev, stab_dirs, scale, shift):
     out = bvh.ray_trace(torch.from_numpy(ro).to(dev), torch.from_numpy(rd).to(dev))
     check_rays(oracle, v, f, ro, rd, out)
     assert (_np(out[1]) >= 0).mean() > 0.2
+
+
+def test_exact_ties_at_vertices_edges_and_centroids(oracle, dev, stab_dirs):
+    """Queries exactly at the mesh vertices (distance 0 to every incident
+    face), on shared edges, at face centroids, and rays aimed at vertices
+    and edge points: every exact tie goes to the lowest face index, as in
+    the oracle, and all outputs equal it bit for bit."""
+    v, f = W.random_tori(2, n_tori=2, n_major=32, n_minor=10)
+    v, f = np.asarray(v, np.float32), np.asarray(f, np.int64)
+    rng = np.random.default_rng(77)
+    e = np.concatenate([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]])
+    mid = (0.5 * (v[e[:, 0]].astype(np.float64) + v[e[:, 1]])).astype(np.float32)
+    cen = v[f].astype(np.float64).mean(1).astype(np.float32)
+    used = v[np.unique(f)]                     # vertices of at least one face
+    pts = np.concatenate([used, mid[rng.permutation(len(mid))[:3000]], cen[:2000]])
+    bvh = cubvh.cuBVH(v, f)
+    P = torch.from_numpy(pts).to(dev)
+    out = bvh.unsigned_distance(P, return_uvw=True)
+    check_udf(oracle, v, f, pts, out)
+    d = _np(out[0])
+    assert (d[:len(used)] == 0).all()
+    _, _, _, _, nn = oracle.udf64(v, f, pts)
+    assert (nn[:len(used)] >= 2).mean() > 0.9  # vertices: ties among the incident faces
+    got = bvh.signed_distance(P, return_uvw=True, mode="watertight")
+    sd, fid, _ = oracle.sdf_watertight64(v, f, pts)
+    check_sdf(got, sd, fid, "watertight")
+    got = bvh.signed_distance(P, mode="raystab")
+    sd, fid, _ = oracle.sdf_raystab64(v, f, pts, dirs=stab_dirs(len(pts)))
+    check_sdf(got, sd, fid, "raystab")
+    tgt = np.concatenate([used[rng.integers(0, len(used), 3000)], mid[rng.integers(0, len(mid), 3000)]]).astype(np.float64)
+    ro = rng.uniform(-2, 2, (6000, 3))
+    rd = tgt - ro
+    rd = (rd / np.linalg.norm(rd, axis=1, keepdims=True)).astype(np.float32)
+    ro = ro.astype(np.float32)
+    out = bvh.ray_trace(torch.from_numpy(ro).to(dev), torch.from_numpy(rd).to(dev))
+    fl = check_rays(oracle, v, f, ro, rd, out)
+    assert (_np(out[1]) >= 0).mean() > 0.8 and (fl & 2).sum() > 10   # with exact ties in t
+
+
+def test_ray_trace_window_order(oracle, dev):
+    """Calls of at least 65,536 rays trace them in packets of nearby rays
+    (a sort of each 8,192-ray window by box entry point): camera rays, rays
+    from inside, rays that miss the box, axis-parallel and non-finite rays,
+    and a last window that is only partly filled.  Results equal the oracle's
+    and those of the same rays traced in calls below that size."""
+    v, f = W.displaced_icosphere(4, 1)
+    bvh = cubvh.cuBVH(v, f)
+    ro_c, rd_c = W.camera_rays(4, 128, 50.0, 2.5, 7)
+    rng = np.random.default_rng(81)
+    m = 20000 + 123
+    ro_r = rng.uniform(-1.5, 1.5, (m, 3)).astype(np.float32)
+    rd_r = rng.standard_normal((m, 3)).astype(np.float32)
+    rd_r[:500, 0] = 0.0
+    rd_r[500:600, 1:] = 0.0
+    rd_r /= np.linalg.norm(rd_r, axis=1, keepdims=True)
+    ro_r[600:700] += np.float32(10.0)           # far outside, pointing anywhere: mostly misses
+    ro = np.concatenate([ro_c, ro_r]).astype(np.float32)
+    rd = np.concatenate([rd_c, rd_r]).astype(np.float32)
+    n = len(ro)
+    assert n >= 65536 and n % 8192 != 0
+    ro_t, rd_t = torch.from_numpy(ro).to(dev), torch.from_numpy(rd).to(dev)
+    whole = bvh.ray_trace(ro_t, rd_t)
+    parts = [bvh.ray_trace(ro_t[i:i + 30000], rd_t[i:i + 30000]) for i in range(0, n, 30000)]
+    for k in range(3):
+        assert torch.equal(whole[k], torch.cat([p[k] for p in parts]))
+    check_rays(oracle, v, f, ro, rd, whole)
+    hit = _np(whole[1]) >= 0
+    assert 0.2 < hit.mean() < 0.9
+    bad = rd.copy()
+    bad[rng.choice(n, 64, replace=False), 0] = np.nan
+    bad[rng.choice(n, 64, replace=False), 2] = np.inf
+    keep = np.isfinite(bad).all(1)
+    got = bvh.ray_trace(ro_t, torch.from_numpy(bad).to(dev))
+    m_t = torch.from_numpy(keep).to(dev)
+    for x, y in zip(got, whole):
+        assert torch.equal(x[m_t], y[m_t])
