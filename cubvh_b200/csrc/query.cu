@@ -282,6 +282,52 @@ __device__ __forceinline__ void ray_child_keys(const NodeLinks& nd, const float*
         k[j] = need ? __float_as_uint(key) : kFull;
     }
 }
+// Closest-hit step of one lane's own walk: entry distance (ordered bits of
+// max(tn, 0), child index in the low 3 bits) of the ray into each child of
+// nd that it enters within [0, cull], kFull for the others.  degen (a zero
+// or subnormal direction component): box_ray<true> on the decoded boxes;
+// else the affine fold of push_ray_children_affine (same error margins).
+__device__ __forceinline__ void lane_child_keys(const NodeView& nd, float3 o, float3 inv, bool degen, float cull,
+                                                uint32_t k[8]) {
+    if (degen) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            float3 lo, hi;
+            child_box(nd, j, lo, hi);
+            float tn, tf;
+            box_ray<true>(o, inv, lo, hi, tn, tf);
+            const float key = fmaxf(tn, 0.f);
+            const bool need = meta_of(nd, j) != kEmpty && tn <= tf && tf >= 0.f && key <= cull;
+            k[j] = need ? ((__float_as_uint(key) & ~7u) | (uint32_t)j) : kFull;
+        }
+        return;
+    }
+    const float ax = nd.sx * inv.x, ay = nd.sy * inv.y, az = nd.sz * inv.z;
+    const float bx = (nd.ox - o.x) * inv.x, by = (nd.oy - o.y) * inv.y, bz = (nd.oz - o.z) * inv.z;
+    const float ex = 1e-6f * (fabsf(nd.ox * inv.x) + 255.f * fabsf(ax) + fabsf(bx));
+    const float ey = 1e-6f * (fabsf(nd.oy * inv.y) + 255.f * fabsf(ay) + fabsf(by));
+    const float ez = 1e-6f * (fabsf(nd.oz * inv.z) + 255.f * fabsf(az) + fabsf(bz));
+    const float nbx = bx - ex, fbx = bx + ex, nby = by - ey, fby = by + ey, nbz = bz - ez, fbz = bz + ez;
+    const bool px = inv.x >= 0.f, py = inv.y >= 0.f, pz = inv.z >= 0.f;
+    const uint32_t nx0 = px ? nd.lx0 : nd.hx0, nx1 = px ? nd.lx1 : nd.hx1;
+    const uint32_t fx0 = px ? nd.hx0 : nd.lx0, fx1 = px ? nd.hx1 : nd.lx1;
+    const uint32_t ny0 = py ? nd.ly0 : nd.hy0, ny1 = py ? nd.ly1 : nd.hy1;
+    const uint32_t fy0 = py ? nd.hy0 : nd.ly0, fy1 = py ? nd.hy1 : nd.ly1;
+    const uint32_t nz0 = pz ? nd.lz0 : nd.hz0, nz1 = pz ? nd.lz1 : nd.hz1;
+    const uint32_t fz0 = pz ? nd.hz0 : nd.lz0, fz1 = pz ? nd.hz1 : nd.lz1;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int b = j & 3;
+        const bool h = j >= 4;
+        const float tn = fmaxf(fmaxf(fmaf(qbyte(h ? nx1 : nx0, b), ax, nbx), fmaf(qbyte(h ? ny1 : ny0, b), ay, nby)),
+                               fmaf(qbyte(h ? nz1 : nz0, b), az, nbz));
+        const float tf = fminf(fminf(fmaf(qbyte(h ? fx1 : fx0, b), ax, fbx), fmaf(qbyte(h ? fy1 : fy0, b), ay, fby)),
+                               fmaf(qbyte(h ? fz1 : fz0, b), az, fbz));
+        const float key = fmaxf(tn, 0.f);
+        const bool need = meta_of(nd, j) != kEmpty && tn <= tf && tf >= 0.f && key <= cull;
+        k[j] = need ? ((__float_as_uint(key) & ~7u) | (uint32_t)j) : kFull;
+    }
+}
 __device__ __forceinline__ float cull_of(double best) { return __double2float_ru(dM(best, 1.000001)); }
 __device__ __forceinline__ void leaf_range(int ref, int& s0, int& s1) {
     const int code = -ref - 1;
@@ -1273,9 +1319,25 @@ __global__ void __launch_bounds__(kQBlock, 10) k_sign_raystab_lines(const float*
 
 // ---------------------------------------------------------------- rays
 constexpr int kUnit = 8;   // rays per unit of the ray packet order (k_ray_order), 4 units per packet
+// Ray of `lane` in packet pk: the unit lane / 8 of the packet's four entries
+// of order[] (units of 8 consecutive rays); n when there is none.
+__device__ __forceinline__ int64_t packet_ray(int64_t pk, int lane, int64_t n, const uint32_t* __restrict__ order) {
+    const int64_t units = (n + kUnit - 1) / kUnit;
+    const int64_t slot = pk * (32 / kUnit) + lane / kUnit;
+    return slot < units ? (int64_t)__ldg(order + slot) * kUnit + lane % kUnit : n;
+}
+// A packet is traced as a packet only when its rays are nearly parallel
+// (unit directions within kCohDir, max-norm, of one another's: about 6
+// degrees) and start close together (origins within kCohOrigin of the root
+// box's extent), as k_ray_order judges it; the others go to k_ray_lanes,
+// where each ray walks alone: the union of 32 unrelated walks costs far more
+// than their longest one.
+constexpr float kCohDir = 0.1f;
+constexpr float kCohOrigin = 0.01f;
 // Closest hit of 32 rays per warp (a packet: the rays of 4 consecutive
 // entries of `order`, units of 8 consecutive rays sorted so that nearby ones
-// are side by side (k_ray_order), or 32 consecutive rays when it is null):
+// are side by side (k_ray_order); packets k_ray_order marked incoherent are
+// skipped, k_ray_lanes traces them):
 // warp-uniform walk of
 // the union of the rays' paths, children in the order of the smallest entry
 // distance of any ray that needs them.  Each lane keeps U, an upper bound of
@@ -1288,20 +1350,17 @@ __global__ void __launch_bounds__(kQBlock) k_ray(int64_t n, const uint32_t* __re
                                                  const float* __restrict__ rd, float* __restrict__ pos,
                                                  int64_t* __restrict__ face_id, float* __restrict__ depth,
                                                  const CNode* __restrict__ nodes, const CTri* __restrict__ tris,
-                                                 unsigned long long* __restrict__ ctr, int64_t grab) {
+                                                 unsigned long long* __restrict__ ctr, int64_t grab,
+                                                 const uint8_t* __restrict__ skip) {
     const int lane = threadIdx.x & 31;
     __shared__ __align__(16) float s_box[kQBlock / 32][64];
     float* sb = s_box[threadIdx.x >> 5];
     __shared__ int s_sref[kQBlock / 32][kSmemStack];
     __shared__ uint32_t s_skey[kQBlock / 32][kSmemStack];
     PacketQueue pq(ctr, (n + 31) >> 5, grab);
-    const int64_t units = (n + kUnit - 1) / kUnit;
     for (int64_t pk = pq.take(); pk >= 0; pk = pq.take()) {
-        int64_t q = pk * 32 + lane;
-        if (order) {                  // unit lane / 8 of the packet, ray lane % 8 of the unit
-            const int64_t slot = pk * (32 / kUnit) + lane / kUnit;
-            q = slot < units ? (int64_t)__ldg(order + slot) * kUnit + lane % kUnit : n;
-        }
+        if (__ldg(skip + pk)) continue;   // incoherent: k_ray_lanes traces it
+        const int64_t q = packet_ray(pk, lane, n, order);
         const bool act = q < n;
         const float3 o = act ? load3(ro, q) : make_float3(0.f, 0.f, 0.f);
         const float3 d = act ? load3(rd, q) : make_float3(1.f, 1.f, 1.f);
@@ -1456,28 +1515,128 @@ __global__ void k_cell_scatter(int64_t n, const float* __restrict__ pts, const u
         order[atomicAdd(&offs[cell_of(load3(pts, i), box, bits)], 1u)] = (uint32_t)i;
 }
 
+// Closest hit of the rays of the incoherent packets k_ray listed: a warp
+// takes a packet, and each lane walks its own ray alone (own stack in local
+// memory, children nearest first, a child popped only while its entry
+// distance is within the lane's bound U).  A step is one node or one leaf.
+// Filters, candidate list and the FP64 settlement are k_ray's, so every
+// result is the one k_ray would give.
+__global__ void __launch_bounds__(kQBlock) k_ray_lanes(int64_t n, const uint32_t* __restrict__ order,
+                                                       const float* __restrict__ ro, const float* __restrict__ rd,
+                                                       float* __restrict__ pos, int64_t* __restrict__ face_id,
+                                                       float* __restrict__ depth, const CNode* __restrict__ nodes,
+                                                       const CTri* __restrict__ tris,
+                                                       const uint32_t* __restrict__ lanes,
+                                                       const unsigned long long* __restrict__ lanes_n,
+                                                       unsigned long long* __restrict__ next) {
+    const int lane = threadIdx.x & 31;
+    const unsigned long long count = *lanes_n;
+    int st_ref[kStack];
+    uint32_t st_key[kStack];
+    while (true) {
+        unsigned long long c = 0;
+        if (lane == 0) c = atomicAdd(next, 1ull);
+        c = __shfl_sync(kFull, c, 0);
+        if (c >= count) break;
+        const int64_t q = packet_ray((int64_t)lanes[c], lane, n, order);
+        const bool act = q < n;
+        const float3 o = act ? load3(ro, q) : make_float3(0.f, 0.f, 0.f);
+        const float3 d = act ? load3(rd, q) : make_float3(1.f, 1.f, 1.f);
+        const float3 inv = ray_inv(d);
+        const bool degen = ray_degenerate(inv);
+        const float dinf = f3inf(d);
+        const d3 od = to_d3(o), dd = to_d3(d);
+        float U = 1000.0f;                          // MAX_DIST
+        float cull = U * 1.000002f;
+        int cs[kCand];
+        float cl[kCand];
+        int nc = 0;
+        double bt = 1000.0;
+        int sx = -1, ix = -1;
+        auto flush = [&](bool final_pass) {
+            for (int i = 0; i < nc; ++i) {
+                if (final_pass && cl[i] > U) continue;
+                const TriV t = load_tri(tris, cs[i]);
+                double t64;
+                if (!ray_tri_d(od, dd, to_d3(t.a), to_d3(t.b), to_d3(t.c), 1000.0, &t64)) continue;
+                if (t64 < bt || (t64 == bt && (sx < 0 || t.id < ix))) { bt = t64; sx = cs[i]; ix = t.id; }
+            }
+            nc = 0;
+        };
+        int sp = 0, cur = 0;
+        bool live = act;
+        while (live) {
+            if (cur >= 0) {
+                const NodeView nd = load_node(nodes, cur);
+                uint32_t k[8];
+                lane_child_keys(nd, o, inv, degen, cull, k);
+                sort8(k);
+#pragma unroll
+                for (int i = 7; i >= 1; --i)
+                    if (k[i] != kFull) { st_ref[sp] = child_ref(nd, meta_of(nd, (int)(k[i] & 7u))); st_key[sp] = k[i] & ~7u; ++sp; }
+                if (k[0] != kFull) { cur = child_ref(nd, meta_of(nd, (int)(k[0] & 7u))); continue; }
+            } else {
+                int s0, s1;
+                leaf_range(cur, s0, s1);
+                for (int s = s0; s < s1; ++s) {
+                    const TriV t = load_tri(tris, s);
+                    float tt, terr;
+                    const int r = ray_tri_f(o, d, dinf, t, 1000.0f, &tt, &terr);
+                    const float lb = tt - terr;
+                    if (r != 0 && lb <= U) {
+                        if (r == 1) U = fminf(U, tt + terr);
+                        if (nc == kCand) {
+                            int m = 0;
+                            for (int i = 0; i < nc; ++i)
+                                if (cl[i] <= U) { cs[m] = cs[i]; cl[m] = cl[i]; ++m; }
+                            nc = m;
+                            if (nc == kCand) {
+                                flush(false);
+                                if (sx >= 0) U = fminf(U, __double2float_ru(bt));
+                            }
+                        }
+                        cs[nc] = s; cl[nc] = lb; ++nc;
+                    }
+                }
+                cull = U * 1.000002f;
+            }
+            live = false;             // the next entry whose box is still within the bound
+            while (sp > 0) {
+                --sp;
+                if (__uint_as_float(st_key[sp]) <= cull) { cur = st_ref[sp]; live = true; break; }
+            }
+        }
+        if (!act) continue;
+        flush(true);
+        depth[q] = __double2float_rn(bt);
+        pos[3 * q] = __double2float_rn(dA((double)o.x, dM(bt, (double)d.x)));
+        pos[3 * q + 1] = __double2float_rn(dA((double)o.y, dM(bt, (double)d.y)));
+        pos[3 * q + 2] = __double2float_rn(dA((double)o.z, dM(bt, (double)d.z)));
+        face_id[q] = sx >= 0 ? (int64_t)ix : (int64_t)-1;
+    }
+}
+
 // ---------------------------------------------------------- ray windows
 // Packet order of rays.  Rays are taken in units of kUnit consecutive rays,
 // and each window of kOrdUnits consecutive units is sorted by the Morton
 // code of the point where one ray of the unit (its fourth) enters the root
-// node's box (its origin when it starts inside; units whose ray misses the
-// box go last, then the window's tail past the last unit), on cells of one
-// size on all three axes (the window's largest extent / 1024).  A packet is
-// four consecutive units of the sorted order.  Camera rays stored row by row
-// then make packets of 8 pixels from each of 4 neighbouring rows instead of
-// 32 x 1 strips, and the union of the 32 rays' walks visits far fewer nodes
-// (C1 camera rays: 6.4 -> 5.3 ms in k_ray, for a sort of 1,024 keys per
-// 8,192 rays that reads one ray in eight).  The order changes no result:
-// each ray's hit is its own.
+// node's box (its origin when it starts inside), on cells of one size on all
+// three axes (the window's largest extent / 1024); units whose ray misses
+// the box go after the others, in the Morton order of where that ray passes
+// closest to the box centre (clamped into the cells), then the window's tail
+// past the last unit.  A packet is four consecutive units of the sorted
+// order.  Camera rays stored row by row then make packets of 8 pixels from
+// each of 4 neighbouring rows instead of 32 x 1 strips, and the union of the
+// 32 rays' walks visits far fewer nodes (C1 camera rays: k_ray 6.4 -> 5.1
+// ms, for a sort of 1,024 keys per 8,192 rays).  The order changes no
+// result: each ray's hit is its own.
 constexpr int kOrdThreads = 256, kOrdItems = 4;
 constexpr int kOrdUnits = kOrdThreads * kOrdItems;    // 1024 units = 8192 rays per window
-constexpr int64_t kOrdMinRays = 1 << 16;
-// Entry point of ray q into the box [lo, lo + 255 * 2^ex] (the origin when
+// Entry point of ray (o, d) into the box [lo, lo + 255 * 2^ex] (the origin when
 // the ray starts inside; non-finite coordinates become 0): 0, or 1 when the
-// ray misses the box (e = the origin).
-__device__ __forceinline__ int ray_entry(const float* __restrict__ ro, const float* __restrict__ rd, int64_t q,
-                                         const float lo[3], const int ex[3], float e[3]) {
-    const float3 o = load3(ro, q), d = load3(rd, q);
+// ray misses the box (e = the point where it passes closest to the box
+// centre, for t >= 0).
+__device__ __forceinline__ int ray_entry(float3 o, float3 d, const float lo[3], const int ex[3], float e[3]) {
     const float oc[3] = {o.x, o.y, o.z}, dc[3] = {d.x, d.y, d.z};
     float tn = 0.f, tf = CUDART_INF_F;
 #pragma unroll
@@ -1489,45 +1648,82 @@ __device__ __forceinline__ int ray_entry(const float* __restrict__ ro, const flo
         tf = fminf(tf, fmaxf(ta, tb));
     }
     const int miss = tn <= tf ? 0 : 1;
+    if (miss) {                       // where the ray passes closest to the box centre
+        float cd = 0.f, dd = 0.f;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float c = 0.5f * (lo[k] + fmaf(255.f, exp2i(ex[k]), lo[k]));
+            cd = fmaf(c - oc[k], dc[k], cd);
+            dd = fmaf(dc[k], dc[k], dd);
+        }
+        tn = fmaxf(cd / dd, 0.f);
+    }
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        const float v = miss ? oc[k] : fmaf(dc[k], tn, oc[k]);
+        const float v = fmaf(dc[k], tn, oc[k]);
         e[k] = isfinite(v) ? v : 0.f;
     }
     return miss;
 }
 // One block per window: entry points of the units' rays, the box of those
 // that enter, Morton keys, a block radix sort of (key, unit in the window),
-// and the sorted unit indices written to order[].
+// and the sorted unit indices written to order[].  Then each packet of the
+// window (4 consecutive sorted units) is judged: coherent when the first,
+// fourth and last rays of its units all lie within kCohDir (directions) and
+// kCohOrigin (origins) of its first unit's fourth ray.  skip[p] = 1 marks
+// the others for k_ray, and they are listed for k_ray_lanes.
 __global__ void __launch_bounds__(kOrdThreads) k_ray_order(int64_t n, const float* __restrict__ ro,
                                                            const float* __restrict__ rd,
                                                            const CNode* __restrict__ nodes,
-                                                           uint32_t* __restrict__ order) {
+                                                           uint32_t* __restrict__ order, uint8_t* __restrict__ skip,
+                                                           uint32_t* __restrict__ lanes,
+                                                           unsigned long long* __restrict__ lanes_n) {
     using Sort = cub::BlockRadixSort<uint32_t, kOrdThreads, kOrdItems, uint16_t>;
     __shared__ typename Sort::TempStorage s_sort;
     __shared__ uint32_t s_box[6];
+    __shared__ float s_ray[kOrdUnits][6];     // each unit's fourth ray: unit direction, origin
+    __shared__ uint8_t s_bad[kOrdUnits];       // the unit's first or last ray strays from its fourth
+    __shared__ uint16_t s_sorted[kOrdUnits];
     const int64_t units = (n + kUnit - 1) / kUnit;
     const int64_t u0 = (int64_t)blockIdx.x * kOrdUnits;
     const int t = threadIdx.x;
     if (t < 3) s_box[t] = 0xFFFFFFFFu;
     else if (t < 6) s_box[t] = 0u;
-    const float blo[3] = {nodes[0].ox, nodes[0].oy, nodes[0].oz};
+    const NodeView root = load_node(nodes, 0);
+    const float blo[3] = {root.ox, root.oy, root.oz};
     const int bex[3] = {nodes[0].ex, nodes[0].ey, nodes[0].ez};
+    const float spread_max = kCohOrigin * 255.f * fmaxf(fmaxf(root.sx, root.sy), root.sz);
     float ep[kOrdItems][3];
     int kind[kOrdItems];              // 0 enters the box, 1 misses it, 2 past the last unit
     uint32_t lo[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, hi[3] = {0u, 0u, 0u};
 #pragma unroll
     for (int i = 0; i < kOrdItems; ++i) {
-        const int64_t u = u0 + i * kOrdThreads + t;
+        const int li = i * kOrdThreads + t;
+        const int64_t u = u0 + li;
         kind[i] = 2;
         ep[i][0] = ep[i][1] = ep[i][2] = 0.f;
         if (u >= units) continue;
-        const int64_t q = min(u * kUnit + 3, n - 1);
-        kind[i] = ray_entry(ro, rd, q, blo, bex, ep[i]);
+        const int64_t q = min(u * kUnit + kUnit / 2 - 1, n - 1);
+        const float3 o = load3(ro, q), d = load3(rd, q);
+        kind[i] = ray_entry(o, d, blo, bex, ep[i]);
         if (kind[i] == 0) {
 #pragma unroll
             for (int k = 0; k < 3; ++k) { lo[k] = min(lo[k], f2o(ep[i][k])); hi[k] = max(hi[k], f2o(ep[i][k])); }
         }
+        const float il = rsqrtf(f3dot(d, d));
+        const float3 v = make_float3(d.x * il, d.y * il, d.z * il);
+        bool bad = false;
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const int64_t qe = e == 0 ? u * kUnit : min(u * kUnit + kUnit - 1, n - 1);
+            const float3 oe = load3(ro, qe), de = load3(rd, qe);
+            const float ie = rsqrtf(f3dot(de, de));
+            const float3 ve = make_float3(de.x * ie, de.y * ie, de.z * ie);
+            bad |= !(f3inf(f3sub(ve, v)) <= kCohDir && f3inf(f3sub(oe, o)) <= spread_max);   // NaN: bad
+        }
+        s_ray[li][0] = v.x; s_ray[li][1] = v.y; s_ray[li][2] = v.z;
+        s_ray[li][3] = o.x; s_ray[li][4] = o.y; s_ray[li][5] = o.z;
+        s_bad[li] = bad || !(f3inf(v) <= 1.f);   // a non-finite fourth ray: bad
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -1552,17 +1748,45 @@ __global__ void __launch_bounds__(kOrdThreads) k_ray_order(int64_t n, const floa
 #pragma unroll
     for (int i = 0; i < kOrdItems; ++i) {
         val[i] = (uint16_t)(i * kOrdThreads + t);
-        if (kind[i] != 0) { key[i] = kind[i] == 1 ? 0x40000000u : 0x80000000u; continue; }
+        if (kind[i] == 2) { key[i] = 0x80000000u; continue; }
         uint32_t g[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) g[k] = (uint32_t)fminf(fmaxf((ep[i][k] - wlo[k]) * sc, 0.f), 1023.f);
-        key[i] = spread3(g[0]) | (spread3(g[1]) << 1) | (spread3(g[2]) << 2);
+        key[i] = spread3(g[0]) | (spread3(g[1]) << 1) | (spread3(g[2]) << 2) | (kind[i] == 1 ? 0x40000000u : 0u);
     }
     Sort(s_sort).SortBlockedToStriped(key, val, 0, 32);
 #pragma unroll
     for (int i = 0; i < kOrdItems; ++i) {
-        const int64_t r = u0 + i * kOrdThreads + t;      // rank i * kOrdThreads + t of the window
-        if (r < units) order[r] = (uint32_t)(u0 + val[i]);
+        const int rank = i * kOrdThreads + t;            // rank of the window
+        s_sorted[rank] = val[i];
+        if (u0 + rank < units) order[u0 + rank] = (uint32_t)(u0 + val[i]);
+    }
+    __syncthreads();
+    // packet t of the window: sorted units 4t .. 4t + 3
+    const int64_t pk = (int64_t)blockIdx.x * (kOrdUnits / 4) + t;
+    const bool valid = u0 + 4 * t < units;
+    bool inc = false;
+    if (valid) {
+        const int f = s_sorted[4 * t];
+        inc = s_bad[f];
+        for (int j = 1; j < 4 && u0 + 4 * t + j < units; ++j) {
+            const int v = s_sorted[4 * t + j];
+            float dv = 0.f, dov = 0.f;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                dv = fmaxf(dv, fabsf(s_ray[v][k] - s_ray[f][k]));
+                dov = fmaxf(dov, fabsf(s_ray[v][3 + k] - s_ray[f][3 + k]));
+            }
+            inc |= s_bad[v] || !(dv <= kCohDir && dov <= spread_max);
+        }
+        skip[pk] = inc ? 1 : 0;
+    }
+    const unsigned m = __ballot_sync(kFull, valid && inc);
+    if (m) {                          // one atomic per warp
+        unsigned long long base = 0;
+        if ((t & 31) == __ffs(m) - 1) base = atomicAdd(lanes_n, (unsigned long long)__popc(m));
+        base = __shfl_sync(kFull, base, __ffs(m) - 1);
+        if (valid && inc) lanes[base + __popc(m & ((1u << (t & 31)) - 1u))] = (uint32_t)pk;
     }
 }
 
@@ -1609,6 +1833,22 @@ float packets_per_warp(int64_t packets, unsigned grid) {
 }
 }  // namespace
 
+namespace {
+// Ray launch workspace: counters (256 bytes), the unit order, a skip flag
+// per packet, the list of incoherent packets; byte offsets and total.
+struct RayWs { size_t order, skip, lanes, end; };
+RayWs ray_ws(int64_t n) {
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t units = (size_t)((n + kUnit - 1) / kUnit), packets = (size_t)((n + 31) / 32);
+    RayWs r;
+    r.order = 256;
+    r.skip = r.order + al(sizeof(uint32_t) * units);
+    r.lanes = r.skip + al(packets);
+    r.end = r.lanes + al(sizeof(uint32_t) * packets);
+    return r;
+}
+}  // namespace
+
 size_t query_workspace_bytes(int mode, int64_t n) {
     size_t b = 256;                                               // packet counters
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
@@ -1623,7 +1863,7 @@ size_t query_workspace_bytes(int mode, int64_t n) {
     if (mode == 1) b += al(sizeof(uint32_t) * n);                 // watertight overflow queue
     if (mode >= 0) b += al(sizeof(uint2) * heavy_cap_for(n));     // heavy-query list
     if (mode == 2) b += al(sizeof(uint4) * n);                    // raystab candidates (second pass)
-    if (mode == -1 && n >= kOrdMinRays) b += al(sizeof(uint32_t) * ((n + kUnit - 1) / kUnit));   // ray unit order
+    if (mode == -1) b = ray_ws(n).end;                           // unit order, skip flags, incoherent packets
     return b;
 }
 
@@ -1640,6 +1880,8 @@ enum : int {
     kCtOvfN = 10,       // watertight overflow queue length
     kCtCandN = 12,      // raystab second-pass candidates
     kCtLinesNext = 13,  // raystab second-pass queue
+    kCtRayLanesN = 14,  // incoherent ray packets listed by k_ray
+    kCtRayLanesNext = 15,  // k_ray_lanes queue
 };
 // packets per atomic grab: about 64 grabs per warp of the launch
 int64_t grab_for(int64_t n, unsigned grid) {
@@ -1789,15 +2031,20 @@ cudaError_t launch_ray(int64_t n, const float* ro, const float* rd, float* pos, 
     unsigned long long* ctr = reinterpret_cast<unsigned long long*>(ws);
     cudaError_t e = cudaMemsetAsync(ctr, 0, 256, stream);
     if (e != cudaSuccess) return e;
-    uint32_t* order = nullptr;
-    if (n >= kOrdMinRays) {
-        order = reinterpret_cast<uint32_t*>(static_cast<char*>(ws) + 256);
-        const int64_t units = (n + kUnit - 1) / kUnit;
-        k_ray_order<<<(unsigned)((units + kOrdUnits - 1) / kOrdUnits), kOrdThreads, 0, stream>>>(n, ro, rd, nodes,
-                                                                                                order); count_launch();
-    }
+    const RayWs r = ray_ws(n);
+    char* w = static_cast<char*>(ws);
+    uint32_t* order = reinterpret_cast<uint32_t*>(w + r.order);
+    uint8_t* skip = reinterpret_cast<uint8_t*>(w + r.skip);
+    uint32_t* lanes = reinterpret_cast<uint32_t*>(w + r.lanes);
+    const int64_t units = (n + kUnit - 1) / kUnit;
+    k_ray_order<<<(unsigned)((units + kOrdUnits - 1) / kOrdUnits), kOrdThreads, 0, stream>>>(
+        n, ro, rd, nodes, order, skip, lanes, ctr + kCtRayLanesN); count_launch();
     const unsigned g = persistent_grid(k_ray, n);
-    k_ray<<<g, kQBlock, 0, stream>>>(n, order, ro, rd, pos, fid, depth, nodes, tris, ctr + kCtUdf, grab_for(n, g)); count_launch();
+    k_ray<<<g, kQBlock, 0, stream>>>(n, order, ro, rd, pos, fid, depth, nodes, tris, ctr + kCtUdf, grab_for(n, g),
+                                     skip); count_launch();
+    const unsigned gl = persistent_grid(k_ray_lanes, n);
+    k_ray_lanes<<<gl, kQBlock, 0, stream>>>(n, order, ro, rd, pos, fid, depth, nodes, tris, lanes,
+                                            ctr + kCtRayLanesN, ctr + kCtRayLanesNext); count_launch();
     return cudaGetLastError();
 }
 
