@@ -1,7 +1,7 @@
 """Throughput benchmark of the cubvh query path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload rays_displaced|udf_icosphere|dense_tori|raystab_displaced|
+                    [--workload rays_displaced|rays_incoherent|udf_icosphere|dense_tori|raystab_displaced|
                                 grad_displaced|batch_256|sparse_mc_band]
 
 Default workload (``rays_displaced``): displaced icosphere level 6 (81,920
@@ -203,6 +203,13 @@ def build_workload(name: str, res: int = 2048, sdf_points: int = 8 << 20, grid: 
                     ops=[("ray", (w["rays_o"], w["rays_d"])), ("sdf_watertight", (w["points"],))],
                     desc=f"displaced icosphere L6 (81,920 faces); {8 * res * res:,} rays (8 x {res}^2 pinhole, "
                          f"fov 50, r 2.5) + {sdf_points:,} watertight SDF points")
+    if name == "rays_incoherent":
+        v, f = W.displaced_icosphere(6, 1)
+        n = 16 << 20
+        ro, rd = W.incoherent_rays(n)
+        return dict(name=name, vertices=v, faces=f, ops=[("ray", (ro, rd))], cpu_sample=1 << 20,
+                    desc=f"displaced icosphere L6 (81,920 faces); {n:,} incoherent rays: half from U[-1,1]^3 in "
+                         "random directions, half from the radius-3 sphere at random points of [-0.8,0.8]^3")
     if name == "udf_icosphere":
         w = W.udf_icosphere()
         return dict(name=name, vertices=w["vertices"], faces=w["faces"],
@@ -1216,7 +1223,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="rays_displaced",
-                    choices=["rays_displaced", "udf_icosphere", "dense_tori", "raystab_displaced",
+                    choices=["rays_displaced", "rays_incoherent", "udf_icosphere", "dense_tori", "raystab_displaced",
                              "grad_displaced", "batch_256", "sparse_mc_band"])
     ap.add_argument("--adam-steps", type=int, default=200, help="grad_displaced: sphere-fitting steps")
     ap.add_argument("--meshes", type=int, default=256, help="batch_256: number of meshes")

@@ -1668,10 +1668,11 @@ __device__ __forceinline__ int ray_entry(float3 o, float3 d, const float lo[3], 
 // One block per window: entry points of the units' rays, the box of those
 // that enter, Morton keys, a block radix sort of (key, unit in the window),
 // and the sorted unit indices written to order[].  Then each packet of the
-// window (4 consecutive sorted units) is judged: coherent when the first,
-// fourth and last rays of its units all lie within kCohDir (directions) and
-// kCohOrigin (origins) of its first unit's fourth ray.  skip[p] = 1 marks
-// the others for k_ray, and they are listed for k_ray_lanes.
+// window (4 consecutive sorted units) is judged: coherent when each unit's
+// first and last rays lie within kCohDir (unit directions, max-norm) and
+// kCohOrigin (origins) of the unit's fourth ray, and each unit's fourth ray
+// within the same of the first unit's.  skip[p] = 1 marks the others for
+// k_ray, and they are listed for k_ray_lanes.
 __global__ void __launch_bounds__(kOrdThreads) k_ray_order(int64_t n, const float* __restrict__ ro,
                                                            const float* __restrict__ rd,
                                                            const CNode* __restrict__ nodes,

@@ -256,6 +256,24 @@ def rays_displaced(res: int = 2048, n_poses: int = 8, n_sdf: int = 8 << 20):
     return dict(vertices=v, faces=f, rays_o=ro, rays_d=rd, points=pts)
 
 
+def incoherent_rays(n: int, seed: int = 5):
+    """n float32 rays without coherence between neighbours: the first half
+    start uniformly in [-1, 1]^3 with uniformly random unit directions, the
+    second half start on the sphere of radius 3 and point at uniform random
+    points of [-0.8, 0.8]^3."""
+    rng = np.random.default_rng(seed)
+    h = n // 2
+    o1 = rng.uniform(-1, 1, (h, 3))
+    d1 = rng.standard_normal((h, 3))
+    s = rng.standard_normal((n - h, 3))
+    o2 = 3 * s / np.linalg.norm(s, axis=1, keepdims=True)
+    d2 = rng.uniform(-0.8, 0.8, (n - h, 3)) - o2
+    o = np.concatenate([o1, o2]).astype(np.float32)
+    d = np.concatenate([d1, d2])
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    return o, d
+
+
 def dense_tori(res: int = 512):
     v, f = random_tori(2)
     return dict(vertices=v, faces=f, grid_res=res)
