@@ -127,6 +127,9 @@ int cubvh_signed_distance(cubvh_bvh* bvh, const float* points, int64_t n, uint32
 /* Closest hit along each ray with 0 <= t < 1000.
  * rays_o, rays_d float32 [n, 3]; positions float32 [n, 3] = o + t d;
  * face_id int64 [n] (-1 on a miss); depth float32 [n] (1000 on a miss).
+ * Rays are traced in groups of nearby rays (groups of rays that are not
+ * near one another ray by ray); each ray's result is its own, whatever the
+ * order of the rays or how they are split across calls.
  * Replaces cuBVH::ray_trace (src/api_gpu.cu:70-81, src/bvh.cu:490-513,
  * 714-740). */
 int cubvh_ray_trace(cubvh_bvh* bvh, const float* rays_o, const float* rays_d, int64_t n, float* positions,
