@@ -1724,7 +1724,7 @@ __global__ void __launch_bounds__(kOrdThreads) k_ray_order(int64_t n, const floa
         }
         s_ray[li][0] = v.x; s_ray[li][1] = v.y; s_ray[li][2] = v.z;
         s_ray[li][3] = o.x; s_ray[li][4] = o.y; s_ray[li][5] = o.z;
-        s_bad[li] = bad || !(f3inf(v) <= 1.f);   // a non-finite fourth ray: bad
+        s_bad[li] = bad || !(f3inf(v) <= 2.f);   // a non-finite (or zero) fourth direction: bad
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
