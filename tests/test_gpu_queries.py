@@ -540,3 +540,20 @@ def test_ray_trace_window_order(oracle, dev):
     m_t = torch.from_numpy(keep).to(dev)
     for x, y in zip(got, whole):
         assert torch.equal(x[m_t], y[m_t])
+
+
+def test_ray_trace_axis_parallel_grid(oracle, dev):
+    """A 256 x 256 grid of rays along +z and along -x (the rays of a
+    voxeliser or a parity test: zero direction components, one direction
+    for all), traced in packets: results equal the oracle's."""
+    v, f = W.displaced_icosphere(4, 1)
+    bvh = cubvh.cuBVH(v, f)
+    g = np.linspace(-1.1, 1.1, 256)
+    x, y = np.meshgrid(g, g, indexing="ij")
+    ro_z = np.stack([x.ravel(), y.ravel(), np.full(x.size, -2.0)], 1)
+    ro_x = np.stack([np.full(x.size, 2.0), x.ravel(), y.ravel()], 1)
+    ro = np.concatenate([ro_z, ro_x]).astype(np.float32)
+    rd = np.concatenate([np.tile([0.0, 0.0, 1.0], (x.size, 1)), np.tile([-1.0, 0.0, 0.0], (x.size, 1))]).astype(np.float32)
+    out = bvh.ray_trace(torch.from_numpy(ro).to(dev), torch.from_numpy(rd).to(dev))
+    check_rays(oracle, v, f, ro, rd, out)
+    assert 0.2 < (_np(out[1]) >= 0).mean() < 0.9
