@@ -448,3 +448,22 @@ def test_bench_reference_arm_contract():
     assert d["cpu_baseline"]["kind"] in ("reference", "port") and d["cpu_baseline"]["value"] == d["value"]
     assert d["e2e"] == {"value": d["value"], "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     assert d["config"]["workload"] == "rays_displaced"
+
+
+def test_incoherent_rays_workload():
+    """The incoherent-ray generator behind bench.py's rays_incoherent
+    workload: float32 unit directions; the first half start in [-1, 1]^3, the
+    second half on the radius-3 sphere, pointing into [-0.8, 0.8]^3."""
+    o, d = W.incoherent_rays(1001, seed=3)
+    assert o.shape == d.shape == (1001, 3) and o.dtype == d.dtype == np.float32
+    np.testing.assert_allclose(np.linalg.norm(d, axis=1), 1.0, rtol=1e-6)
+    h = 1001 // 2
+    assert (np.abs(o[:h]) <= 1).all()
+    np.testing.assert_allclose(np.linalg.norm(o[h:], axis=1), 3.0, rtol=1e-6)
+    # the second half's rays pass through a point of the inner box, so they
+    # come within its half-diagonal 0.8 sqrt(3) of the centre
+    oo, dd = o[h:].astype(np.float64), d[h:].astype(np.float64)
+    closest = oo - dd * (oo * dd).sum(1, keepdims=True)
+    assert (np.linalg.norm(closest, axis=1) <= 0.8 * np.sqrt(3) + 1e-5).all()
+    o2, d2 = W.incoherent_rays(1001, seed=3)
+    assert np.array_equal(o, o2) and np.array_equal(d, d2)
